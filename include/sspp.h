@@ -1,0 +1,136 @@
+/*
+ * sspp.h - C ABI of the B200 persistent-homology reduction engine.
+ *
+ * The reference (SpecSeq++) exposes no library API: its only entry points are
+ * the `specseq++` command line (src/main.cu:269-352) and the header-only C++
+ * class SpecSeqPlusPlus (include/specseq.h:63-1194).  Every function below
+ * names the reference interface it replaces.  Conventions: plain pointers and
+ * sizes, no CUDA or torch types; int status codes (SSPP_OK = 0) instead of the
+ * reference's exit(EXIT_FAILURE) (include/kernel.h:26-32); the caller owns
+ * input buffers, the context owns all device state; one context per host
+ * thread.  Streams are passed as `void*` holding a cudaStream_t (NULL = the
+ * context's own stream).
+ */
+#ifndef SSPP_H_
+#define SSPP_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define SSPP_OK 0
+#define SSPP_ERR_BAD_INPUT 1  /* malformed matrix, bad parameter, bad file       */
+#define SSPP_ERR_CAPACITY 2   /* device arena or a size limit exhausted          */
+#define SSPP_ERR_CUDA 3       /* a CUDA runtime call failed                      */
+#define SSPP_ERR_TIMEOUT 4    /* a bounded device loop hit its iteration limit   */
+#define SSPP_ERR_STATE 5      /* call out of order (e.g. compute before init)    */
+#define SSPP_ERR_IO 6         /* file could not be opened / written              */
+
+/* file formats of src/main.cu:34-37 */
+#define SSPP_ASCII 0
+#define SSPP_BINARY 1
+
+typedef struct sspp_ctx sspp_ctx;
+
+typedef struct sspp_config {
+    int32_t device;          /* CUDA device ordinal                                  */
+    int64_t arena_bytes;     /* initial column arena; 0 = sized from the input       */
+    int32_t verbose;         /* 0 = silent                                           */
+} sspp_config;
+
+/* The reference's 12 positional CLI values (src/main.cu:281-294) minus file
+ * names/formats.  `autotune` != 0 replaces ss_block_size, growth, queue_size and
+ * the level capacities with the engine's tuned values for the input's size
+ * class. */
+typedef struct sspp_params {
+    int32_t dualize;          /* 0/1                                                  */
+    int32_t model;            /* bit0 high-dimension guided clearing, bit1 collapse   */
+    int32_t max_iteration;    /* candidates per simplex for guided clearing           */
+    int32_t ss_block_size;    /* initial spectral-sequence block size                 */
+    float growth;             /* block_size_growth_rate (>= 1)                        */
+    int32_t queue_size;       /* concurrent column workers per launch                 */
+    int32_t level1_capacity;  /* per-worker on-chip column capacity (ints)            */
+    int32_t level2_capacity;  /* per-block on-chip column capacity (ints)             */
+    int32_t autotune;
+} sspp_params;
+
+/* Per-run counters (device-side counters plus host timings). */
+typedef struct sspp_stats {
+    int64_t ncols, nnz;
+    int64_t active_after_init;   /* columns left for the reduction after init     */
+    int64_t apparent_pairs;      /* pivots found by the init pass                  */
+    int64_t cleared_init;        /* columns cleared by the init pass               */
+    int64_t highclear_cleared;   /* top-dimension columns cleared by guided clear  */
+    int64_t collapse_dropped;    /* columns removed by edge collapse               */
+    int64_t additions;           /* column additions performed on the device       */
+    int64_t add_ints;            /* sum of |a| + |b| + |a xor b| over additions    */
+    int64_t published_ints;      /* arena ints written by the reduction            */
+    int64_t displaced;           /* pivot owners displaced by smaller columns      */
+    int64_t ss_steps;            /* spectral-sequence launches                     */
+    int64_t npairs, nessential;
+    double init_ms, compute_ms;  /* GPU_Init / GPU_Compute equivalents            */
+} sspp_stats;
+
+/* Replaces: the SpecSeqPlusPlus constructor's allocation (include/specseq.h:486-512). */
+sspp_ctx* sspp_create(const sspp_config* cfg);
+void sspp_destroy(sspp_ctx* ctx);
+const char* sspp_last_error(const sspp_ctx* ctx);
+/* Fills *p with the reference's defaults (README.md:26-51): no dualize,
+ * model 0, max_iteration 0, ss_block_size 102400, growth 1.05,
+ * queue_size 65536, level capacities 1000 / 8000. */
+void sspp_default_params(sspp_params* p);
+
+/* Replaces: processFiles (src/main.cu:90-167).  fmt = SSPP_ASCII / SSPP_BINARY.
+ * Ascii indices are 0-based face indices; binary is PHAT's int64 layout (the
+ * reference skips the +1 shift for binary files, src/main.cu:146-155; here both
+ * formats are read the same way). */
+int32_t sspp_load_phat(sspp_ctx* ctx, const char* path, int32_t fmt);
+
+/* Replaces: the hv_csc / hv_dim vectors handed to the SpecSeqPlusPlus
+ * constructor (src/main.cu:324-335).  Host arrays in filtration order:
+ * dims[ncols], col_ptr[ncols+1] (int64), rows[col_ptr[ncols]] with each column's
+ * face indices ascending and unique.  Copied to the device at once. */
+int32_t sspp_load_csc(sspp_ctx* ctx, int64_t ncols, const int32_t* dims, const int64_t* col_ptr, const int32_t* rows);
+
+/* Same, for arrays already resident in device memory (no host copy). */
+int32_t sspp_load_csc_device(sspp_ctx* ctx, int64_t ncols, const int32_t* d_dims, const int64_t* d_col_ptr,
+                             const int32_t* d_rows);
+
+/* Replaces: SpecSeqPlusPlus::GPU_Init (include/specseq.h:513-590): dimension
+ * reorder, edge collapse, guided clearing, init passes, dualization, active
+ * lists.  Blocks until done. */
+int32_t sspp_init(sspp_ctx* ctx, const sspp_params* p, void* stream);
+
+/* Replaces: SpecSeqPlusPlus::GPU_Compute (include/specseq.h:592-1060): the
+ * spectral-sequence reduction, entirely on the device (no CPU tail stage).
+ * Blocks until done. */
+int32_t sspp_compute(sspp_ctx* ctx, void* stream);
+
+/* sspp_init + sspp_compute. */
+int32_t sspp_reduce(sspp_ctx* ctx, const sspp_params* p, void* stream);
+
+/* Replaces: GetPersistencePairs (include/specseq.h:1182-1193).  Pairs in input
+ * (0-based) indices, sorted by (birth, death), written as birth,death int64
+ * pairs.  Returns the number of pairs, or -1 on error; copies at most cap pairs. */
+int64_t sspp_num_pairs(sspp_ctx* ctx);
+int64_t sspp_pairs(sspp_ctx* ctx, int64_t* out_birth_death, int64_t cap);
+
+/* Essential (never paired) simplices in input indices, ascending; simplices
+ * removed by edge collapse are not listed.  The reference does not report
+ * these; PHAT's pair files do not either. */
+int64_t sspp_num_essential(sspp_ctx* ctx);
+int64_t sspp_essentials(sspp_ctx* ctx, int64_t* out, int64_t cap);
+
+/* Replaces: writeVectorToFile (src/main.cu:191-229). */
+int32_t sspp_write_pairs(sspp_ctx* ctx, const char* path, int32_t fmt);
+
+int32_t sspp_get_stats(const sspp_ctx* ctx, sspp_stats* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SSPP_H_ */

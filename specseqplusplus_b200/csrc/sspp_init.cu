@@ -1,0 +1,426 @@
+// Dimension reorder, init passes, active lists and pair extraction.
+//
+// Reference counterparts:
+//   dimension-stable reorder           include/specseq.h:439-483 (Formatted)
+//   lowest one / leftmost column       include/kernel.h:444-457 (initleft_kernel)
+//   apparent pivots, youngest-facet
+//   clearing, negative columns         include/kernel.h:459-481 (initlookup_kernel)
+//   clearing                           include/kernel.h:483-493 (clearing_kernel)
+//   row compression                    include/kernel.h:495-520 (compress_kernel)
+//   active list and per-dim bounds     include/specseq.h:365-409 (ColumnShrink)
+//   pairs in input indices, sorted     include/specseq.h:1182-1193
+// Here the reorder, the padded column layout and the compaction are device
+// passes (the reference does them on the host), the active list is a device
+// stream compaction, and pairs come out sorted by construction (each simplex is
+// the birth of at most one pair, so compaction in birth order sorts them).
+#include <climits>
+
+#include "sspp_launch.h"
+#include "sspp_scan.cuh"
+
+namespace sspp {
+
+__global__ void __launch_bounds__(1024) k_scan_blocks(int64_t* blk, int64_t nb) {
+    __shared__ int64_t wt[32];
+    __shared__ int64_t carry;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    if (tid == 0) carry = 0;
+    __syncthreads();
+    for (int64_t base = 0; base < nb; base += 1024) {
+        int64_t i = base + tid;
+        int64_t v = i < nb ? blk[i] : 0;
+        int64_t inc = warp_inclusive_scan(v);
+        if (lane == 31) wt[wid] = inc;
+        __syncthreads();
+        if (wid == 0) {
+            int64_t t = wt[lane];
+            int64_t ti = warp_inclusive_scan(t);
+            wt[lane] = ti - t;
+        }
+        __syncthreads();
+        int64_t ex = carry + wt[wid] + inc - v;
+        if (i < nb) blk[i] = ex;
+        __syncthreads();
+        if (tid == 1023) carry = ex + v;
+        __syncthreads();
+    }
+    if (tid == 0) blk[nb] = carry;
+}
+
+template <typename T>
+__global__ void k_fill(T* p, T v, int64_t n) {
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) p[i] = v;
+}
+
+static unsigned grid_for(int64_t n, int threads) {
+    int64_t g = (n + threads - 1) / threads;
+    if (g < 1) g = 1;
+    if (g > (int64_t(1) << 30)) g = int64_t(1) << 30;
+    return unsigned(g);
+}
+
+void fill_i32(int32_t* p, int32_t v, int64_t n, cudaStream_t s) {
+    if (n > 0) k_fill<int32_t><<<grid_for(n, 256) > 4096 ? 4096 : grid_for(n, 256), 256, 0, s>>>(p, v, n);
+}
+void fill_i64(int64_t* p, int64_t v, int64_t n, cudaStream_t s) {
+    if (n > 0) k_fill<int64_t><<<grid_for(n, 256) > 4096 ? 4096 : grid_for(n, 256), 256, 0, s>>>(p, v, n);
+}
+
+// Input validation before any index is used: dimensions in range and col_ptr
+// non-decreasing from 0 (device-resident inputs are only checked here).
+__global__ void k_validate(const int32_t* dims, const int64_t* colptr, int64_t n, int* err) {
+    for (int64_t j = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; j < n; j += int64_t(gridDim.x) * blockDim.x) {
+        int d = dims[j];
+        int64_t a = colptr[j], b = colptr[j + 1];
+        if (d < 0 || d > kMaxDim || b < a || b - a > kMaxColLen || (j == 0 && a != 0)) atomicOr(err, ERRB_BAD_INPUT);
+    }
+}
+
+void validate(Device& D, cudaStream_t s) {
+    if (D.n > 0) k_validate<<<grid_for(D.n, 256) > 4096 ? 4096 : grid_for(D.n, 256), 256, 0, s>>>(D.in_dims, D.in_colptr, D.n, D.err);
+}
+
+// ------------------------------------------------------------------ reorder
+constexpr int kPartThreads = 256;
+
+// per-block count of columns of each dimension; flags dims out of range
+__global__ void __launch_bounds__(kPartThreads) k_dim_count(const int32_t* dims, int64_t n, int32_t* dimcnt, int* err) {
+    __shared__ int cnt[kNumDims];
+    if (threadIdx.x < kNumDims) cnt[threadIdx.x] = 0;
+    __syncthreads();
+    int64_t j = int64_t(blockIdx.x) * kPartThreads + threadIdx.x;
+    if (j < n) {
+        int d = dims[j];
+        if (d < 0 || d > kMaxDim) atomicOr(err, ERRB_BAD_INPUT);
+        else atomicAdd(&cnt[d], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x < kNumDims) dimcnt[int64_t(blockIdx.x) * kNumDims + threadIdx.x] = cnt[threadIdx.x];
+}
+
+// one block: per-dimension exclusive scan over blocks, then global dim starts
+__global__ void __launch_bounds__(1024) k_dim_offsets(int32_t* dimcnt, int64_t nb, DimInfo* info) {
+    __shared__ int64_t tot[kNumDims];
+    __shared__ int64_t wt[32];
+    __shared__ int64_t carry;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    for (int d = 0; d < kNumDims; d++) {
+        if (tid == 0) carry = 0;
+        __syncthreads();
+        for (int64_t base = 0; base < nb; base += 1024) {
+            int64_t i = base + tid;
+            int64_t v = i < nb ? dimcnt[i * kNumDims + d] : 0;
+            int64_t inc = warp_inclusive_scan(v);
+            if (lane == 31) wt[wid] = inc;
+            __syncthreads();
+            if (wid == 0) {
+                int64_t t = wt[lane];
+                int64_t ti = warp_inclusive_scan(t);
+                wt[lane] = ti - t;
+            }
+            __syncthreads();
+            int64_t ex = carry + wt[wid] + inc - v;
+            if (i < nb) dimcnt[i * kNumDims + d] = int32_t(ex);
+            __syncthreads();
+            if (tid == 1023) carry = ex + v;
+            __syncthreads();
+        }
+        if (tid == 0) tot[d] = carry;
+        __syncthreads();
+    }
+    if (tid == 0) {
+        int64_t s = 0;
+        for (int d = 0; d < kNumDims; d++) {
+            info->col_begin[d] = int32_t(s);
+            s += tot[d];
+            info->col_end[d] = int32_t(s);
+        }
+    }
+}
+
+// stable rank of each column inside its dimension -> reordered index
+__global__ void __launch_bounds__(kPartThreads) k_dim_assign(const int32_t* dims, int64_t n, const int32_t* dimcnt,
+                                                             const DimInfo* info, int32_t* newidx, int32_t* perm,
+                                                             int32_t* rdim) {
+    __shared__ int wcnt[kPartThreads / 32][kNumDims];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int64_t j = int64_t(blockIdx.x) * kPartThreads + threadIdx.x;
+    int d = (j < n) ? dims[j] : -1;
+    if (d > kMaxDim) d = -1;
+    unsigned my_ballot = 0;
+#pragma unroll
+    for (int v = 0; v < kNumDims; v++) {
+        unsigned b = __ballot_sync(kFull, d == v);
+        if (d == v) my_ballot = b;
+        if (lane == 0) wcnt[wid][v] = __popc(b);
+    }
+    __syncthreads();
+    if (d >= 0) {
+        int r = __popc(my_ballot & lanemask_lt());
+        for (int w = 0; w < wid; w++) r += wcnt[w][d];
+        int32_t idx = info->col_begin[d] + dimcnt[int64_t(blockIdx.x) * kNumDims + d] + r;
+        newidx[j] = idx;
+        perm[idx] = int32_t(j);
+        rdim[idx] = d;
+    }
+}
+
+// Copies input column perm[i] into its padded arena slot with rows remapped to
+// reordered indices; validates face dimension, range and strict order.
+__global__ void k_scatter_cols(int64_t n, const int64_t* colptr, const int32_t* rows, const int32_t* dims,
+                               const int32_t* perm, const int32_t* newidx, const int64_t* off, int32_t* arena,
+                               uint64_t* desc, int32_t* leftmost, int* err) {
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+        const int32_t j = perm[i];
+        const int64_t b = colptr[j], e = colptr[j + 1];
+        const int64_t len = e - b;
+        const int64_t o = off[i];
+        const int dj = dims[j];
+        bool bad = len < 0 || len > kMaxColLen;
+        int32_t prev = -1;
+        for (int64_t k = 0; k < len && !bad; k++) {
+            int32_t r = rows[b + k];
+            if (r < 0 || r >= n || r <= prev || dims[r] != dj - 1) { bad = true; break; }
+            prev = r;
+            arena[o + k] = newidx[r];
+        }
+        if (bad) {
+            atomicOr(err, ERRB_BAD_INPUT);
+            desc[i] = pack_desc(uint64_t(o), 0);
+        } else {
+            for (int64_t k = len; k < pad4(len); k++) arena[o + k] = INT_MAX;
+            desc[i] = pack_desc(uint64_t(o), uint32_t(len));
+        }
+        leftmost[i] = INT_MAX;
+    }
+}
+
+int64_t reorder_total_slot(const Device& D) { return scan_blocks(D.n); }
+
+void reorder(Device& D, cudaStream_t s) {
+    const int64_t n = D.n;
+    const int64_t nb = (n + kPartThreads - 1) / kPartThreads;
+    k_dim_count<<<unsigned(nb), kPartThreads, 0, s>>>(D.in_dims, n, D.dimcnt, D.err);
+    k_dim_offsets<<<1, 1024, 0, s>>>(D.dimcnt, nb, D.diminfo);
+    k_dim_assign<<<unsigned(nb), kPartThreads, 0, s>>>(D.in_dims, n, D.dimcnt, D.diminfo, D.newidx, D.perm, D.dim);
+    // padded column offsets in reordered order
+    const int64_t* colptr = D.in_colptr;
+    const int32_t* perm = D.perm;
+    int64_t* off = D.scratch64;
+    scan([=] __device__(int64_t i) -> int64_t { int32_t j = perm[i]; return pad4(colptr[j + 1] - colptr[j]); },
+         [=] __device__(int64_t i, int64_t pre, int64_t) { off[i] = pre; }, n, D.blk, s);
+    k_scatter_cols<<<grid_for(n, 256) > 65536 ? 65536 : grid_for(n, 256), 256, 0, s>>>(
+        n, D.in_colptr, D.in_rows, D.in_dims, D.perm, D.newidx, off, D.arena, D.desc, D.leftmost, D.err);
+}
+
+// ------------------------------------------------------------- init passes
+__global__ void k_init_low(int64_t n, const int32_t* arena, const uint64_t* desc, int32_t* low, int32_t* leftmost,
+                           int32_t* pivot, uint8_t* cleared, uint8_t* negative) {
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+        uint64_t d = desc[i];
+        const int32_t* c = arena + desc_off(d);
+        uint32_t len = desc_len(d);
+        low[i] = len ? c[len - 1] : -1;
+        for (uint32_t k = 0; k < len; k++) atomicMin(&leftmost[c[k]], int32_t(i));
+        pivot[i] = -1;
+        cleared[i] = 0;
+        negative[i] = 0;
+    }
+}
+
+__global__ void k_init_apparent(int64_t n, const int32_t* arena, const uint64_t* desc, const int32_t* low,
+                                const int32_t* leftmost, int32_t* pivot, uint8_t* cleared, uint8_t* negative,
+                                long long* counters) {
+    long long app = 0;
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+        int32_t l = low[i];
+        if (l < 0) continue;
+        cleared[l] = 1;  // the youngest facet of any simplex is positive
+        if (leftmost[l] == int32_t(i)) {
+            pivot[l] = int32_t(i);  // no earlier column can ever reach row l
+            app++;
+        }
+        uint64_t d = desc[i];
+        const int32_t* c = arena + desc_off(d);
+        uint32_t len = desc_len(d);
+        for (uint32_t k = 0; k < len; k++)
+            if (leftmost[c[k]] == int32_t(i)) { negative[i] = 1; break; }
+    }
+    app = warp_sum(app);
+    if ((threadIdx.x & 31) == 0 && app) cnt_add(&counters[CNT_APPARENT], app);
+}
+
+// Clears positive columns and removes negative rows in place.
+__global__ void k_init_compress(int64_t n, int32_t* arena, uint64_t* desc, int32_t* low, const int32_t* pivot,
+                                const uint8_t* cleared, const uint8_t* negative, uint8_t* state,
+                                const uint8_t* dropped, long long* counters, int* err) {
+    long long ncl = 0, nact = 0;
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+        uint64_t d = desc[i];
+        int32_t* c = arena + desc_off(d);
+        uint32_t len = desc_len(d);
+        if (dropped && dropped[i]) {
+            desc[i] = pack_desc(desc_off(d), 0);
+            low[i] = -1;
+            state[i] = ST_DROPPED;
+            continue;
+        }
+        if (cleared[i]) {
+            if (len && pivot[low[i]] == int32_t(i)) atomicOr(err, ERRB_BAD_INPUT);  // positive and negative at once
+            desc[i] = pack_desc(desc_off(d), 0);
+            low[i] = -1;
+            state[i] = ST_CLEARED;
+            ncl++;
+            continue;
+        }
+        uint32_t m = 0;
+        for (uint32_t k = 0; k < len; k++) {
+            int32_t r = c[k];
+            if (!negative[r]) c[m++] = r;
+        }
+        for (uint32_t k = m; k < len; k++) c[k] = INT_MAX;
+        desc[i] = pack_desc(desc_off(d), m);
+        int32_t l = m ? c[m - 1] : -1;
+        low[i] = l;
+        uint8_t st = (m == 0) ? ST_ZERO : (pivot[l] == int32_t(i) ? ST_OWNER : ST_ACTIVE);
+        state[i] = st;
+        nact += (st == ST_ACTIVE);
+    }
+    ncl = warp_sum(ncl);
+    nact = warp_sum(nact);
+    if ((threadIdx.x & 31) == 0) {
+        if (ncl) cnt_add(&counters[CNT_CLEARED], ncl);
+        if (nact) cnt_add(&counters[CNT_ACTIVE], nact);
+    }
+}
+
+// per-dimension min first row over non-empty columns and max low + 1 over
+// active columns (ColumnShrink, include/specseq.h:374-398)
+__global__ void k_dim_rows(int64_t n, const int32_t* rdim, const int32_t* arena, const uint64_t* desc,
+                           const int32_t* low, const uint8_t* state, DimInfo* info) {
+    __shared__ int smin[kNumDims], smax[kNumDims];
+    if (threadIdx.x < kNumDims) { smin[threadIdx.x] = INT_MAX; smax[threadIdx.x] = -1; }
+    __syncthreads();
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+        uint64_t d = desc[i];
+        uint32_t len = desc_len(d);
+        if (!len) continue;
+        int dm = rdim[i];
+        atomicMin(&smin[dm], arena[desc_off(d)]);
+        if (state[i] == ST_ACTIVE) atomicMax(&smax[dm], low[i] + 1);
+    }
+    __syncthreads();
+    if (threadIdx.x < kNumDims) {
+        if (smin[threadIdx.x] != INT_MAX) atomicMin(&info->min_row[threadIdx.x], smin[threadIdx.x]);
+        if (smax[threadIdx.x] >= 0) atomicMax(&info->max_row[threadIdx.x], smax[threadIdx.x]);
+    }
+}
+
+__global__ void k_diminfo_reset(DimInfo* info) {
+    int d = threadIdx.x;
+    if (d < kNumDims) { info->min_row[d] = INT_MAX; info->max_row[d] = -1; }
+}
+
+void init_passes(Device& D, cudaStream_t s) {
+    const int64_t n = D.n;
+    const unsigned g = grid_for(n, 256) > 65536 ? 65536 : grid_for(n, 256);
+    k_init_low<<<g, 256, 0, s>>>(n, D.arena, D.desc, D.low, D.leftmost, D.pivot, D.cleared, D.negative);
+    k_init_apparent<<<g, 256, 0, s>>>(n, D.arena, D.desc, D.low, D.leftmost, D.pivot, D.cleared, D.negative,
+                                      D.counters);
+}
+
+void init_compress(Device& D, const uint8_t* dropped, cudaStream_t s) {
+    const int64_t n = D.n;
+    const unsigned g = grid_for(n, 256) > 65536 ? 65536 : grid_for(n, 256);
+    k_init_compress<<<g, 256, 0, s>>>(n, D.arena, D.desc, D.low, D.pivot, D.cleared, D.negative, D.state, dropped,
+                                      D.counters, D.err);
+}
+
+// Active list in reordered order (dimension segments are contiguous) and the
+// per-dimension bounds.
+__global__ void k_act_segments(const int64_t* actpos, int64_t n, DimInfo* info) {
+    int d = threadIdx.x;
+    if (d < kNumDims) {
+        int32_t b = info->col_begin[d], e = info->col_end[d];
+        info->act_begin[d] = int32_t(b < n ? actpos[b] : actpos[n]);
+        info->act_end[d] = int32_t(e < n ? actpos[e] : actpos[n]);
+    }
+}
+
+void active_list(Device& D, cudaStream_t s) {
+    const int64_t n = D.n;
+    const uint8_t* state = D.state;
+    int32_t* act = D.active;
+    int64_t* pos = D.scratch64;
+    scan([=] __device__(int64_t i) -> int64_t { return state[i] == ST_ACTIVE ? 1 : 0; },
+         [=] __device__(int64_t i, int64_t pre, int64_t v) {
+             pos[i] = pre;
+             if (v) act[pre] = int32_t(i);
+         },
+         n, D.blk, s);
+    // pos[n] = total
+    cudaMemcpyAsync(pos + n, D.blk + scan_blocks(n), sizeof(int64_t), cudaMemcpyDeviceToDevice, s);
+    k_act_segments<<<1, 32, 0, s>>>(pos, n, D.diminfo);
+    k_diminfo_reset<<<1, 32, 0, s>>>(D.diminfo);
+    const unsigned g = grid_for(n, 256) > 4096 ? 4096 : grid_for(n, 256);
+    k_dim_rows<<<g, 256, 0, s>>>(n, D.dim, D.arena, D.desc, D.low, D.state, D.diminfo);
+}
+
+// ------------------------------------------------------------------- pairs
+// primal: row r (reordered) owned by column c -> (perm[r], perm[c]).
+// dual: the dual row r' owned by dual column c' maps back to the primal pair
+// (n-1-c', n-1-r') of the dualized matrix's own numbering; `dual_to_input`
+// then maps those primal reordered indices to input indices.
+__global__ void k_pairs_scatter(int64_t n, const int32_t* pivot, const int32_t* perm, int64_t* death_of,
+                                uint8_t* paired, int dual) {
+    for (int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; r < n; r += int64_t(gridDim.x) * blockDim.x) {
+        int32_t c = pivot[r];
+        if (c < 0) continue;
+        int64_t birth, death;
+        if (!dual) {
+            birth = perm[r];
+            death = perm[c];
+        } else {
+            birth = perm[n - 1 - c];
+            death = perm[n - 1 - r];
+        }
+        death_of[birth] = death;
+        paired[birth] = 1;
+        paired[death] = 1;
+    }
+}
+
+__global__ void k_mark_dropped(int64_t n, const uint8_t* dropped, const int32_t* perm, uint8_t* paired) {
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+        if (dropped[i]) paired[perm[i]] = 1;
+}
+
+void extract_pairs(Device& D, int dual, const uint8_t* dropped, cudaStream_t s) {
+    const int64_t n = D.n;
+    const unsigned g = grid_for(n, 256) > 65536 ? 65536 : grid_for(n, 256);
+    fill_i64(D.death_of, -1, n, s);
+    cudaMemsetAsync(D.negative, 0, n, s);  // reused as the "paired or dropped" mark
+    k_pairs_scatter<<<g, 256, 0, s>>>(n, D.pivot, D.perm, D.death_of, D.negative, dual);
+    if (dropped) k_mark_dropped<<<g, 256, 0, s>>>(n, dropped, D.perm, D.negative);
+    const int64_t* death_of = D.death_of;
+    int64_t* pairs = D.pairs;
+    scan([=] __device__(int64_t i) -> int64_t { return death_of[i] >= 0 ? 1 : 0; },
+         [=] __device__(int64_t i, int64_t pre, int64_t v) {
+             if (v) {
+                 pairs[2 * pre] = i;
+                 pairs[2 * pre + 1] = death_of[i];
+             }
+         },
+         n, D.blk, s);
+    cudaMemcpyAsync(&D.counters[CNT_NPAIRS], D.blk + scan_blocks(n), sizeof(int64_t), cudaMemcpyDeviceToDevice, s);
+    const uint8_t* paired = D.negative;
+    int64_t* ess = D.ess;
+    scan([=] __device__(int64_t i) -> int64_t { return paired[i] ? 0 : 1; },
+         [=] __device__(int64_t i, int64_t pre, int64_t v) {
+             if (v) ess[pre] = i;
+         },
+         n, D.blk, s);
+    cudaMemcpyAsync(&D.counters[CNT_NESS], D.blk + scan_blocks(n), sizeof(int64_t), cudaMemcpyDeviceToDevice, s);
+}
+
+}  // namespace sspp

@@ -1,0 +1,112 @@
+// Internal types shared by the engine's translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/sspp.h"
+
+namespace sspp {
+
+constexpr int kMaxDim = 7;          // dimensions 0..7 (the reference's MAXDIM is 5, include/bupt.h:48)
+constexpr int kNumDims = kMaxDim + 1;
+
+// Column states (one byte per column).
+enum : uint8_t {
+    ST_ACTIVE = 0,   // needs (more) reduction
+    ST_OWNER = 1,    // owns the pivot at its lowest row
+    ST_ZERO = 2,     // reduced to zero (positive) or empty input column
+    ST_CLEARED = 3,  // zeroed by clearing (positive), never reduced
+    ST_DROPPED = 4,  // removed by edge collapse
+};
+
+// A column is stored in the arena at a 16-byte aligned offset, padded with
+// INT32_MAX to a multiple of four ints.  Its descriptor packs
+// (offset in ints << 24) | length.
+constexpr int kLenBits = 24;
+constexpr uint64_t kLenMask = (1ull << kLenBits) - 1;
+constexpr int64_t kMaxColLen = int64_t(kLenMask);
+__host__ __device__ inline uint64_t pack_desc(uint64_t off, uint32_t len) { return (off << kLenBits) | len; }
+__host__ __device__ inline uint64_t desc_off(uint64_t d) { return d >> kLenBits; }
+__host__ __device__ inline uint32_t desc_len(uint64_t d) { return uint32_t(d & kLenMask); }
+__host__ __device__ inline int64_t pad4(int64_t x) { return (x + 3) & ~int64_t(3); }
+
+// Error word bits set by kernels (device int).
+enum : int {
+    ERRB_BAD_INPUT = 1,
+    ERRB_CAPACITY = 2,
+    ERRB_TIMEOUT = 4,
+    ERRB_LEN = 8,       // a column exceeded kMaxColLen
+};
+
+// Per-dimension summary after the init passes (in reordered numbering).
+struct DimInfo {
+    int32_t col_begin[kNumDims];   // reordered columns of dim d: [col_begin, col_end)
+    int32_t col_end[kNumDims];
+    int32_t act_begin[kNumDims];   // active list segment of dim d
+    int32_t act_end[kNumDims];
+    int32_t min_row[kNumDims];     // min first row over non-empty columns (DimMinRow)
+    int32_t max_row[kNumDims];     // max low + 1 over active columns (DimMaxRow)
+};
+
+// Device counters (int64 each), reset at the start of a run.
+enum CounterIdx {
+    CNT_ADDITIONS = 0,
+    CNT_ADD_INTS,
+    CNT_PUBLISHED,
+    CNT_DISPLACED,
+    CNT_APPARENT,
+    CNT_CLEARED,
+    CNT_HIGHCLEAR,
+    CNT_DROPPED,
+    CNT_ACTIVE,
+    CNT_NPAIRS,
+    CNT_NESS,
+    CNT_NUM
+};
+
+struct Device {
+    int64_t n = 0;        // columns
+    int64_t nnz = 0;
+    int64_t cap_n = 0;    // allocated column capacity
+    int64_t cap_nnz = 0;
+    // input in filtration order
+    int32_t* in_dims = nullptr;
+    int64_t* in_colptr = nullptr;
+    int32_t* in_rows = nullptr;
+    // reordered matrix
+    int32_t* dim = nullptr;      // reordered dims
+    int32_t* perm = nullptr;     // reordered -> input
+    int32_t* newidx = nullptr;   // input -> reordered
+    int64_t* scratch64 = nullptr;   // n+1 int64 (scans)
+    // arena of columns
+    int32_t* arena = nullptr;
+    int64_t arena_cap = 0;       // ints
+    unsigned long long* arena_top = nullptr;
+    uint64_t* desc = nullptr;
+    int32_t* low = nullptr;
+    int32_t* pivot = nullptr;
+    uint8_t* state = nullptr;
+    uint8_t* cleared = nullptr;
+    uint8_t* negative = nullptr;
+    int32_t* leftmost = nullptr;
+    int32_t* active = nullptr;
+    // block-scan scratch
+    int64_t* blk = nullptr;      // block sums
+    int64_t cap_blk = 0;
+    int32_t* dimcnt = nullptr;   // [nblocks * kNumDims]
+    int64_t cap_dimcnt = 0;
+    DimInfo* diminfo = nullptr;
+    int* err = nullptr;
+    long long* counters = nullptr;
+    int* step_ctr = nullptr;     // per-launch work counters
+    int64_t cap_steps = 0;
+    // pairs output (input indices)
+    int64_t* death_of = nullptr;   // [n]
+    int64_t* pairs = nullptr;      // [2n]
+    int64_t* ess = nullptr;        // [n]
+};
+
+}  // namespace sspp

@@ -1,0 +1,231 @@
+"""Python host mirror of the engine's C ABI (``include/sspp.h``).
+
+``SpecSeqPlusPlus`` keeps the reference's class interface
+(``include/specseq.h:486-512``: constructor with the matrix and the CLI
+parameters, ``GPU_Init``, ``GPU_Compute``, ``GetPersistencePairs``); ``Engine``
+is the lower-level context wrapper.  All computation happens in ``libsspp.so``
+on the GPU: if the library cannot be loaded this module raises, there is no
+CPU path.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, fields
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libsspp.so")
+
+OK, ERR_BAD_INPUT, ERR_CAPACITY, ERR_CUDA, ERR_TIMEOUT, ERR_STATE, ERR_IO = range(7)
+ASCII, BINARY = 0, 1
+_ERR_NAMES = {1: "BAD_INPUT", 2: "CAPACITY", 3: "CUDA", 4: "TIMEOUT", 5: "STATE", 6: "IO"}
+
+
+class SsppError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{_ERR_NAMES.get(code, code)}] {msg}")
+        self.code = code
+
+
+class _Config(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int32), ("arena_bytes", ctypes.c_int64), ("verbose", ctypes.c_int32)]
+
+
+class _Params(ctypes.Structure):
+    _fields_ = [("dualize", ctypes.c_int32), ("model", ctypes.c_int32), ("max_iteration", ctypes.c_int32),
+                ("ss_block_size", ctypes.c_int32), ("growth", ctypes.c_float), ("queue_size", ctypes.c_int32),
+                ("level1_capacity", ctypes.c_int32), ("level2_capacity", ctypes.c_int32),
+                ("autotune", ctypes.c_int32)]
+
+
+class _Stats(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_int64) for k in (
+        "ncols", "nnz", "active_after_init", "apparent_pairs", "cleared_init", "highclear_cleared",
+        "collapse_dropped", "additions", "add_ints", "published_ints", "displaced", "ss_steps", "npairs",
+        "nessential")] + [("init_ms", ctypes.c_double), ("compute_ms", ctypes.c_double)]
+
+
+@dataclass
+class Params:
+    """The reference's CLI parameters (src/main.cu:281-294, README.md:26-51)."""
+
+    dualize: int = 0
+    model: int = 0
+    max_iteration: int = 0
+    ss_block_size: int = 102400
+    growth: float = 1.05
+    queue_size: int = 65536
+    level1_capacity: int = 1000
+    level2_capacity: int = 8000
+    autotune: int = 0
+
+    def _c(self) -> _Params:
+        return _Params(*(getattr(self, f.name) for f in fields(self)))
+
+
+_lib = None
+
+
+def load_library():
+    """Loads libsspp.so; raises if it is missing (no fallback path exists)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with __graft_entry__.build()")
+    lib = ctypes.CDLL(LIB_PATH)
+    vp, i32, i64 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64
+    sig = {
+        "sspp_create": (vp, [ctypes.POINTER(_Config)]),
+        "sspp_destroy": (None, [vp]),
+        "sspp_last_error": (ctypes.c_char_p, [vp]),
+        "sspp_default_params": (None, [ctypes.POINTER(_Params)]),
+        "sspp_load_phat": (i32, [vp, ctypes.c_char_p, i32]),
+        "sspp_load_csc": (i32, [vp, i64, vp, vp, vp]),
+        "sspp_load_csc_device": (i32, [vp, i64, vp, vp, vp]),
+        "sspp_init": (i32, [vp, ctypes.POINTER(_Params), vp]),
+        "sspp_compute": (i32, [vp, vp]),
+        "sspp_reduce": (i32, [vp, ctypes.POINTER(_Params), vp]),
+        "sspp_num_pairs": (i64, [vp]),
+        "sspp_pairs": (i64, [vp, vp, i64]),
+        "sspp_num_essential": (i64, [vp]),
+        "sspp_essentials": (i64, [vp, vp, i64]),
+        "sspp_write_pairs": (i32, [vp, ctypes.c_char_p, i32]),
+        "sspp_get_stats": (i32, [vp, ctypes.POINTER(_Stats)]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+EXPORTED = ("sspp_create", "sspp_destroy", "sspp_last_error", "sspp_default_params", "sspp_load_phat",
+            "sspp_load_csc", "sspp_load_csc_device", "sspp_init", "sspp_compute", "sspp_reduce", "sspp_num_pairs",
+            "sspp_pairs", "sspp_num_essential", "sspp_essentials", "sspp_write_pairs", "sspp_get_stats")
+
+
+class Engine:
+    """One device context (include/sspp.h)."""
+
+    def __init__(self, device: int = 0, arena_bytes: int = 0, verbose: int = 0):
+        self._lib = load_library()
+        cfg = _Config(device, arena_bytes, verbose)
+        self._h = self._lib.sspp_create(ctypes.byref(cfg))
+        if not self._h:
+            raise SsppError(ERR_CUDA, "sspp_create failed (no usable CUDA device?)")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.sspp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, rc: int):
+        if rc != OK:
+            raise SsppError(rc, self._lib.sspp_last_error(self._h).decode(errors="replace"))
+
+    def load_csc(self, m) -> None:
+        dims = np.ascontiguousarray(m.dims, dtype=np.int32)
+        col_ptr = np.ascontiguousarray(m.col_ptr, dtype=np.int64)
+        rows = np.ascontiguousarray(m.rows, dtype=np.int32)
+        self._check(self._lib.sspp_load_csc(self._h, dims.shape[0], dims.ctypes.data, col_ptr.ctypes.data,
+                                            rows.ctypes.data))
+
+    def load_csc_device(self, ncols: int, d_dims: int, d_col_ptr: int, d_rows: int) -> None:
+        self._check(self._lib.sspp_load_csc_device(self._h, ncols, d_dims, d_col_ptr, d_rows))
+
+    def load_phat(self, path: str, fmt: int = ASCII) -> None:
+        self._check(self._lib.sspp_load_phat(self._h, path.encode(), fmt))
+
+    def init(self, params: Params | None = None, stream: int = 0) -> None:
+        p = (params or Params())._c()
+        self._check(self._lib.sspp_init(self._h, ctypes.byref(p), stream or None))
+
+    def compute(self, stream: int = 0) -> None:
+        self._check(self._lib.sspp_compute(self._h, stream or None))
+
+    def reduce(self, params: Params | None = None, stream: int = 0) -> None:
+        p = (params or Params())._c()
+        self._check(self._lib.sspp_reduce(self._h, ctypes.byref(p), stream or None))
+
+    def pairs(self) -> np.ndarray:
+        n = self._lib.sspp_num_pairs(self._h)
+        if n < 0:
+            self._check(ERR_STATE)
+        out = np.empty((n, 2), dtype=np.int64)
+        got = self._lib.sspp_pairs(self._h, out.ctypes.data, n)
+        if got != n:
+            self._check(ERR_CUDA)
+        return out
+
+    def essentials(self) -> np.ndarray:
+        n = self._lib.sspp_num_essential(self._h)
+        if n < 0:
+            self._check(ERR_STATE)
+        out = np.empty(n, dtype=np.int64)
+        got = self._lib.sspp_essentials(self._h, out.ctypes.data, n)
+        if got != n:
+            self._check(ERR_CUDA)
+        return out
+
+    def write_pairs(self, path: str, fmt: int = ASCII) -> None:
+        self._check(self._lib.sspp_write_pairs(self._h, path.encode(), fmt))
+
+    def stats(self) -> dict:
+        st = _Stats()
+        self._check(self._lib.sspp_get_stats(self._h, ctypes.byref(st)))
+        return {k: getattr(st, k) for k, _ in _Stats._fields_}
+
+
+def compute_persistence_pairs(m, params: Params | None = None, device: int = 0):
+    """Sorted (birth, death) pairs and essential simplices of a boundary matrix."""
+    with Engine(device) as e:
+        e.load_csc(m)
+        e.reduce(params)
+        return e.pairs(), e.essentials()
+
+
+class SpecSeqPlusPlus:
+    """Mirror of the reference's host class (include/specseq.h:486-512, 513, 592, 1182).
+
+    ``level_capacity`` is the reference's 4-entry array whose entries 1 and 2 are
+    the CLI's level-1/level-2 capacities (src/main.cu:292-294).
+    """
+
+    def __init__(self, matrix, level_capacity, dualize, model, highclear_maxneighbors, ss_block_size,
+                 block_size_growth_rate, queue_size, device: int = 0):
+        self.params = Params(dualize=int(dualize), model=int(model), max_iteration=int(highclear_maxneighbors),
+                             ss_block_size=int(ss_block_size), growth=float(block_size_growth_rate),
+                             queue_size=int(queue_size), level1_capacity=int(level_capacity[1]),
+                             level2_capacity=int(level_capacity[2]))
+        self._e = Engine(device)
+        self._e.load_csc(matrix)
+
+    def GPU_Init(self) -> float:
+        self._e.init(self.params)
+        return self._e.stats()["init_ms"] / 1000.0
+
+    def GPU_Compute(self) -> float:
+        self._e.compute()
+        return self._e.stats()["compute_ms"] / 1000.0
+
+    def GetPersistencePairs(self) -> np.ndarray:
+        return self._e.pairs()
+
+    def GetEssentials(self) -> np.ndarray:
+        return self._e.essentials()
+
+    def stats(self) -> dict:
+        return self._e.stats()

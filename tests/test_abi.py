@@ -1,0 +1,57 @@
+"""CPU checks of the drop-in boundary: the C-ABI library loads and exports
+every symbol include/sspp.h declares; the command line keeps the reference's
+argument handling (src/main.cu:269-321)."""
+import ctypes
+import os
+import re
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB = os.path.join(ROOT, "specseqplusplus_b200", "libsspp.so")
+CLI = os.path.join(ROOT, "specseqplusplus_b200", "bin", "specseq++")
+
+
+def declared(header):
+    text = open(os.path.join(ROOT, "include", header)).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(sspp_[a-z_0-9]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    assert os.path.exists(LIB), "run __graft_entry__.build() first"
+    lib = ctypes.CDLL(LIB)
+    names = declared("sspp.h")
+    assert len(names) >= 16
+    for name in names:
+        assert hasattr(lib, name), name
+
+
+def test_python_mirror_binds_every_symbol():
+    from specseqplusplus_b200 import engine
+
+    assert set(declared("sspp.h")) <= set(engine.EXPORTED) | {"sspp_default_params"}
+
+
+def test_cli_help_and_argument_errors(tmp_path):
+    assert os.path.exists(CLI)
+    r = subprocess.run([CLI, "-help"], capture_output=True, text=True)
+    assert r.returncode == 0 and "Usage" in r.stdout
+    r = subprocess.run([CLI, "a", "b"], capture_output=True, text=True)
+    assert r.returncode == 1 and "Invalid number of arguments" in r.stderr
+    args = ["in", "out", "text", "ascii", "0", "0", "0", "100", "1.05", "64", "100", "200"]
+    r = subprocess.run([CLI] + args, capture_output=True, text=True)
+    assert r.returncode == 1 and "Invalid input format" in r.stderr
+    args[2], args[3] = "ascii", "xml"
+    r = subprocess.run([CLI] + args, capture_output=True, text=True)
+    assert r.returncode == 1 and "Invalid output format" in r.stderr
+
+
+def test_no_oracle_on_product_path():
+    # the product never imports, links or runs the oracle
+    for dirpath, _, files in os.walk(os.path.join(ROOT, "specseqplusplus_b200")):
+        for f in files:
+            if f.endswith((".py", ".cu", ".cpp", ".h", ".cuh")):
+                text = open(os.path.join(dirpath, f)).read()
+                assert "import oracle" not in text and "liboracle" not in text, f
