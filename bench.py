@@ -1,0 +1,315 @@
+#!/usr/bin/env python
+"""Benchmark: reduced columns/s of the engine on the 64^3 lower-star workload.
+
+Workload (one "step" = one full reduction, init passes to sorted pairs): the
+lower-star filtration of the Freudenthal triangulation of a 64^3 grid (all
+vertices, edges, triangles and tetrahedra: 6,573,043 columns, 18,646,740
+non-zeros) whose vertex values are seeded Gaussian white noise smoothed by a
+Gaussian of sigma = 2 voxels (float32); ties broken by dimension then
+lexicographic vertex order; int32 indices; model 1 (high-dimension guided
+clearing, max_iteration 10), ss_block_size 102400, growth 1.05.  Synthetic,
+seeded data stands in for the reference's input files.
+
+  value  = columns / device time with the matrix already resident in HBM
+           (CUDA events on the launching stream, L2 flushed between steps)
+  e2e    = the same metric through the C ABI from pinned host buffers,
+           host->device copy of the matrix and device->host copy of the pairs
+           and essential classes inside the timed region
+  --impl reference: the CPU restatement of the reference's reduction (the
+           reference's own CPU path, phat-highclear, cannot be built: its PHAT
+           library headers are not part of the reference tree), timed on the
+           host on the same workload.
+
+Multi-GPU: one process per GPU (torchrun); a single reduction does not shard,
+so every rank reduces its own replica of the workload (request-level weak
+scaling, no collective on the data path); value = total columns / max time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+GRID, SIGMA, SEED = 64, 2.0, 2
+MODEL, MAX_ITER, SS, GROWTH, QUEUE, L1, L2 = 1, 10, 102400, 1.05, 65536, 64, 8192
+METRIC, UNIT = "reduced_columns_per_s", "columns/s"
+
+
+def workload_config(n, nnz):
+    return {"workload": f"lower-star Freudenthal {GRID}^3, sigma {SIGMA}, model {MODEL}, max_iteration {MAX_ITER}, "
+                        f"ss_block_size {SS}, growth {GROWTH}",
+            "ncols": n, "nnz": nnz, "grid": GRID, "sigma": SIGMA, "seed": SEED, "model": MODEL,
+            "max_iteration": MAX_ITER, "ss_block_size": SS, "growth": GROWTH, "queue_size": QUEUE,
+            "level1_capacity": L1, "level2_capacity": L2, "dualize": 0, "index": "int32", "values": "float32",
+            "l2": "flushed between steps (256 MiB write); inputs (149 MB) also exceed L2"}
+
+
+def dist_info():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+class Clocks:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    def __init__(self, device):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(device), f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.f.name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def load_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))), "measured"
+    except (OSError, ValueError):
+        return {"hbm_gbs": 6650.0}, "fallback"
+
+
+def load_traffic():
+    try:
+        return json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
+    except (OSError, ValueError):
+        return {}
+
+
+def oracle_run(m):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    t = time.perf_counter()
+    r = oracle.reduce(m, model=MODEL, max_iteration=MAX_ITER)
+    return time.perf_counter() - t, r
+
+
+def reference_arm(args):
+    rank, world, _ = dist_info()
+    if rank != 0:
+        return 0
+    from specseqplusplus_b200 import gen
+
+    m = gen.lowerstar(GRID, SIGMA, SEED)
+    for _ in range(args.warmup):
+        oracle_run(m)
+    times = []
+    for _ in range(args.steps):
+        dt, r = oracle_run(m)
+        times.append(dt)
+    total = sum(times)
+    value = m.ncols * len(times) / total
+    sample = f"full workload ({m.ncols} columns) per step, single-threaded C++ restatement (oracle/sspp_oracle.cpp)"
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / len(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+            "config": workload_config(m.ncols, m.nnz),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return reference_arm(args)
+
+    import numpy as np
+    import torch
+
+    from specseqplusplus_b200 import Engine, Params, gen
+
+    rank, world, local = dist_info()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    m = gen.lowerstar(GRID, SIGMA, SEED)
+    n, nnz = m.ncols, m.nnz
+    p = Params(model=MODEL, max_iteration=MAX_ITER, ss_block_size=SS, growth=GROWTH, queue_size=QUEUE,
+               level1_capacity=L1, level2_capacity=L2)
+    dev = torch.device("cuda", local)
+    d_dims = torch.from_numpy(m.dims).to(dev)
+    d_colptr = torch.from_numpy(m.col_ptr).to(dev)
+    d_rows = torch.from_numpy(m.rows).to(dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sh = stream.cuda_stream
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # ---------------------------------------------------------- device-resident
+    eng = Engine(local, profile=1)
+    eng.load_csc_device(n, d_dims.data_ptr(), d_colptr.data_ptr(), d_rows.data_ptr())
+    for _ in range(args.warmup):
+        eng.reduce(p, stream=sh)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = Clocks(local)
+    per_step, phases, launches = [], {"init_gpu_ms": 0.0, "light_gpu_ms": 0.0, "heavy_gpu_ms": 0.0,
+                                      "pairs_gpu_ms": 0.0}, 0
+    light_launches = heavy_launches = 0
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        eng.reduce(p, stream=sh)
+        b.record(stream)
+        torch.cuda.synchronize()
+        per_step.append(a.elapsed_time(b))
+        st = eng.stats()
+        for k in phases:
+            phases[k] += st[k]
+        launches += st["launches"]
+        light_launches += st["light_launches"]
+        heavy_launches += st["heavy_launches"]
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    total_ms = sum(per_step)
+    st = eng.stats()
+    dev_pairs = eng.pairs()
+    dev_ess = eng.essentials()
+    eng.close()
+
+    # ---------------------------------------------------------------- e2e
+    h_dims = torch.from_numpy(m.dims).pin_memory()
+    h_colptr = torch.from_numpy(m.col_ptr).pin_memory()
+    h_rows = torch.from_numpy(m.rows).pin_memory()
+    out_pairs = torch.empty(2 * n, dtype=torch.int64).pin_memory()
+    out_ess = torch.empty(n, dtype=torch.int64).pin_memory()
+    hm = gen.BoundaryMatrix(h_dims.numpy(), h_colptr.numpy(), h_rows.numpy())
+    e2 = Engine(local)
+    for _ in range(max(1, args.warmup)):
+        e2.load_csc(hm)
+        e2.reduce(p)
+        e2.pairs(out_pairs.numpy())
+        e2.essentials(out_ess.numpy())
+    barrier()
+    e2e_ms = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e2.load_csc(hm)
+        e2.reduce(p)
+        pr = e2.pairs(out_pairs.numpy())
+        es = e2.essentials(out_ess.numpy())
+        e2e_ms.append(1000 * (time.perf_counter() - t0))
+    h2d = 4 * n + 8 * (n + 1) + 4 * nnz
+    d2h = 16 * len(pr) + 8 * len(es)
+    ok_e2e = np.array_equal(pr, dev_pairs) and np.array_equal(es, dev_ess)
+    e2.close()
+
+    # --------------------------------------------------------- max over ranks
+    tot = torch.tensor([total_ms, sum(e2e_ms)], dtype=torch.float64, device=dev)
+    if dist is not None:
+        dist.all_reduce(tot, op=dist.ReduceOp.MAX)
+    total_ms, e2e_total = float(tot[0]), float(tot[1])
+    if dist is not None:
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+
+    value = world * n * args.steps / (total_ms / 1000)
+    e2e_value = world * n * args.steps / (e2e_total / 1000)
+
+    # roofline of the dominant device phase (algorithmic bytes per step)
+    peaks, peak_kind = load_peaks()
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    cpu = None
+    alg_add_bytes = None
+    if not args.no_cpu_baseline:
+        dt, r = oracle_run(m)
+        alg_add_bytes = r.stats["add_bytes"]
+        assert np.array_equal(dev_pairs, r.pairs) and np.array_equal(dev_ess, r.essential), "parity failure"
+        cpu = {"value": n / dt, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": f"full workload ({n} columns), one run, single-threaded C++ restatement"}
+    ph = {k: v / args.steps for k, v in phases.items()}
+    init_bytes = 16 * nnz + 8 * n           # CSC read three times and written once, pivot + low tables
+    red_ms = ph["light_gpu_ms"] + ph["heavy_gpu_ms"]
+    candidates = {"init_passes": (ph["init_gpu_ms"], init_bytes),
+                  "reduction": (red_ms, alg_add_bytes if alg_add_bytes is not None else None)}
+    dom = max(candidates, key=lambda k: candidates[k][0])
+    dom_ms, dom_bytes = candidates[dom]
+    traffic = load_traffic().get(dom)
+    roof = None
+    if dom_bytes is not None and dom_ms > 0:
+        achieved = dom_bytes / (dom_ms / 1000) / 1e9
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "kernel": dom, "peak_kind": peak_kind,
+                "algorithmic_bytes_per_step": dom_bytes, "device_ms_per_step": dom_ms}
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+            "config": workload_config(n, nnz),
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "ms_per_step": e2e_total / args.steps, "pairs_match_device_run": bool(ok_e2e)},
+            "gpu_launches": launches,
+            "phases_ms_per_step": ph,
+            "launches_per_step": {"total": launches // args.steps, "light": light_launches // args.steps,
+                                  "heavy": heavy_launches // args.steps},
+            "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
+            "stats": {k: st[k] for k in ("active_after_init", "apparent_pairs", "cleared_init", "highclear_cleared",
+                                         "additions", "displaced", "ss_steps", "npairs", "nessential")}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

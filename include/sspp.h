@@ -39,6 +39,7 @@ typedef struct sspp_config {
     int32_t device;          /* CUDA device ordinal                                  */
     int64_t arena_bytes;     /* initial column arena; 0 = sized from the input       */
     int32_t verbose;         /* 0 = silent                                           */
+    int32_t profile;         /* 1 = time every device phase with CUDA events         */
 } sspp_config;
 
 /* The reference's 12 positional CLI values (src/main.cu:281-294) minus file
@@ -72,6 +73,11 @@ typedef struct sspp_stats {
     int64_t ss_steps;            /* spectral-sequence launches                     */
     int64_t npairs, nessential;
     double init_ms, compute_ms;  /* GPU_Init / GPU_Compute equivalents            */
+    int64_t launches;            /* kernels launched by the last init + compute    */
+    /* device time per phase (profile = 1 only): init passes, light-tier and
+     * heavy-tier reduction launches, pair extraction */
+    double init_gpu_ms, light_gpu_ms, heavy_gpu_ms, pairs_gpu_ms;
+    int64_t light_launches, heavy_launches;
 } sspp_stats;
 
 /* Replaces: the SpecSeqPlusPlus constructor's allocation (include/specseq.h:486-512). */
@@ -95,7 +101,9 @@ int32_t sspp_load_phat(sspp_ctx* ctx, const char* path, int32_t fmt);
  * face indices ascending and unique.  Copied to the device at once. */
 int32_t sspp_load_csc(sspp_ctx* ctx, int64_t ncols, const int32_t* dims, const int64_t* col_ptr, const int32_t* rows);
 
-/* Same, for arrays already resident in device memory (no host copy). */
+/* Same, for arrays already resident in device memory: nothing is copied, the
+ * context reads them in place, so they must stay valid and unmodified until
+ * the next load or sspp_destroy.  Validated on the device. */
 int32_t sspp_load_csc_device(sspp_ctx* ctx, int64_t ncols, const int32_t* d_dims, const int64_t* d_col_ptr,
                              const int32_t* d_rows);
 

@@ -18,11 +18,38 @@
 #include <type_traits>
 #include <vector>
 
+#include "sspp_highclear.h"
 #include "sspp_internal.h"
 #include "sspp_io.h"
 #include "sspp_launch.h"
 
 using namespace sspp;
+
+namespace {
+enum Phase { PH_INIT = 0, PH_LIGHT, PH_HEAVY, PH_PAIRS, PH_NUM };
+
+// CUDA-event spans per phase (only recorded when the context profiles).
+struct Prof {
+    std::vector<cudaEvent_t> pool;
+    size_t used = 0;
+    struct Span { int phase; cudaEvent_t a, b; };
+    std::vector<Span> spans;
+    void reset() { used = 0; spans.clear(); }
+    cudaEvent_t get() {
+        if (used == pool.size()) {
+            cudaEvent_t e;
+            cudaEventCreate(&e);
+            pool.push_back(e);
+        }
+        return pool[used++];
+    }
+    void release() {
+        for (auto e : pool) cudaEventDestroy(e);
+        pool.clear();
+        reset();
+    }
+};
+}  // namespace
 
 struct sspp_ctx {
     sspp_config cfg{};
@@ -35,8 +62,9 @@ struct sspp_ctx {
     DimInfo hinfo{};
     long long hcounters[CNT_NUM] = {};
     int num_sms = 0;
-    int blocks_per_sm = 0;
-    int configured_cap = -1;
+    int light_blocks_per_sm = 0;
+    int heavy_blocks_per_sm = 0;
+    int configured_cap1 = -1, configured_cap2 = -1;
     int64_t arena_request = 0;     // ints requested for the arena (grows on CAPACITY)
     double init_ms = 0, compute_ms = 0;
     int64_t ss_steps = 0;
@@ -46,6 +74,15 @@ struct sspp_ctx {
     unsigned long long* h_top = nullptr;
     uint8_t* dropped = nullptr;    // primal reordered numbering (model bit 2)
     int64_t cap_dropped = 0;
+    // input buffers owned by the context (host loads); device loads are read in place
+    int32_t* own_dims = nullptr;
+    int64_t* own_colptr = nullptr;
+    int32_t* own_rows = nullptr;
+    int64_t cap_own_n = 0, cap_own_nnz = 0;
+    HighclearScratch hc;
+    Prof prof;
+    double ph_ms[PH_NUM] = {};
+    int64_t launches = 0, light_launches = 0, heavy_launches = 0;
 };
 
 namespace {
@@ -75,9 +112,9 @@ cudaError_t grow(T*& p, int64_t& cap, int64_t want) {
 }
 
 void free_device(Device& D) {
-    void* ptrs[] = {D.in_dims, D.in_colptr, D.in_rows, D.dim, D.perm, D.newidx, D.scratch64, D.arena, D.arena_top,
+    void* ptrs[] = {D.dim, D.perm, D.newidx, D.scratch64, D.arena, D.arena_top,
                     D.desc, D.low, D.pivot, D.state, D.cleared, D.negative, D.leftmost, D.active, D.blk, D.dimcnt,
-                    D.diminfo, D.err, D.counters, D.step_ctr, D.death_of, D.pairs, D.ess};
+                    D.diminfo, D.err, D.counters, D.step_ctr, D.heavy, D.death_of, D.pairs, D.ess};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     D = Device();
@@ -95,8 +132,6 @@ int ensure_columns(sspp_ctx* ctx, int64_t n, int64_t nnz) {
             if (p) { cudaFree(p); p = nullptr; }
             return grow<T>(p, cap, c * mult + 1);
         };
-        CK(g(D.in_dims, 1));
-        CK(g(D.in_colptr, 1));
         CK(g(D.dim, 1));
         CK(g(D.perm, 1));
         CK(g(D.newidx, 1));
@@ -109,6 +144,7 @@ int ensure_columns(sspp_ctx* ctx, int64_t n, int64_t nnz) {
         CK(g(D.negative, 1));
         CK(g(D.leftmost, 1));
         CK(g(D.active, 1));
+        CK(g(D.heavy, 1));
         CK(g(D.death_of, 1));
         CK(g(D.pairs, 2));
         CK(g(D.ess, 1));
@@ -117,13 +153,6 @@ int ensure_columns(sspp_ctx* ctx, int64_t n, int64_t nnz) {
         CK(grow(D.blk, D.cap_blk, nb));
         int64_t nbp = (c + 255) / 256 + 1;
         CK(grow(D.dimcnt, D.cap_dimcnt, nbp * kNumDims));
-    }
-    if (nnz > D.cap_nnz) {
-        if (D.in_rows) cudaFree(D.in_rows);
-        D.in_rows = nullptr;
-        int64_t cap = 0;
-        CK(grow(D.in_rows, cap, nnz));
-        D.cap_nnz = nnz;
     }
     if (!D.diminfo) {
         CK(cudaMalloc(&D.diminfo, sizeof(DimInfo)));
@@ -193,34 +222,110 @@ int check_params(sspp_ctx* ctx, const sspp_params* p) {
     if (p->level1_capacity < 0 || p->level2_capacity < 0)
         return set_err(ctx, SSPP_ERR_BAD_INPUT, "level capacities must be >= 0");
     if (p->dualize) return set_err(ctx, SSPP_ERR_BAD_INPUT, "dualize is not available in this build");
-    if (p->model & 3) return set_err(ctx, SSPP_ERR_BAD_INPUT, "model bits are not available in this build");
+    if (p->model & 2) return set_err(ctx, SSPP_ERR_BAD_INPUT, "edge collapse is not available in this build");
     return SSPP_OK;
 }
 
+// Shared-memory capacities (ints) of the two tiers: a warp holds three
+// buffers of level1 ints, a CTA three of level2 ints.
 int level1_cap(const sspp_params& p) {
-    int c = std::max(64, p.level1_capacity);
+    int c = std::max(32, p.level1_capacity);
     c = std::min(c, 4096);
     return (c + 31) & ~31;
+}
+int level2_cap(const sspp_params& p) {
+    int c = std::max(level1_cap(p), p.level2_capacity);
+    c = std::min(c, 18432);
+    return (c + 31) & ~31;
+}
+
+void span_begin(sspp_ctx* ctx, cudaEvent_t& a) {
+    if (ctx->cfg.profile) {
+        a = ctx->prof.get();
+        cudaEventRecord(a, ctx->stream);
+    }
+}
+void span_end(sspp_ctx* ctx, int phase, cudaEvent_t a) {
+    if (ctx->cfg.profile) {
+        cudaEvent_t b = ctx->prof.get();
+        cudaEventRecord(b, ctx->stream);
+        ctx->prof.spans.push_back({phase, a, b});
+    }
+}
+// after a stream synchronisation: fold the recorded spans into ph_ms
+void span_collect(sspp_ctx* ctx) {
+    for (auto& sp : ctx->prof.spans) {
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, sp.a, sp.b) == cudaSuccess) ctx->ph_ms[sp.phase] += ms;
+    }
+    ctx->prof.reset();
+}
+
+// Sizes the guided-clearing scratch from the per-dimension column ranges and
+// runs it (needs one host read of the ranges).
+int run_highclear(sspp_ctx* ctx) {
+    Device& D = ctx->D;
+    cudaStream_t s = ctx->stream;
+    CK(cudaMemcpyAsync(ctx->h_info, D.diminfo, sizeof(DimInfo), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    const DimInfo info = *ctx->h_info;
+    HighclearScratch& S = ctx->hc;
+    int top = -1;
+    for (int d = kMaxDim; d >= 1; d--)
+        if (info.col_end[d] > info.col_begin[d]) { top = d; break; }
+    if (top < 1) return SSPP_OK;
+    for (int d = 1; d <= top; d++)
+        CK(grow(S.tup[d], S.cap_tup[d], int64_t(d + 1) * (info.col_end[d] - info.col_begin[d]) + 1));
+    const int64_t nv = info.col_end[0] - info.col_begin[0];
+    const int64_t ne = info.col_end[1] - info.col_begin[1];
+    CK(grow(S.deg, S.cap_deg, nv + 2));
+    CK(grow(S.adj_off, S.cap_adj_off, nv + 2));
+    CK(grow(S.adj, S.cap_adj, 2 * ne + 1));
+    const int64_t ntop = info.col_end[top] - info.col_begin[top];
+    int64_t slots = 1024;
+    while (slots < 2 * ntop) slots *= 2;
+    CK(grow(S.table, S.cap_table, slots));
+    S.mask = uint32_t(slots - 1);
+    ctx->launches += highclear(D, info, ctx->params.max_iteration, nullptr, S, s);
+    return SSPP_OK;
 }
 
 int run_init(sspp_ctx* ctx) {
     Device& D = ctx->D;
     cudaStream_t s = ctx->stream;
     auto t0 = std::chrono::steady_clock::now();
+    ctx->prof.reset();
+    for (double& x : ctx->ph_ms) x = 0;
+    ctx->launches = ctx->light_launches = ctx->heavy_launches = 0;
     CK(cudaMemsetAsync(D.err, 0, sizeof(int), s));
     CK(cudaMemsetAsync(D.counters, 0, sizeof(long long) * CNT_NUM, s));
     int rc = ensure_arena(ctx, arena_need(ctx));
     if (rc) return rc;
-    validate(D, s);
+    if (D.n == 0) {  // nothing to reduce
+        std::memset(&ctx->hinfo, 0, sizeof(ctx->hinfo));
+        std::memset(ctx->hcounters, 0, sizeof(ctx->hcounters));
+        ctx->init_ms = 0;
+        ctx->inited = true;
+        ctx->computed = false;
+        return SSPP_OK;
+    }
+    cudaEvent_t ev0 = nullptr;
+    span_begin(ctx, ev0);
+    ctx->launches += validate(D, s);
     CK(cudaMemcpyAsync(ctx->h_err, D.err, sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     if (*ctx->h_err) return set_err(ctx, SSPP_ERR_BAD_INPUT, "dimension out of range 0..7 or malformed col_ptr");
-    reorder(D, s);
+    ctx->launches += reorder(D, s);
     CK(cudaMemcpyAsync(D.arena_top, D.blk + reorder_total_slot(D), sizeof(unsigned long long),
                        cudaMemcpyDeviceToDevice, s));
-    init_passes(D, s);
-    init_compress(D, nullptr, s);
-    active_list(D, s);
+    ctx->launches += init_passes(D, s);
+    if ((ctx->params.model & 1) && ctx->params.max_iteration > 0) {
+        int rc2 = run_highclear(ctx);
+        if (rc2) return rc2;
+    }
+    ctx->launches += init_compress(D, nullptr, s);
+    ctx->launches += active_list(D, s);
+    span_end(ctx, PH_INIT, ev0);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(ctx->h_info, D.diminfo, sizeof(DimInfo), cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(ctx->h_err, D.err, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -229,6 +334,7 @@ int run_init(sspp_ctx* ctx) {
     ctx->hinfo = *ctx->h_info;
     std::memcpy(ctx->hcounters, ctx->h_counters, sizeof(ctx->hcounters));
     ctx->init_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    span_collect(ctx);
     if (*ctx->h_err & ERRB_BAD_INPUT)
         return set_err(ctx, SSPP_ERR_BAD_INPUT,
                        "malformed boundary matrix (a face index out of range, unsorted, duplicated, or of the "
@@ -244,46 +350,66 @@ int run_compute(sspp_ctx* ctx) {
     Device& D = ctx->D;
     cudaStream_t s = ctx->stream;
     auto t0 = std::chrono::steady_clock::now();
+    if (D.n == 0) {
+        std::memset(ctx->hcounters, 0, sizeof(ctx->hcounters));
+        ctx->compute_ms = 0;
+        ctx->ss_steps = 0;
+        ctx->computed = true;
+        return SSPP_OK;
+    }
     const sspp_params& P = ctx->params;
-    const int cap = level1_cap(P);
-    if (cap != ctx->configured_cap) {
-        CK(reduce_configure(cap, &ctx->blocks_per_sm));
-        ctx->configured_cap = cap;
-        if (ctx->blocks_per_sm < 1) return set_err(ctx, SSPP_ERR_CAPACITY, "level1 capacity too large for shared memory");
+    const int cap1 = level1_cap(P), cap2 = level2_cap(P);
+    if (cap1 != ctx->configured_cap1 || cap2 != ctx->configured_cap2) {
+        CK(reduce_configure(cap1, cap2, &ctx->light_blocks_per_sm, &ctx->heavy_blocks_per_sm));
+        ctx->configured_cap1 = cap1;
+        ctx->configured_cap2 = cap2;
+        if (ctx->light_blocks_per_sm < 1 || ctx->heavy_blocks_per_sm < 1)
+            return set_err(ctx, SSPP_ERR_CAPACITY, "level capacities too large for shared memory");
     }
     // schedule (dimensions high to low)
     std::vector<Step> steps;
-    std::vector<int> step_dim;
     const DimInfo& I = ctx->hinfo;
-    for (int d = kMaxDim; d >= 1; d--) {
-        size_t before = steps.size();
+    for (int d = kMaxDim; d >= 1; d--)
         ss_schedule(P, I.act_begin[d], I.act_end[d], I.min_row[d] == INT_MAX ? 0 : I.min_row[d], I.max_row[d], steps);
-        for (size_t k = before; k < steps.size(); k++) step_dim.push_back(d);
-    }
-    if (int64_t(steps.size()) > D.cap_steps) {
+    if (3 * int64_t(steps.size()) > D.cap_steps) {
         if (D.step_ctr) cudaFree(D.step_ctr);
         D.step_ctr = nullptr;
         D.cap_steps = 0;
-        CK(grow(D.step_ctr, D.cap_steps, int64_t(steps.size()) + 64));
+        CK(grow(D.step_ctr, D.cap_steps, 3 * int64_t(steps.size()) + 64));
     }
-    if (!steps.empty()) CK(cudaMemsetAsync(D.step_ctr, 0, sizeof(int) * steps.size(), s));
-    const int max_blocks = std::max(1, ctx->num_sms * ctx->blocks_per_sm);
+    if (!steps.empty()) CK(cudaMemsetAsync(D.step_ctr, 0, sizeof(int) * 3 * steps.size(), s));
+    const int light_max = std::max(1, ctx->num_sms * ctx->light_blocks_per_sm);
+    const int heavy_grid = std::max(1, ctx->num_sms * ctx->heavy_blocks_per_sm);
     const int q_blocks = std::max(1, (P.queue_size + 3) / 4);
     for (size_t k = 0; k < steps.size(); k++) {
         const Step& st = steps[k];
         int64_t chunks = (int64_t(st.end - st.beg) + 31) / 32;
-        int grid = int(std::min<int64_t>(std::min<int64_t>((chunks + 3) / 4, max_blocks), q_blocks));
+        int grid = int(std::min<int64_t>(std::min<int64_t>((chunks + 3) / 4, light_max), q_blocks));
         grid = std::max(grid, 1);
-        reduce_launch(D, D.active, st.beg, st.end, st.minrow, cap, D.step_ctr + k, grid, s);
+        int* ctr = D.step_ctr + 3 * k;
+        cudaEvent_t a = nullptr, b = nullptr;
+        span_begin(ctx, a);
+        reduce_light_launch(D, D.active, st.beg, st.end, st.minrow, cap1, ctr, grid, s);
+        span_end(ctx, PH_LIGHT, a);
+        span_begin(ctx, b);
+        reduce_heavy_launch(D, st.minrow, cap2, ctr, heavy_grid, s);
+        span_end(ctx, PH_HEAVY, b);
+        ctx->light_launches++;
+        ctx->heavy_launches++;
+        ctx->launches += 2;
     }
     ctx->ss_steps = int64_t(steps.size());
-    extract_pairs(D, 0, nullptr, s);
+    cudaEvent_t ep = nullptr;
+    span_begin(ctx, ep);
+    ctx->launches += extract_pairs(D, 0, nullptr, s);
+    span_end(ctx, PH_PAIRS, ep);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(ctx->h_err, D.err, sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(ctx->h_counters, D.counters, sizeof(long long) * CNT_NUM, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     std::memcpy(ctx->hcounters, ctx->h_counters, sizeof(ctx->hcounters));
     ctx->compute_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    span_collect(ctx);
     const int e = *ctx->h_err;
     if (e & ERRB_CAPACITY) return SSPP_ERR_CAPACITY;
     if (e & ERRB_LEN) return set_err(ctx, SSPP_ERR_CAPACITY, "a column exceeded 2^24 entries");
@@ -295,7 +421,7 @@ int run_compute(sspp_ctx* ctx) {
 
 int load_common(sspp_ctx* ctx, int64_t n, int64_t nnz) {
     ctx->loaded = ctx->inited = ctx->computed = false;
-    int rc = ensure_columns(ctx, n, nnz);
+    int rc = ensure_columns(ctx, std::max<int64_t>(n, 1), std::max<int64_t>(nnz, 1));
     if (rc) return rc;
     ctx->D.n = n;
     ctx->D.nnz = nnz;
@@ -352,6 +478,16 @@ void sspp_destroy(sspp_ctx* ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     free_device(ctx->D);
     if (ctx->dropped) cudaFree(ctx->dropped);
+    if (ctx->own_dims) cudaFree(ctx->own_dims);
+    if (ctx->own_colptr) cudaFree(ctx->own_colptr);
+    if (ctx->own_rows) cudaFree(ctx->own_rows);
+    for (auto* t : ctx->hc.tup)
+        if (t) cudaFree(t);
+    if (ctx->hc.deg) cudaFree(ctx->hc.deg);
+    if (ctx->hc.adj_off) cudaFree(ctx->hc.adj_off);
+    if (ctx->hc.adj) cudaFree(ctx->hc.adj);
+    if (ctx->hc.table) cudaFree(ctx->hc.table);
+    ctx->prof.release();
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     if (ctx->h_err) cudaFreeHost(ctx->h_err);
     if (ctx->h_counters) cudaFreeHost(ctx->h_counters);
@@ -372,11 +508,33 @@ int32_t sspp_load_csc(sspp_ctx* ctx, int64_t ncols, const int32_t* dims, const i
     if (nnz > 0 && !rows) return set_err(ctx, SSPP_ERR_BAD_INPUT, "null rows");
     int rc = load_common(ctx, ncols, nnz);
     if (rc) return rc;
+    if (ncols + 1 > ctx->cap_own_n) {
+        int64_t c1 = 0, c2 = 0;
+        if (ctx->own_dims) cudaFree(ctx->own_dims);
+        if (ctx->own_colptr) cudaFree(ctx->own_colptr);
+        ctx->own_dims = nullptr;
+        ctx->own_colptr = nullptr;
+        ctx->cap_own_n = 0;
+        CK(grow(ctx->own_dims, c1, ncols + 1));
+        CK(grow(ctx->own_colptr, c2, ncols + 1));
+        ctx->cap_own_n = ncols + 1;
+    }
+    if (nnz > ctx->cap_own_nnz || !ctx->own_rows) {
+        int64_t c3 = 0;
+        if (ctx->own_rows) cudaFree(ctx->own_rows);
+        ctx->own_rows = nullptr;
+        ctx->cap_own_nnz = 0;
+        CK(grow(ctx->own_rows, c3, std::max<int64_t>(nnz, 1)));
+        ctx->cap_own_nnz = std::max<int64_t>(nnz, 1);
+    }
     cudaStream_t s = ctx->stream;
-    if (ncols) CK(cudaMemcpyAsync(ctx->D.in_dims, dims, sizeof(int32_t) * ncols, cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(ctx->D.in_colptr, col_ptr, sizeof(int64_t) * (ncols + 1), cudaMemcpyHostToDevice, s));
-    if (nnz) CK(cudaMemcpyAsync(ctx->D.in_rows, rows, sizeof(int32_t) * nnz, cudaMemcpyHostToDevice, s));
+    if (ncols) CK(cudaMemcpyAsync(ctx->own_dims, dims, sizeof(int32_t) * ncols, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(ctx->own_colptr, col_ptr, sizeof(int64_t) * (ncols + 1), cudaMemcpyHostToDevice, s));
+    if (nnz) CK(cudaMemcpyAsync(ctx->own_rows, rows, sizeof(int32_t) * nnz, cudaMemcpyHostToDevice, s));
     CK(cudaStreamSynchronize(s));
+    ctx->D.in_dims = ctx->own_dims;
+    ctx->D.in_colptr = ctx->own_colptr;
+    ctx->D.in_rows = ctx->own_rows;
     ctx->loaded = true;
     return SSPP_OK;
 }
@@ -385,19 +543,18 @@ int32_t sspp_load_csc_device(sspp_ctx* ctx, int64_t ncols, const int32_t* d_dims
                              const int32_t* d_rows) {
     if (!ctx) return SSPP_ERR_BAD_INPUT;
     cudaSetDevice(ctx->cfg.device);
-    if (ncols < 0 || !d_col_ptr) return set_err(ctx, SSPP_ERR_BAD_INPUT, "null input array");
-    // col_ptr is validated on the host: it is small next to the rows
-    std::vector<int64_t> cp(size_t(ncols) + 1);
-    CK(cudaMemcpy(cp.data(), d_col_ptr, sizeof(int64_t) * (ncols + 1), cudaMemcpyDeviceToHost));
-    if (!validate_colptr(cp.data(), ncols)) return set_err(ctx, SSPP_ERR_BAD_INPUT, "col_ptr must start at 0 and be non-decreasing");
-    const int64_t nnz = cp[size_t(ncols)];
+    if (ncols < 0 || !d_col_ptr || (ncols > 0 && !d_dims)) return set_err(ctx, SSPP_ERR_BAD_INPUT, "null input array");
+    // col_ptr is checked on the device by the init pass; only its last entry is read here
+    int64_t nnz = 0;
+    CK(cudaMemcpyAsync(ctx->h_top, d_col_ptr + ncols, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    std::memcpy(&nnz, ctx->h_top, sizeof(int64_t));
+    if (nnz < 0 || (nnz > 0 && !d_rows)) return set_err(ctx, SSPP_ERR_BAD_INPUT, "col_ptr[ncols] out of range");
     int rc = load_common(ctx, ncols, nnz);
     if (rc) return rc;
-    cudaStream_t s = ctx->stream;
-    if (ncols) CK(cudaMemcpyAsync(ctx->D.in_dims, d_dims, sizeof(int32_t) * ncols, cudaMemcpyDeviceToDevice, s));
-    CK(cudaMemcpyAsync(ctx->D.in_colptr, d_col_ptr, sizeof(int64_t) * (ncols + 1), cudaMemcpyDeviceToDevice, s));
-    if (nnz) CK(cudaMemcpyAsync(ctx->D.in_rows, d_rows, sizeof(int32_t) * nnz, cudaMemcpyDeviceToDevice, s));
-    CK(cudaStreamSynchronize(s));
+    ctx->D.in_dims = const_cast<int32_t*>(d_dims);
+    ctx->D.in_colptr = const_cast<int64_t*>(d_col_ptr);
+    ctx->D.in_rows = const_cast<int32_t*>(d_rows);
     ctx->loaded = true;
     return SSPP_OK;
 }
@@ -507,6 +664,13 @@ int32_t sspp_get_stats(const sspp_ctx* ctx, sspp_stats* o) {
     o->nessential = ctx->computed ? c[CNT_NESS] : 0;
     o->init_ms = ctx->init_ms;
     o->compute_ms = ctx->compute_ms;
+    o->launches = ctx->launches;
+    o->init_gpu_ms = ctx->ph_ms[PH_INIT];
+    o->light_gpu_ms = ctx->ph_ms[PH_LIGHT];
+    o->heavy_gpu_ms = ctx->ph_ms[PH_HEAVY];
+    o->pairs_gpu_ms = ctx->ph_ms[PH_PAIRS];
+    o->light_launches = ctx->light_launches;
+    o->heavy_launches = ctx->heavy_launches;
     return SSPP_OK;
 }
 

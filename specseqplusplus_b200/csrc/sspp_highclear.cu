@@ -1,0 +1,279 @@
+// High-dimension guided clearing (model bit 1).
+//
+// Reference counterparts: init_contain_vertics (include/kernel.h:121-188:
+// vertex set of a simplex from its first two facets), maxdim_clear_init
+// (include/kernel.h:202-292: the clearing test on the top dimension), the
+// neighbour lists and binomial key tables (include/specseq.h:215-259) and the
+// driver (include/specseq.h:523-541).
+//
+// Test.  For a top-dimension simplex s = (v0 < ... < vD) the candidates w are
+// the neighbours of v0 in ascending order, at most max_iteration of them.  If
+// w is adjacent to every vertex of s, t = s + {w} is a simplex of the flag
+// complex; when every other facet of t exists and precedes s, s is the
+// youngest facet of t, so the column of s is a sum of earlier columns and s is
+// positive: its column is cleared.  Facets are found through an open-
+// addressing hash of the top-dimension vertex tuples (the reference sorts
+// combinatorial-number keys and binary-searches them).  One warp handles one
+// simplex, one lane one candidate.
+//
+// The reference walks the neighbour lists with a comparison in the wrong
+// direction (include/kernel.h:217), which only ever accepts the smallest
+// common neighbour; this kernel intersects the lists as intended.  Both are
+// sound, so the persistence pairs are the same; more columns are cleared here.
+// Only edges and simplices that survive an edge collapse take part.
+#include <climits>
+
+#include "sspp_highclear.h"
+#include "sspp_kernels.cuh"
+#include "sspp_scan.cuh"
+
+namespace sspp {
+
+static unsigned gridn(int64_t n, int t, int cap = 65536) {
+    int64_t g = (n + t - 1) / t;
+    if (g < 1) g = 1;
+    if (g > cap) g = cap;
+    return unsigned(g);
+}
+
+// Vertex tuple of every column of dimension d >= 1 (sorted, d+1 vertices),
+// from the first two facets' tuples.  tup_d / tup_f point at the tuple arrays of
+// dims d and d-1 (dim-0 tuples are the vertex indices themselves).
+__global__ void k_tuples(int32_t cb, int32_t ce, int d, int32_t fb, const int32_t* arena, const uint64_t* desc,
+                         const int32_t* tup_f, int32_t* tup_d, int* err) {
+    for (int64_t i = cb + blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < ce; i += int64_t(gridDim.x) * blockDim.x) {
+        uint64_t ds = desc[i];
+        const int32_t* c = arena + desc_off(ds);
+        int32_t* out = tup_d + (i - cb) * (d + 1);
+        if (desc_len(ds) < 2 || desc_len(ds) != uint32_t(d + 1)) {
+            // not a simplicial boundary (edge with < 2 vertices etc.): no tuple
+            for (int k = 0; k <= d; k++) out[k] = -1;
+            continue;
+        }
+        int32_t a[kMaxDim + 1], b[kMaxDim + 1];
+        for (int k = 0; k < d; k++) {
+            a[k] = (d == 1) ? c[0] : tup_f[int64_t(c[0] - fb) * d + k];
+            b[k] = (d == 1) ? c[1] : tup_f[int64_t(c[1] - fb) * d + k];
+        }
+        // union of two sorted d-tuples is a sorted (d+1)-tuple
+        int ia = 0, ib = 0, m = 0;
+        bool ok = true;
+        while ((ia < d || ib < d) && m <= d) {
+            int32_t x;
+            if (ib >= d || (ia < d && a[ia] < b[ib])) x = a[ia++];
+            else if (ia >= d || b[ib] < a[ia]) x = b[ib++];
+            else { x = a[ia++]; ib++; }
+            if (x < 0) ok = false;
+            out[m++] = x;
+        }
+        if (!ok || m != d + 1 || ia != d || ib != d) {
+            for (int k = 0; k <= d; k++) out[k] = -1;
+        }
+    }
+}
+
+__device__ __forceinline__ uint32_t tuple_hash(const int32_t* t, int k) {
+    uint64_t h = 0x9E3779B97F4A7C15ull;
+    for (int i = 0; i < k; i++) {
+        h ^= uint64_t(uint32_t(t[i])) + 0x632BE59BD9B4E019ull + (h << 6) + (h >> 2);
+        h *= 0xBF58476D1CE4E5B9ull;
+    }
+    h ^= h >> 31;
+    return uint32_t(h);
+}
+
+__global__ void k_hash_insert(int32_t cb, int32_t ce, int k, const int32_t* tup, const uint8_t* dropped, int32_t* table,
+                              uint32_t mask) {
+    for (int64_t i = cb + blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < ce; i += int64_t(gridDim.x) * blockDim.x) {
+        const int32_t* t = tup + (i - cb) * k;
+        if (t[0] < 0 || (dropped && dropped[i])) continue;
+        uint32_t h = tuple_hash(t, k) & mask;
+        for (uint32_t probe = 0; probe <= mask; probe++) {
+            int32_t old = atomicCAS(table + h, -1, int32_t(i));
+            if (old == -1) break;
+            h = (h + 1) & mask;
+        }
+    }
+}
+
+// column of the top-dimension simplex with vertex tuple t, or -1
+__device__ int32_t hash_find(const int32_t* t, int k, const int32_t* table, uint32_t mask, const int32_t* tup,
+                             int32_t cb) {
+    uint32_t h = tuple_hash(t, k) & mask;
+    for (uint32_t probe = 0; probe <= mask; probe++) {
+        int32_t c = table[h];
+        if (c < 0) return -1;
+        const int32_t* u = tup + int64_t(c - cb) * k;
+        bool eq = true;
+        for (int j = 0; j < k && eq; j++) eq = (u[j] == t[j]);
+        if (eq) return c;
+        h = (h + 1) & mask;
+    }
+    return -1;
+}
+
+// adjacency of the vertices (reordered vertex index = column index in [0, V))
+__global__ void k_degree(int32_t eb, int32_t ee, const int32_t* arena, const uint64_t* desc, const uint8_t* dropped,
+                         int32_t* deg) {
+    for (int64_t i = eb + blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < ee; i += int64_t(gridDim.x) * blockDim.x) {
+        uint64_t ds = desc[i];
+        if (desc_len(ds) != 2 || (dropped && dropped[i])) continue;
+        const int32_t* c = arena + desc_off(ds);
+        atomicAdd(deg + c[0], 1);
+        atomicAdd(deg + c[1], 1);
+    }
+}
+
+__global__ void k_adj_fill(int32_t eb, int32_t ee, const int32_t* arena, const uint64_t* desc, const uint8_t* dropped,
+                           const int64_t* adj_off, int32_t* fill, int32_t* adj) {
+    for (int64_t i = eb + blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < ee; i += int64_t(gridDim.x) * blockDim.x) {
+        uint64_t ds = desc[i];
+        if (desc_len(ds) != 2 || (dropped && dropped[i])) continue;
+        const int32_t* c = arena + desc_off(ds);
+        int32_t u = c[0], v = c[1];
+        adj[adj_off[u] + atomicAdd(fill + u, 1)] = v;
+        adj[adj_off[v] + atomicAdd(fill + v, 1)] = u;
+    }
+}
+
+// heap sort of one adjacency list (any length; O(d log d))
+__device__ void heap_sort(int32_t* a, int64_t n) {
+    auto sift = [&](int64_t root, int64_t end) {
+        while (2 * root + 1 < end) {
+            int64_t c = 2 * root + 1;
+            if (c + 1 < end && a[c] < a[c + 1]) c++;
+            if (a[root] >= a[c]) return;
+            int32_t t = a[root]; a[root] = a[c]; a[c] = t;
+            root = c;
+        }
+    };
+    for (int64_t s = n / 2 - 1; s >= 0; s--) sift(s, n);
+    for (int64_t e = n - 1; e > 0; e--) {
+        int32_t t = a[0]; a[0] = a[e]; a[e] = t;
+        sift(0, e);
+    }
+}
+
+__global__ void k_adj_sort(int64_t nv, const int64_t* adj_off, int32_t* adj) {
+    for (int64_t v = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; v < nv; v += int64_t(gridDim.x) * blockDim.x) {
+        int32_t* a = adj + adj_off[v];
+        int64_t n = adj_off[v + 1] - adj_off[v];
+        if (n <= 32) {
+            for (int64_t i = 1; i < n; i++) {
+                int32_t x = a[i];
+                int64_t j = i - 1;
+                while (j >= 0 && a[j] > x) { a[j + 1] = a[j]; j--; }
+                a[j + 1] = x;
+            }
+        } else {
+            heap_sort(a, n);
+        }
+    }
+}
+
+__device__ __forceinline__ bool adj_has(const int32_t* adj, const int64_t* adj_off, int32_t u, int32_t w) {
+    int64_t lo = adj_off[u], hi = adj_off[u + 1];
+    while (lo < hi) {
+        int64_t mid = (lo + hi) >> 1;
+        if (adj[mid] < w) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo < adj_off[u + 1] && adj[lo] == w;
+}
+
+// one warp per top-dimension simplex, one lane per candidate
+__global__ void k_highclear(int32_t cb, int32_t ce, int D, int max_iter, const int32_t* tup, const int32_t* adj,
+                            const int64_t* adj_off, const int32_t* table, uint32_t mask, const uint8_t* dropped,
+                            uint8_t* cleared, long long* counters) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5;
+    const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+    const int k = D + 1;
+    long long found_total = 0;
+    for (int64_t i = cb + warp; i < ce; i += nwarps) {
+        const int32_t* s = tup + (i - cb) * k;
+        if (s[0] < 0 || (dropped && dropped[i])) continue;
+        const int32_t v0 = s[0];
+        const int64_t nb = adj_off[v0 + 1] - adj_off[v0];
+        const int64_t limit = nb < max_iter ? nb : max_iter;
+        bool found = false;
+        for (int64_t base = 0; base < limit && !found; base += 32) {
+            bool ok = false;
+            int64_t q = base + lane;
+            if (q < limit) {
+                const int32_t w = adj[adj_off[v0] + q];
+                ok = true;
+                for (int j = 1; j < k && ok; j++) ok = adj_has(adj, adj_off, s[j], w);
+                if (ok) {
+                    // t = s + {w}, sorted; every facet other than s must exist and precede column i
+                    int32_t t[kMaxDim + 2];
+                    int m = 0;
+                    bool placed = false;
+                    for (int j = 0; j < k; j++) {
+                        if (!placed && w < s[j]) { t[m++] = w; placed = true; }
+                        t[m++] = s[j];
+                    }
+                    if (!placed) t[m++] = w;
+                    int32_t f[kMaxDim + 1];
+                    for (int drop = 0; drop <= k && ok; drop++) {
+                        if (t[drop] == w) continue;  // that facet is s itself
+                        int mm = 0;
+                        for (int j = 0; j <= k; j++)
+                            if (j != drop) f[mm++] = t[j];
+                        int32_t c = hash_find(f, k, table, mask, tup, cb);
+                        ok = (c >= 0 && c < i);
+                    }
+                }
+            }
+            found = __any_sync(kFull, ok);
+        }
+        if (found && lane == 0) {
+            cleared[i] = 1;
+            found_total++;
+        }
+    }
+    if (lane == 0 && found_total) cnt_add(&counters[CNT_HIGHCLEAR], found_total);
+}
+
+int highclear(Device& D, const DimInfo& info, int max_iteration, const uint8_t* dropped, HighclearScratch& S,
+              cudaStream_t s) {
+    // top dimension with columns
+    int top = -1;
+    for (int d = kMaxDim; d >= 1; d--)
+        if (info.col_end[d] > info.col_begin[d]) { top = d; break; }
+    if (top < 1 || max_iteration <= 0) return 0;
+    int launches = 0;
+    // tuples of dims 1..top
+    const int32_t* prev = nullptr;
+    for (int d = 1; d <= top; d++) {
+        int32_t cb = info.col_begin[d], ce = info.col_end[d];
+        k_tuples<<<gridn(ce - cb, 256), 256, 0, s>>>(cb, ce, d, info.col_begin[d - 1], D.arena, D.desc, prev,
+                                                    S.tup[d], D.err);
+        launches++;
+        prev = S.tup[d];
+    }
+    // adjacency
+    const int64_t nv = info.col_end[0] - info.col_begin[0];
+    cudaMemsetAsync(S.deg, 0, sizeof(int32_t) * (nv + 1), s);
+    k_degree<<<gridn(info.col_end[1] - info.col_begin[1], 256), 256, 0, s>>>(info.col_begin[1], info.col_end[1],
+                                                                            D.arena, D.desc, dropped, S.deg);
+    const int32_t* deg = S.deg;
+    int64_t* adj_off = S.adj_off;
+    scan([=] __device__(int64_t v) -> int64_t { return v < nv ? deg[v] : 0; },
+         [=] __device__(int64_t v, int64_t pre, int64_t) { adj_off[v] = pre; }, nv + 1, D.blk, s);
+    cudaMemsetAsync(S.deg, 0, sizeof(int32_t) * (nv + 1), s);
+    k_adj_fill<<<gridn(info.col_end[1] - info.col_begin[1], 256), 256, 0, s>>>(
+        info.col_begin[1], info.col_end[1], D.arena, D.desc, dropped, S.adj_off, S.deg, S.adj);
+    k_adj_sort<<<gridn(nv, 128), 128, 0, s>>>(nv, S.adj_off, S.adj);
+    launches += 6;
+    // hash of the top-dimension tuples
+    cudaMemsetAsync(S.table, 0xff, sizeof(int32_t) * (size_t(S.mask) + 1), s);
+    const int32_t cb = info.col_begin[top], ce = info.col_end[top];
+    k_hash_insert<<<gridn(ce - cb, 256), 256, 0, s>>>(cb, ce, top + 1, S.tup[top], dropped, S.table, S.mask);
+    k_highclear<<<gridn(int64_t(ce - cb) * 32, 256, 148 * 64), 256, 0, s>>>(
+        cb, ce, top, max_iteration, S.tup[top], S.adj, S.adj_off, S.table, S.mask, dropped, D.cleared, D.counters);
+    launches += 2;
+    return launches;
+}
+
+}  // namespace sspp

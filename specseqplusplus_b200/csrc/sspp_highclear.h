@@ -1,0 +1,25 @@
+// High-dimension guided clearing: scratch buffers and launcher.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "sspp_internal.h"
+
+namespace sspp {
+
+struct HighclearScratch {
+    int32_t* tup[kNumDims] = {};   // vertex tuples of dims 1..top, (d+1) ints per column
+    int64_t cap_tup[kNumDims] = {};
+    int32_t* deg = nullptr;         // [nv + 1]
+    int64_t* adj_off = nullptr;     // [nv + 1]
+    int32_t* adj = nullptr;         // [2 E]
+    int32_t* table = nullptr;       // open addressing, mask + 1 slots
+    uint32_t mask = 0;
+    int64_t cap_deg = 0, cap_adj_off = 0, cap_adj = 0, cap_table = 0;
+};
+
+// Sets cleared[] for the top-dimension columns the test proves positive;
+// returns the number of kernels launched.  Buffers must be sized by the caller.
+int highclear(Device& D, const DimInfo& info, int max_iteration, const uint8_t* dropped, HighclearScratch& S,
+              cudaStream_t s);
+
+}  // namespace sspp

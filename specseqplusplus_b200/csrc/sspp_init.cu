@@ -76,8 +76,10 @@ __global__ void k_validate(const int32_t* dims, const int64_t* colptr, int64_t n
     }
 }
 
-void validate(Device& D, cudaStream_t s) {
-    if (D.n > 0) k_validate<<<grid_for(D.n, 256) > 4096 ? 4096 : grid_for(D.n, 256), 256, 0, s>>>(D.in_dims, D.in_colptr, D.n, D.err);
+int validate(Device& D, cudaStream_t s) {
+    if (D.n <= 0) return 0;
+    k_validate<<<grid_for(D.n, 256) > 4096 ? 4096 : grid_for(D.n, 256), 256, 0, s>>>(D.in_dims, D.in_colptr, D.n, D.err);
+    return 1;
 }
 
 // ------------------------------------------------------------------ reorder
@@ -197,7 +199,7 @@ __global__ void k_scatter_cols(int64_t n, const int64_t* colptr, const int32_t* 
 
 int64_t reorder_total_slot(const Device& D) { return scan_blocks(D.n); }
 
-void reorder(Device& D, cudaStream_t s) {
+int reorder(Device& D, cudaStream_t s) {
     const int64_t n = D.n;
     const int64_t nb = (n + kPartThreads - 1) / kPartThreads;
     k_dim_count<<<unsigned(nb), kPartThreads, 0, s>>>(D.in_dims, n, D.dimcnt, D.err);
@@ -211,6 +213,7 @@ void reorder(Device& D, cudaStream_t s) {
          [=] __device__(int64_t i, int64_t pre, int64_t) { off[i] = pre; }, n, D.blk, s);
     k_scatter_cols<<<grid_for(n, 256) > 65536 ? 65536 : grid_for(n, 256), 256, 0, s>>>(
         n, D.in_colptr, D.in_rows, D.in_dims, D.perm, D.newidx, off, D.arena, D.desc, D.leftmost, D.err);
+    return 7;
 }
 
 // ------------------------------------------------------------- init passes
@@ -321,19 +324,21 @@ __global__ void k_diminfo_reset(DimInfo* info) {
     if (d < kNumDims) { info->min_row[d] = INT_MAX; info->max_row[d] = -1; }
 }
 
-void init_passes(Device& D, cudaStream_t s) {
+int init_passes(Device& D, cudaStream_t s) {
     const int64_t n = D.n;
     const unsigned g = grid_for(n, 256) > 65536 ? 65536 : grid_for(n, 256);
     k_init_low<<<g, 256, 0, s>>>(n, D.arena, D.desc, D.low, D.leftmost, D.pivot, D.cleared, D.negative);
     k_init_apparent<<<g, 256, 0, s>>>(n, D.arena, D.desc, D.low, D.leftmost, D.pivot, D.cleared, D.negative,
                                       D.counters);
+    return 2;
 }
 
-void init_compress(Device& D, const uint8_t* dropped, cudaStream_t s) {
+int init_compress(Device& D, const uint8_t* dropped, cudaStream_t s) {
     const int64_t n = D.n;
     const unsigned g = grid_for(n, 256) > 65536 ? 65536 : grid_for(n, 256);
     k_init_compress<<<g, 256, 0, s>>>(n, D.arena, D.desc, D.low, D.pivot, D.cleared, D.negative, D.state, dropped,
                                       D.counters, D.err);
+    return 1;
 }
 
 // Active list in reordered order (dimension segments are contiguous) and the
@@ -347,7 +352,7 @@ __global__ void k_act_segments(const int64_t* actpos, int64_t n, DimInfo* info) 
     }
 }
 
-void active_list(Device& D, cudaStream_t s) {
+int active_list(Device& D, cudaStream_t s) {
     const int64_t n = D.n;
     const uint8_t* state = D.state;
     int32_t* act = D.active;
@@ -364,6 +369,7 @@ void active_list(Device& D, cudaStream_t s) {
     k_diminfo_reset<<<1, 32, 0, s>>>(D.diminfo);
     const unsigned g = grid_for(n, 256) > 4096 ? 4096 : grid_for(n, 256);
     k_dim_rows<<<g, 256, 0, s>>>(n, D.dim, D.arena, D.desc, D.low, D.state, D.diminfo);
+    return 6;
 }
 
 // ------------------------------------------------------------------- pairs
@@ -395,7 +401,7 @@ __global__ void k_mark_dropped(int64_t n, const uint8_t* dropped, const int32_t*
         if (dropped[i]) paired[perm[i]] = 1;
 }
 
-void extract_pairs(Device& D, int dual, const uint8_t* dropped, cudaStream_t s) {
+int extract_pairs(Device& D, int dual, const uint8_t* dropped, cudaStream_t s) {
     const int64_t n = D.n;
     const unsigned g = grid_for(n, 256) > 65536 ? 65536 : grid_for(n, 256);
     fill_i64(D.death_of, -1, n, s);
@@ -421,6 +427,7 @@ void extract_pairs(Device& D, int dual, const uint8_t* dropped, cudaStream_t s) 
          },
          n, D.blk, s);
     cudaMemcpyAsync(&D.counters[CNT_NESS], D.blk + scan_blocks(n), sizeof(int64_t), cudaMemcpyDeviceToDevice, s);
+    return 8 + (dropped ? 1 : 0);
 }
 
 }  // namespace sspp

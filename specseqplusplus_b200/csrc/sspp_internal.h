@@ -20,6 +20,7 @@ enum : uint8_t {
     ST_ZERO = 2,     // reduced to zero (positive) or empty input column
     ST_CLEARED = 3,  // zeroed by clearing (positive), never reduced
     ST_DROPPED = 4,  // removed by edge collapse
+    ST_HEAVY = 5,    // handed from the warp tier to the CTA tier
 };
 
 // A column is stored in the arena at a 16-byte aligned offset, padded with
@@ -101,7 +102,8 @@ struct Device {
     DimInfo* diminfo = nullptr;
     int* err = nullptr;
     long long* counters = nullptr;
-    int* step_ctr = nullptr;     // per-launch work counters
+    int* step_ctr = nullptr;     // per-step work counters (3 ints per step)
+    int32_t* heavy = nullptr;    // [n] columns handed to the CTA tier
     int64_t cap_steps = 0;
     // pairs output (input indices)
     int64_t* death_of = nullptr;   // [n]

@@ -30,7 +30,8 @@ class SsppError(RuntimeError):
 
 
 class _Config(ctypes.Structure):
-    _fields_ = [("device", ctypes.c_int32), ("arena_bytes", ctypes.c_int64), ("verbose", ctypes.c_int32)]
+    _fields_ = [("device", ctypes.c_int32), ("arena_bytes", ctypes.c_int64), ("verbose", ctypes.c_int32),
+                ("profile", ctypes.c_int32)]
 
 
 class _Params(ctypes.Structure):
@@ -44,7 +45,9 @@ class _Stats(ctypes.Structure):
     _fields_ = [(k, ctypes.c_int64) for k in (
         "ncols", "nnz", "active_after_init", "apparent_pairs", "cleared_init", "highclear_cleared",
         "collapse_dropped", "additions", "add_ints", "published_ints", "displaced", "ss_steps", "npairs",
-        "nessential")] + [("init_ms", ctypes.c_double), ("compute_ms", ctypes.c_double)]
+        "nessential")] + [("init_ms", ctypes.c_double), ("compute_ms", ctypes.c_double), ("launches", ctypes.c_int64)] + [
+        (k, ctypes.c_double) for k in ("init_gpu_ms", "light_gpu_ms", "heavy_gpu_ms", "pairs_gpu_ms")] + [
+        ("light_launches", ctypes.c_int64), ("heavy_launches", ctypes.c_int64)]
 
 
 @dataclass
@@ -111,9 +114,9 @@ EXPORTED = ("sspp_create", "sspp_destroy", "sspp_last_error", "sspp_default_para
 class Engine:
     """One device context (include/sspp.h)."""
 
-    def __init__(self, device: int = 0, arena_bytes: int = 0, verbose: int = 0):
+    def __init__(self, device: int = 0, arena_bytes: int = 0, verbose: int = 0, profile: int = 0):
         self._lib = load_library()
-        cfg = _Config(device, arena_bytes, verbose)
+        cfg = _Config(device, arena_bytes, verbose, profile)
         self._h = self._lib.sspp_create(ctypes.byref(cfg))
         if not self._h:
             raise SsppError(ERR_CUDA, "sspp_create failed (no usable CUDA device?)")
@@ -160,25 +163,34 @@ class Engine:
         p = (params or Params())._c()
         self._check(self._lib.sspp_reduce(self._h, ctypes.byref(p), stream or None))
 
-    def pairs(self) -> np.ndarray:
+    def num_pairs(self) -> int:
+        return int(self._lib.sspp_num_pairs(self._h))
+
+    def num_essential(self) -> int:
+        return int(self._lib.sspp_num_essential(self._h))
+
+    def pairs(self, out: np.ndarray | None = None) -> np.ndarray:
+        """Sorted (birth, death) pairs; `out` (int64, >= 2 * npairs entries, e.g. pinned) is filled if given."""
         n = self._lib.sspp_num_pairs(self._h)
         if n < 0:
             self._check(ERR_STATE)
-        out = np.empty((n, 2), dtype=np.int64)
+        if out is None:
+            out = np.empty((n, 2), dtype=np.int64)
         got = self._lib.sspp_pairs(self._h, out.ctypes.data, n)
         if got != n:
             self._check(ERR_CUDA)
-        return out
+        return out.reshape(-1)[: 2 * n].reshape(n, 2)
 
-    def essentials(self) -> np.ndarray:
+    def essentials(self, out: np.ndarray | None = None) -> np.ndarray:
         n = self._lib.sspp_num_essential(self._h)
         if n < 0:
             self._check(ERR_STATE)
-        out = np.empty(n, dtype=np.int64)
+        if out is None:
+            out = np.empty(n, dtype=np.int64)
         got = self._lib.sspp_essentials(self._h, out.ctypes.data, n)
         if got != n:
             self._check(ERR_CUDA)
-        return out
+        return out[:n]
 
     def write_pairs(self, path: str, fmt: int = ASCII) -> None:
         self._check(self._lib.sspp_write_pairs(self._h, path.encode(), fmt))
