@@ -56,6 +56,7 @@ typedef struct sspp_params {
     int32_t level1_capacity;  /* per-worker on-chip column capacity (ints)            */
     int32_t level2_capacity;  /* per-block on-chip column capacity (ints)             */
     int32_t autotune;
+    int32_t heavy_threads;    /* threads per heavy-tier column: 128 or 256 (0 = 256)  */
 } sspp_params;
 
 /* Per-run counters (device-side counters plus host timings). */

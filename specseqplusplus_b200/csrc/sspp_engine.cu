@@ -56,6 +56,10 @@ struct sspp_ctx {
     std::string err;
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
+    static constexpr int kSide = 16;
+    cudaStream_t side[kSide] = {};     // heavy-tier launches overlap later light steps and each other
+    std::vector<cudaEvent_t> step_ev;  // light step k done
+    cudaEvent_t join_ev[kSide] = {};   // side stream joins
     Device D;
     sspp_params params{};
     bool loaded = false, inited = false, computed = false;
@@ -64,8 +68,9 @@ struct sspp_ctx {
     int num_sms = 0;
     int light_blocks_per_sm = 0;
     int heavy_blocks_per_sm = 0;
-    int configured_cap1 = -1, configured_cap2 = -1;
+    int configured_cap1 = -1, configured_cap2 = -1, configured_ht = -1;
     int64_t arena_request = 0;     // ints requested for the arena (grows on CAPACITY)
+    int64_t pool_request = 0;      // heavy pool entries requested (grows on CAPACITY)
     double init_ms = 0, compute_ms = 0;
     int64_t ss_steps = 0;
     int* h_err = nullptr;          // pinned
@@ -114,7 +119,7 @@ cudaError_t grow(T*& p, int64_t& cap, int64_t want) {
 void free_device(Device& D) {
     void* ptrs[] = {D.dim, D.perm, D.newidx, D.scratch64, D.arena, D.arena_top,
                     D.desc, D.low, D.pivot, D.state, D.cleared, D.negative, D.leftmost, D.active, D.blk, D.dimcnt,
-                    D.diminfo, D.err, D.counters, D.step_ctr, D.heavy, D.death_of, D.pairs, D.ess};
+                    D.diminfo, D.err, D.counters, D.step_ctr, D.heavy, D.pool_tail, D.death_of, D.pairs, D.ess};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     D = Device();
@@ -144,7 +149,6 @@ int ensure_columns(sspp_ctx* ctx, int64_t n, int64_t nnz) {
         CK(g(D.negative, 1));
         CK(g(D.leftmost, 1));
         CK(g(D.active, 1));
-        CK(g(D.heavy, 1));
         CK(g(D.death_of, 1));
         CK(g(D.pairs, 2));
         CK(g(D.ess, 1));
@@ -159,9 +163,14 @@ int ensure_columns(sspp_ctx* ctx, int64_t n, int64_t nnz) {
         CK(cudaMalloc(&D.err, sizeof(int)));
         CK(cudaMalloc(&D.counters, sizeof(long long) * CNT_NUM));
         CK(cudaMalloc(&D.arena_top, sizeof(unsigned long long)));
+        CK(cudaMalloc(&D.pool_tail, sizeof(int)));
     }
     return SSPP_OK;
 }
+
+// Guard ints after the usable arena: staging reads a whole first round of a
+// slot (up to 1024 ints) without knowing its length yet.
+constexpr int64_t kArenaGuard = 8192;
 
 int ensure_arena(sspp_ctx* ctx, int64_t ints) {
     Device& D = ctx->D;
@@ -169,13 +178,13 @@ int ensure_arena(sspp_ctx* ctx, int64_t ints) {
     if (D.arena) cudaFree(D.arena);
     D.arena = nullptr;
     D.arena_cap = 0;
-    CK(cudaMalloc(&D.arena, size_t(ints) * sizeof(int32_t)));
+    CK(cudaMalloc(&D.arena, size_t(ints + kArenaGuard) * sizeof(int32_t)));
     D.arena_cap = ints;
     return SSPP_OK;
 }
 
 int64_t arena_need(const sspp_ctx* ctx) {
-    const int64_t base = ctx->D.nnz + 3 * ctx->D.n + 4;
+    const int64_t base = ctx->D.nnz + (kHdr + 3) * ctx->D.n + 4;
     int64_t want = base + std::max<int64_t>(2 * base, int64_t(16) << 20);
     if (ctx->cfg.arena_bytes > 0) want = std::max<int64_t>(want, ctx->cfg.arena_bytes / 4);
     return std::max(want, ctx->arena_request);
@@ -219,6 +228,8 @@ int check_params(sspp_ctx* ctx, const sspp_params* p) {
     if (!(p->growth >= 1.0f) || !std::isfinite(p->growth))
         return set_err(ctx, SSPP_ERR_BAD_INPUT, "block_size_growth_rate must be >= 1");
     if (p->queue_size < 1) return set_err(ctx, SSPP_ERR_BAD_INPUT, "queue_size must be >= 1");
+    if (p->heavy_threads != 0 && p->heavy_threads != 128 && p->heavy_threads != 256)
+        return set_err(ctx, SSPP_ERR_BAD_INPUT, "heavy_threads must be 0, 128 or 256");
     if (p->level1_capacity < 0 || p->level2_capacity < 0)
         return set_err(ctx, SSPP_ERR_BAD_INPUT, "level capacities must be >= 0");
     if (p->dualize) return set_err(ctx, SSPP_ERR_BAD_INPUT, "dualize is not available in this build");
@@ -239,16 +250,16 @@ int level2_cap(const sspp_params& p) {
     return (c + 31) & ~31;
 }
 
-void span_begin(sspp_ctx* ctx, cudaEvent_t& a) {
+void span_begin(sspp_ctx* ctx, cudaEvent_t& a, cudaStream_t st = nullptr) {
     if (ctx->cfg.profile) {
         a = ctx->prof.get();
-        cudaEventRecord(a, ctx->stream);
+        cudaEventRecord(a, st ? st : ctx->stream);
     }
 }
-void span_end(sspp_ctx* ctx, int phase, cudaEvent_t a) {
+void span_end(sspp_ctx* ctx, int phase, cudaEvent_t a, cudaStream_t st = nullptr) {
     if (ctx->cfg.profile) {
         cudaEvent_t b = ctx->prof.get();
-        cudaEventRecord(b, ctx->stream);
+        cudaEventRecord(b, st ? st : ctx->stream);
         ctx->prof.spans.push_back({phase, a, b});
     }
 }
@@ -359,10 +370,12 @@ int run_compute(sspp_ctx* ctx) {
     }
     const sspp_params& P = ctx->params;
     const int cap1 = level1_cap(P), cap2 = level2_cap(P);
-    if (cap1 != ctx->configured_cap1 || cap2 != ctx->configured_cap2) {
-        CK(reduce_configure(cap1, cap2, &ctx->light_blocks_per_sm, &ctx->heavy_blocks_per_sm));
+    const int ht = P.heavy_threads == 128 ? 128 : 256;
+    if (cap1 != ctx->configured_cap1 || cap2 != ctx->configured_cap2 || ht != ctx->configured_ht) {
+        CK(reduce_configure(cap1, cap2, ht, &ctx->light_blocks_per_sm, &ctx->heavy_blocks_per_sm));
         ctx->configured_cap1 = cap1;
         ctx->configured_cap2 = cap2;
+        ctx->configured_ht = ht;
         if (ctx->light_blocks_per_sm < 1 || ctx->heavy_blocks_per_sm < 1)
             return set_err(ctx, SSPP_ERR_CAPACITY, "level capacities too large for shared memory");
     }
@@ -371,32 +384,80 @@ int run_compute(sspp_ctx* ctx) {
     const DimInfo& I = ctx->hinfo;
     for (int d = kMaxDim; d >= 1; d--)
         ss_schedule(P, I.act_begin[d], I.act_end[d], I.min_row[d] == INT_MAX ? 0 : I.min_row[d], I.max_row[d], steps);
-    if (3 * int64_t(steps.size()) > D.cap_steps) {
+    if (4 * int64_t(steps.size()) > D.cap_steps) {
         if (D.step_ctr) cudaFree(D.step_ctr);
         D.step_ctr = nullptr;
         D.cap_steps = 0;
-        CK(grow(D.step_ctr, D.cap_steps, 3 * int64_t(steps.size()) + 64));
+        CK(grow(D.step_ctr, D.cap_steps, 4 * int64_t(steps.size()) + 64));
     }
-    if (!steps.empty()) CK(cudaMemsetAsync(D.step_ctr, 0, sizeof(int) * 3 * steps.size(), s));
+    if (!steps.empty()) CK(cudaMemsetAsync(D.step_ctr, 0, sizeof(int) * 4 * steps.size(), s));
+    // heavy pool: deferrals are rare (heavy columns and displaced owners); a
+    // full pool sets the capacity bit and the run is repeated with a larger one
+    const int64_t want_pool = std::max<int64_t>(ctx->pool_request, std::max<int64_t>(D.n / 4, 1 << 16));
+    if (want_pool > D.pool_cap) {
+        if (D.heavy) cudaFree(D.heavy);
+        D.heavy = nullptr;
+        D.pool_cap = 0;
+        CK(grow(D.heavy, D.pool_cap, want_pool));
+    }
+    CK(cudaMemsetAsync(D.pool_tail, 0, sizeof(int), s));
     const int light_max = std::max(1, ctx->num_sms * ctx->light_blocks_per_sm);
-    const int heavy_grid = std::max(1, ctx->num_sms * ctx->heavy_blocks_per_sm);
+    const int heavy_grid = std::max(1, std::min(ctx->num_sms * ctx->heavy_blocks_per_sm, 2 * ctx->num_sms));
     const int q_blocks = std::max(1, (P.queue_size + 3) / 4);
+    const int chunk = 8;
+    // Heavy launches go to side streams (round robin) after their light step:
+    // they overlap the following light steps and each other, so long chains of
+    // different steps run concurrently.  Each dimension's completion sweep, and
+    // the next dimension, wait for all of them (twist clearing needs the
+    // finished dimension).
+    const bool overlap = true;
+    while (ctx->step_ev.size() < steps.size() + 1) {
+        cudaEvent_t ev;
+        CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        ctx->step_ev.push_back(ev);
+    }
+    auto join_sides = [&]() -> int {
+        for (int q = 0; q < sspp_ctx::kSide; q++) {
+            CK(cudaEventRecord(ctx->join_ev[q], ctx->side[q]));
+            CK(cudaStreamWaitEvent(s, ctx->join_ev[q], 0));
+        }
+        return SSPP_OK;
+    };
     for (size_t k = 0; k < steps.size(); k++) {
         const Step& st = steps[k];
-        int64_t chunks = (int64_t(st.end - st.beg) + 31) / 32;
+        const bool last_of_dim = st.minrow == INT32_MIN;
+        if (overlap && last_of_dim) {  // join: everything heavy of this dimension is done
+            int rcj = join_sides();
+            if (rcj) return rcj;
+        }
+        int64_t chunks = (int64_t(st.end - st.beg) + chunk - 1) / chunk;
         int grid = int(std::min<int64_t>(std::min<int64_t>((chunks + 3) / 4, light_max), q_blocks));
         grid = std::max(grid, 1);
-        int* ctr = D.step_ctr + 3 * k;
+        int* ctr = D.step_ctr + 4 * k;
         cudaEvent_t a = nullptr, b = nullptr;
         span_begin(ctx, a);
-        reduce_light_launch(D, D.active, st.beg, st.end, st.minrow, cap1, ctr, grid, s);
+        reduce_light_launch(D, D.active, st.beg, st.end, st.minrow, cap1, chunk, ctr, grid, s);
         span_end(ctx, PH_LIGHT, a);
-        span_begin(ctx, b);
-        reduce_heavy_launch(D, st.minrow, cap2, ctr, heavy_grid, s);
-        span_end(ctx, PH_HEAVY, b);
+        heavy_slice_mark(D, ctr, k + 1 < steps.size() ? ctr + 4 : nullptr, s);
+        if (overlap && !last_of_dim) {
+            cudaStream_t hs = ctx->side[k % sspp_ctx::kSide];
+            CK(cudaEventRecord(ctx->step_ev[k], s));
+            CK(cudaStreamWaitEvent(hs, ctx->step_ev[k], 0));
+            span_begin(ctx, b, hs);
+            reduce_heavy_launch(D, cap2, ht, ctr, heavy_grid, hs);
+            span_end(ctx, PH_HEAVY, b, hs);
+        } else {
+            span_begin(ctx, b);
+            reduce_heavy_launch(D, cap2, ht, ctr, heavy_grid, s);
+            span_end(ctx, PH_HEAVY, b);
+        }
         ctx->light_launches++;
         ctx->heavy_launches++;
-        ctx->launches += 2;
+        ctx->launches += 3;
+    }
+    if (overlap) {  // nothing may still run on a side stream past this point
+        int rcj = join_sides();
+        if (rcj) return rcj;
     }
     ctx->ss_steps = int64_t(steps.size());
     cudaEvent_t ep = nullptr;
@@ -414,6 +475,7 @@ int run_compute(sspp_ctx* ctx) {
     if (e & ERRB_CAPACITY) return SSPP_ERR_CAPACITY;
     if (e & ERRB_LEN) return set_err(ctx, SSPP_ERR_CAPACITY, "a column exceeded 2^24 entries");
     if (e & ERRB_TIMEOUT) return set_err(ctx, SSPP_ERR_TIMEOUT, "per-column merge limit reached");
+    if (e & ERRB_CHECK) return set_err(ctx, SSPP_ERR_BAD_INPUT, "reduction self-check failed (bad index skipped)");
     if (e) return set_err(ctx, SSPP_ERR_BAD_INPUT, "device error word set");
     ctx->computed = true;
     return SSPP_OK;
@@ -451,6 +513,7 @@ void sspp_default_params(sspp_params* p) {
     p->level1_capacity = 1000;
     p->level2_capacity = 8000;
     p->autotune = 0;
+    p->heavy_threads = 0;
 }
 
 sspp_ctx* sspp_create(const sspp_config* cfg) {
@@ -459,6 +522,13 @@ sspp_ctx* sspp_create(const sspp_config* cfg) {
     if (cfg) ctx->cfg = *cfg;
     if (cudaSetDevice(ctx->cfg.device) != cudaSuccess) { delete ctx; return nullptr; }
     if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess) { delete ctx; return nullptr; }
+    for (int q = 0; q < sspp_ctx::kSide; q++) {
+        if (cudaStreamCreateWithFlags(&ctx->side[q], cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&ctx->join_ev[q], cudaEventDisableTiming) != cudaSuccess) {
+            delete ctx;
+            return nullptr;
+        }
+    }
     ctx->stream = ctx->own_stream;
     cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->cfg.device);
     if (cudaMallocHost(&ctx->h_err, sizeof(int)) != cudaSuccess ||
@@ -488,6 +558,13 @@ void sspp_destroy(sspp_ctx* ctx) {
     if (ctx->hc.adj) cudaFree(ctx->hc.adj);
     if (ctx->hc.table) cudaFree(ctx->hc.table);
     ctx->prof.release();
+    for (int q = 0; q < sspp_ctx::kSide; q++)
+        if (ctx->side[q]) cudaStreamSynchronize(ctx->side[q]);
+    for (auto ev : ctx->step_ev) cudaEventDestroy(ev);
+    for (int q = 0; q < sspp_ctx::kSide; q++) {
+        if (ctx->join_ev[q]) cudaEventDestroy(ctx->join_ev[q]);
+        if (ctx->side[q]) cudaStreamDestroy(ctx->side[q]);
+    }
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     if (ctx->h_err) cudaFreeHost(ctx->h_err);
     if (ctx->h_counters) cudaFreeHost(ctx->h_counters);
@@ -587,8 +664,9 @@ int32_t sspp_compute(sspp_ctx* ctx, void* stream) {
     for (int attempt = 0; attempt < 6; attempt++) {
         int rc = run_compute(ctx);
         if (rc != SSPP_ERR_CAPACITY || !ctx->err.empty()) return rc;
-        // arena exhausted: grow it and redo the whole reduction from the input
+        // arena or heavy pool exhausted: grow both and redo the whole reduction from the input
         ctx->arena_request = std::max<int64_t>(ctx->D.arena_cap * 2, arena_need(ctx));
+        ctx->pool_request = std::max<int64_t>(ctx->D.pool_cap * 2, 1 << 16);
         rc = run_init(ctx);
         if (rc) return rc;
     }

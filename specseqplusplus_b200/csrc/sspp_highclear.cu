@@ -43,7 +43,7 @@ __global__ void k_tuples(int32_t cb, int32_t ce, int d, int32_t fb, const int32_
                          const int32_t* tup_f, int32_t* tup_d, int* err) {
     for (int64_t i = cb + blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < ce; i += int64_t(gridDim.x) * blockDim.x) {
         uint64_t ds = desc[i];
-        const int32_t* c = arena + desc_off(ds);
+        const int32_t* c = arena + desc_off(ds) + kHdr;
         int32_t* out = tup_d + (i - cb) * (d + 1);
         if (desc_len(ds) < 2 || desc_len(ds) != uint32_t(d + 1)) {
             // not a simplicial boundary (edge with < 2 vertices etc.): no tuple
@@ -118,7 +118,7 @@ __global__ void k_degree(int32_t eb, int32_t ee, const int32_t* arena, const uin
     for (int64_t i = eb + blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < ee; i += int64_t(gridDim.x) * blockDim.x) {
         uint64_t ds = desc[i];
         if (desc_len(ds) != 2 || (dropped && dropped[i])) continue;
-        const int32_t* c = arena + desc_off(ds);
+        const int32_t* c = arena + desc_off(ds) + kHdr;
         atomicAdd(deg + c[0], 1);
         atomicAdd(deg + c[1], 1);
     }
@@ -129,7 +129,7 @@ __global__ void k_adj_fill(int32_t eb, int32_t ee, const int32_t* arena, const u
     for (int64_t i = eb + blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < ee; i += int64_t(gridDim.x) * blockDim.x) {
         uint64_t ds = desc[i];
         if (desc_len(ds) != 2 || (dropped && dropped[i])) continue;
-        const int32_t* c = arena + desc_off(ds);
+        const int32_t* c = arena + desc_off(ds) + kHdr;
         int32_t u = c[0], v = c[1];
         adj[adj_off[u] + atomicAdd(fill + u, 1)] = v;
         adj[adj_off[v] + atomicAdd(fill + v, 1)] = u;

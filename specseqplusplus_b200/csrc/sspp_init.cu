@@ -180,18 +180,21 @@ __global__ void k_scatter_cols(int64_t n, const int64_t* colptr, const int32_t* 
         const int dj = dims[j];
         bool bad = len < 0 || len > kMaxColLen;
         int32_t prev = -1;
+        int32_t* data = arena + o + kHdr;
         for (int64_t k = 0; k < len && !bad; k++) {
             int32_t r = rows[b + k];
             if (r < 0 || r >= n || r <= prev || dims[r] != dj - 1) { bad = true; break; }
             prev = r;
-            arena[o + k] = newidx[r];
+            data[k] = newidx[r];
         }
         if (bad) {
             atomicOr(err, ERRB_BAD_INPUT);
             desc[i] = pack_desc(uint64_t(o), 0);
+            *reinterpret_cast<int4*>(arena + o) = make_int4(0, int32_t(i), 0, 0);
         } else {
-            for (int64_t k = len; k < pad4(len); k++) arena[o + k] = INT_MAX;
+            for (int64_t k = len; k < pad4(len); k++) data[k] = INT_MAX;
             desc[i] = pack_desc(uint64_t(o), uint32_t(len));
+            *reinterpret_cast<int4*>(arena + o) = make_int4(int32_t(len), int32_t(i), 0, 0);
         }
         leftmost[i] = INT_MAX;
     }
@@ -209,7 +212,7 @@ int reorder(Device& D, cudaStream_t s) {
     const int64_t* colptr = D.in_colptr;
     const int32_t* perm = D.perm;
     int64_t* off = D.scratch64;
-    scan([=] __device__(int64_t i) -> int64_t { int32_t j = perm[i]; return pad4(colptr[j + 1] - colptr[j]); },
+    scan([=] __device__(int64_t i) -> int64_t { int32_t j = perm[i]; return slot_ints(colptr[j + 1] - colptr[j]); },
          [=] __device__(int64_t i, int64_t pre, int64_t) { off[i] = pre; }, n, D.blk, s);
     k_scatter_cols<<<grid_for(n, 256) > 65536 ? 65536 : grid_for(n, 256), 256, 0, s>>>(
         n, D.in_colptr, D.in_rows, D.in_dims, D.perm, D.newidx, off, D.arena, D.desc, D.leftmost, D.err);
@@ -218,33 +221,33 @@ int reorder(Device& D, cudaStream_t s) {
 
 // ------------------------------------------------------------- init passes
 __global__ void k_init_low(int64_t n, const int32_t* arena, const uint64_t* desc, int32_t* low, int32_t* leftmost,
-                           int32_t* pivot, uint8_t* cleared, uint8_t* negative) {
+                           uint64_t* pivot, uint8_t* cleared, uint8_t* negative) {
     for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
         uint64_t d = desc[i];
-        const int32_t* c = arena + desc_off(d);
+        const int32_t* c = arena + desc_off(d) + kHdr;
         uint32_t len = desc_len(d);
         low[i] = len ? c[len - 1] : -1;
         for (uint32_t k = 0; k < len; k++) atomicMin(&leftmost[c[k]], int32_t(i));
-        pivot[i] = -1;
+        pivot[i] = kNoOwner;
         cleared[i] = 0;
         negative[i] = 0;
     }
 }
 
 __global__ void k_init_apparent(int64_t n, const int32_t* arena, const uint64_t* desc, const int32_t* low,
-                                const int32_t* leftmost, int32_t* pivot, uint8_t* cleared, uint8_t* negative,
+                                const int32_t* leftmost, uint64_t* pivot, uint8_t* cleared, uint8_t* negative,
                                 long long* counters) {
     long long app = 0;
     for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
         int32_t l = low[i];
         if (l < 0) continue;
         cleared[l] = 1;  // the youngest facet of any simplex is positive
+        uint64_t d = desc[i];
         if (leftmost[l] == int32_t(i)) {
-            pivot[l] = int32_t(i);  // no earlier column can ever reach row l
+            pivot[l] = pv_pack(int32_t(i), desc_off(d));  // no earlier column can ever reach row l
             app++;
         }
-        uint64_t d = desc[i];
-        const int32_t* c = arena + desc_off(d);
+        const int32_t* c = arena + desc_off(d) + kHdr;
         uint32_t len = desc_len(d);
         for (uint32_t k = 0; k < len; k++)
             if (leftmost[c[k]] == int32_t(i)) { negative[i] = 1; break; }
@@ -254,23 +257,26 @@ __global__ void k_init_apparent(int64_t n, const int32_t* arena, const uint64_t*
 }
 
 // Clears positive columns and removes negative rows in place.
-__global__ void k_init_compress(int64_t n, int32_t* arena, uint64_t* desc, int32_t* low, const int32_t* pivot,
+__global__ void k_init_compress(int64_t n, int32_t* arena, uint64_t* desc, int32_t* low, const uint64_t* pivot,
                                 const uint8_t* cleared, const uint8_t* negative, uint8_t* state,
                                 const uint8_t* dropped, long long* counters, int* err) {
     long long ncl = 0, nact = 0;
     for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
         uint64_t d = desc[i];
-        int32_t* c = arena + desc_off(d);
+        int32_t* hdr = arena + desc_off(d);
+        int32_t* c = hdr + kHdr;
         uint32_t len = desc_len(d);
         if (dropped && dropped[i]) {
             desc[i] = pack_desc(desc_off(d), 0);
+            hdr[0] = 0;
             low[i] = -1;
             state[i] = ST_DROPPED;
             continue;
         }
         if (cleared[i]) {
-            if (len && pivot[low[i]] == int32_t(i)) atomicOr(err, ERRB_BAD_INPUT);  // positive and negative at once
+            if (len && pv_col(pivot[low[i]]) == int32_t(i)) atomicOr(err, ERRB_BAD_INPUT);  // positive and negative
             desc[i] = pack_desc(desc_off(d), 0);
+            hdr[0] = 0;
             low[i] = -1;
             state[i] = ST_CLEARED;
             ncl++;
@@ -283,9 +289,10 @@ __global__ void k_init_compress(int64_t n, int32_t* arena, uint64_t* desc, int32
         }
         for (uint32_t k = m; k < len; k++) c[k] = INT_MAX;
         desc[i] = pack_desc(desc_off(d), m);
+        hdr[0] = int32_t(m);
         int32_t l = m ? c[m - 1] : -1;
         low[i] = l;
-        uint8_t st = (m == 0) ? ST_ZERO : (pivot[l] == int32_t(i) ? ST_OWNER : ST_ACTIVE);
+        uint8_t st = (m == 0) ? ST_ZERO : (pv_col(pivot[l]) == int32_t(i) ? ST_OWNER : ST_ACTIVE);
         state[i] = st;
         nact += (st == ST_ACTIVE);
     }
@@ -309,7 +316,7 @@ __global__ void k_dim_rows(int64_t n, const int32_t* rdim, const int32_t* arena,
         uint32_t len = desc_len(d);
         if (!len) continue;
         int dm = rdim[i];
-        atomicMin(&smin[dm], arena[desc_off(d)]);
+        atomicMin(&smin[dm], arena[desc_off(d) + kHdr]);
         if (state[i] == ST_ACTIVE) atomicMax(&smax[dm], low[i] + 1);
     }
     __syncthreads();
@@ -377,11 +384,12 @@ int active_list(Device& D, cudaStream_t s) {
 // dual: the dual row r' owned by dual column c' maps back to the primal pair
 // (n-1-c', n-1-r') of the dualized matrix's own numbering; `dual_to_input`
 // then maps those primal reordered indices to input indices.
-__global__ void k_pairs_scatter(int64_t n, const int32_t* pivot, const int32_t* perm, int64_t* death_of,
+__global__ void k_pairs_scatter(int64_t n, const uint64_t* pivot, const int32_t* perm, int64_t* death_of,
                                 uint8_t* paired, int dual) {
     for (int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; r < n; r += int64_t(gridDim.x) * blockDim.x) {
-        int32_t c = pivot[r];
-        if (c < 0) continue;
+        uint64_t e = pivot[r];
+        if (e == kNoOwner) continue;
+        int32_t c = pv_col(e);
         int64_t birth, death;
         if (!dual) {
             birth = perm[r];

@@ -23,16 +23,30 @@ enum : uint8_t {
     ST_HEAVY = 5,    // handed from the warp tier to the CTA tier
 };
 
-// A column is stored in the arena at a 16-byte aligned offset, padded with
-// INT32_MAX to a multiple of four ints.  Its descriptor packs
-// (offset in ints << 24) | length.
+// A column version occupies an arena slot at a 16-byte aligned offset: a
+// 16-byte header {length, column, 0, 0} followed by the sorted row indices,
+// padded with INT32_MAX to a multiple of four ints.  A column's descriptor
+// packs (slot offset in ints << 24) | length.
 constexpr int kLenBits = 24;
 constexpr uint64_t kLenMask = (1ull << kLenBits) - 1;
 constexpr int64_t kMaxColLen = int64_t(kLenMask);
+constexpr int kHdr = 4;  // header ints
 __host__ __device__ inline uint64_t pack_desc(uint64_t off, uint32_t len) { return (off << kLenBits) | len; }
 __host__ __device__ inline uint64_t desc_off(uint64_t d) { return d >> kLenBits; }
 __host__ __device__ inline uint32_t desc_len(uint64_t d) { return uint32_t(d & kLenMask); }
 __host__ __device__ inline int64_t pad4(int64_t x) { return (x + 3) & ~int64_t(3); }
+__host__ __device__ inline int64_t slot_ints(int64_t len) { return kHdr + pad4(len); }
+
+// Pivot table entry of a row: the owning column (31 bits) and the arena slot
+// of the owner's version (in 16-byte units, 33 bits), so a reader reaches the
+// owner's entries with one dependent load.  No owner = all ones, which reads
+// as a column index larger than any column.
+constexpr uint64_t kNoOwner = ~0ull;
+__host__ __device__ inline uint64_t pv_pack(int32_t col, uint64_t slot_off_ints) {
+    return ((slot_off_ints >> 2) << 31) | uint64_t(uint32_t(col));
+}
+__host__ __device__ inline int32_t pv_col(uint64_t e) { return int32_t(e & 0x7fffffffu); }
+__host__ __device__ inline uint64_t pv_slot(uint64_t e) { return (e >> 31) << 2; }  // slot offset in ints
 
 // Error word bits set by kernels (device int).
 enum : int {
@@ -40,6 +54,7 @@ enum : int {
     ERRB_CAPACITY = 2,
     ERRB_TIMEOUT = 4,
     ERRB_LEN = 8,       // a column exceeded kMaxColLen
+    ERRB_CHECK = 16,    // a self-check of the reduction failed (bad index skipped)
 };
 
 // Per-dimension summary after the init passes (in reordered numbering).
@@ -88,7 +103,7 @@ struct Device {
     unsigned long long* arena_top = nullptr;
     uint64_t* desc = nullptr;
     int32_t* low = nullptr;
-    int32_t* pivot = nullptr;
+    uint64_t* pivot = nullptr;   // [n] pivot entries (see pv_pack)
     uint8_t* state = nullptr;
     uint8_t* cleared = nullptr;
     uint8_t* negative = nullptr;
@@ -102,8 +117,10 @@ struct Device {
     DimInfo* diminfo = nullptr;
     int* err = nullptr;
     long long* counters = nullptr;
-    int* step_ctr = nullptr;     // per-step work counters (3 ints per step)
-    int32_t* heavy = nullptr;    // [n] columns handed to the CTA tier
+    int* step_ctr = nullptr;     // per-step work counters (4 ints per step)
+    int32_t* heavy = nullptr;    // pool of columns handed to the CTA tier, appended step after step
+    int64_t pool_cap = 0;
+    int* pool_tail = nullptr;
     int64_t cap_steps = 0;
     // pairs output (input indices)
     int64_t* death_of = nullptr;   // [n]

@@ -22,9 +22,11 @@ int init_compress(Device& D, const uint8_t* dropped, cudaStream_t s);
 int active_list(Device& D, cudaStream_t s);
 int extract_pairs(Device& D, int dual, const uint8_t* dropped, cudaStream_t s);
 
-cudaError_t reduce_configure(int cap1, int cap2, int* light_blocks_per_sm, int* heavy_blocks_per_sm);
+cudaError_t reduce_configure(int cap1, int cap2, int heavy_threads, int* light_blocks_per_sm,
+                             int* heavy_blocks_per_sm);
 void reduce_light_launch(const Device& D, const int32_t* active, int32_t beg, int32_t end, int32_t minrow, int cap,
-                         int* ctr, int grid, cudaStream_t s);
-void reduce_heavy_launch(const Device& D, int32_t minrow, int cap, int* ctr, int grid, cudaStream_t s);
+                         int chunk, int* ctr, int grid, cudaStream_t s);
+void heavy_slice_mark(const Device& D, int* ctr_k, int* ctr_next, cudaStream_t s);
+void reduce_heavy_launch(const Device& D, int cap, int threads, int* ctr, int grid, cudaStream_t s);
 
 }  // namespace sspp

@@ -15,23 +15,28 @@
 // and beyond that in exact-size arena buffers.  Both tiers run the same
 // column routine, written once over a "group" (warp or CTA).
 //
-// Merge.  Each addition stages the pivot column into shared memory with
-// 16-byte vector loads and merges the two sorted index lists (symmetric
-// difference: equal indices cancel) by rank: an element's output slot is its
-// own index plus its rank in the other list minus twice the cancelled pairs
-// before it (ballot + popcount prefix), so no atomics and no global scratch.
+// Pivot table.  pivot[row] holds the owning column and the arena slot of the
+// owner's version (pv_pack), so the owner's entries are one dependent load
+// away.  A column whose lowest row L has no owner, or an owner with a larger
+// index, publishes its current entries (fresh arena slot, then its
+// descriptor) and claims L with a 64-bit compare-and-swap.  Published column
+// versions are never modified afterwards, so a reader holding an older entry
+// still adds a valid earlier column with the same lowest row.  Displacing a
+// larger owner hands that owner to the displacing group, which reduces it
+// next (no other group can reach it), so there is no work queue to wait on and
+// no spin-wait at all.  Every addition adds an earlier column with the same
+// lowest row, so the result is a left-to-right reduction and the pairs equal
+// those of any sequential one.  Claiming a row also clears the row's own
+// column (twist clearing).
 //
-// Pivot table.  pivot[row] holds the column that owns the row (-1 = none).  A
-// column whose lowest row L has no owner, or an owner with a larger index,
-// publishes its current entries (fresh arena space, then its descriptor) and
-// claims L with a compare-and-swap.  Published column versions are never
-// modified afterwards, so a reader holding an older version still adds a valid
-// earlier column with the same lowest row.  Displacing a larger owner hands that
-// owner to the displacing group, which reduces it next (no other group can
-// reach it), so there is no work queue to wait on and no spin-wait at all.
-// Every addition adds an earlier column with the same lowest row, so the
-// result is a left-to-right reduction and the pairs equal those of any
-// sequential one.  Claiming a row also clears the row's own column (twist).
+// Addition.  The addend is staged into shared memory with 16-byte vector loads
+// (header and entries in one round when it fits).  The next lowest row is
+// known before the merge - it is the largest index at which the tops of the
+// two lists stop agreeing - so the pivot entry of that row is requested before
+// the merge starts and arrives while it runs.  The merge computes each
+// element's output slot from its rank in the other list minus twice the
+// cancelled pairs before it (one ballot/prefix per round for both lists): no
+// atomics, no scratch in global memory.
 #include <climits>
 
 #include "sspp_kernels.cuh"
@@ -40,25 +45,35 @@
 namespace sspp {
 
 struct ReduceArgs {
+    int32_t ncols;
     const int32_t* active;
     int32_t beg, end;
     int32_t minrow;
     int32_t cap;          // shared-memory capacity per buffer (ints), multiple of 32
+    int32_t chunk;        // light tier: window entries taken per fetch (1..32)
     int32_t* arena;
     int64_t arena_cap;
     unsigned long long* arena_top;
     uint64_t* desc;
     int32_t* low;
-    int32_t* pivot;
+    uint64_t* pivot;
     uint8_t* state;
     uint8_t* cleared;
-    int* ctr;             // [0] chunk counter, [1] heavy list length, [2] heavy pull counter
-    int32_t* heavy;       // heavy list
+    int* ctr;             // per step: [0] chunk counter, [1] [2] heavy pool range, [3] heavy pull counter
+    int32_t* heavy;       // heavy pool (columns handed to the CTA tier, appended in step order)
+    int* pool_tail;
+    int64_t pool_cap;
     int* err;
     long long* counters;
 };
 
 constexpr int kMaxMergesPerColumn = 1 << 24;
+
+__device__ __forceinline__ uint64_t ld_acquire_u64(const uint64_t* p) {
+    uint64_t v;
+    asm volatile("ld.acquire.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
 
 // ------------------------------------------------------------------ groups
 struct WarpG {
@@ -66,85 +81,170 @@ struct WarpG {
     __device__ __forceinline__ int rank() const { return threadIdx.x & 31; }
     __device__ __forceinline__ bool leader() const { return (threadIdx.x & 31) == 0; }
     __device__ __forceinline__ void sync() const { __syncwarp(); }
-    __device__ __forceinline__ int bcast(int v) const { return __shfl_sync(kFull, v, 0); }
-    __device__ __forceinline__ unsigned long long bcast64(unsigned long long v) const {
+    // __syncwarp orders the leader's preceding memory accesses (an acquire in
+    // particular) before the other lanes' following ones
+    __device__ __forceinline__ int bcast(int v) const {
+        __syncwarp();
         return __shfl_sync(kFull, v, 0);
     }
-    // exclusive count of f over lower ranks; tot = count over the group
-    __device__ __forceinline__ int prefix(bool f, int& tot) const {
-        unsigned m = __ballot_sync(kFull, f);
-        tot = __popc(m);
-        return __popc(m & lanemask_lt());
+    __device__ __forceinline__ unsigned long long bcast64(unsigned long long v) const {
+        __syncwarp();
+        return __shfl_sync(kFull, v, 0);
+    }
+    __device__ __forceinline__ unsigned long long bcast64_last(unsigned long long v) const {
+        __syncwarp();
+        return __shfl_sync(kFull, v, 31);
+    }
+    // exclusive counts of fa and fb over lower ranks, and their group totals
+    __device__ __forceinline__ void prefix2(bool fa, bool fb, int& pa, int& pb, int& ta, int& tb) const {
+        const unsigned lt = lanemask_lt();
+        unsigned ma = __ballot_sync(kFull, fa), mb = __ballot_sync(kFull, fb);
+        pa = __popc(ma & lt);
+        pb = __popc(mb & lt);
+        ta = __popc(ma);
+        tb = __popc(mb);
     }
     __device__ __forceinline__ int sum(int v) const { return warp_sum(v); }
+    // exclusive prefix of v over lower ranks; tot = group total
+    __device__ __forceinline__ int prefix_int(int v, int& tot) const {
+        int inc = warp_inclusive_scan(v);
+        tot = __shfl_sync(kFull, inc, 31);
+        return inc - v;
+    }
 };
 
 template <int T>
 struct BlockG {
     static constexpr int kSize = T;
     static constexpr int kWarps = T / 32;
-    int* sm;                  // kWarps + 2 ints
-    unsigned long long* sb;   // one 8-byte slot
+    int* sm;                  // 2 * (kWarps + 2) ints: two scan buffers, used alternately
+    unsigned long long* sb;   // two 8-byte broadcast slots, used alternately
+    mutable int slot = 0;
+    mutable int sbuf = 0;
+    // alternating buffers: buffer b is rewritten only two collectives later,
+    // after every thread has passed the barrier of the collective in between
+    __device__ __forceinline__ int* scan_buf() const {
+        int* b = sm + sbuf * (kWarps + 2);
+        sbuf ^= 1;
+        return b;
+    }
     __device__ __forceinline__ int rank() const { return threadIdx.x; }
     __device__ __forceinline__ bool leader() const { return threadIdx.x == 0; }
     __device__ __forceinline__ void sync() const { __syncthreads(); }
+    // one barrier: consecutive broadcasts alternate slots, and a slot is only
+    // rewritten after every thread has passed the following broadcast's barrier
     __device__ __forceinline__ unsigned long long bcast64(unsigned long long v) const {
-        if (threadIdx.x == 0) *sb = v;
+        unsigned long long* p = sb + slot;
+        slot ^= 1;
+        if (threadIdx.x == 0) *p = v;
         __syncthreads();
-        unsigned long long r = *sb;
-        __syncthreads();
-        return r;
+        return *p;
     }
     __device__ __forceinline__ int bcast(int v) const { return int(bcast64((unsigned long long)(unsigned)v)); }
-    __device__ __forceinline__ int prefix(bool f, int& tot) const {
+    __device__ __forceinline__ unsigned long long bcast64_last(unsigned long long v) const {
+        unsigned long long* p = sb + slot;
+        slot ^= 1;
+        if (threadIdx.x == T - 1) *p = v;
+        __syncthreads();
+        return *p;
+    }
+    __device__ __forceinline__ void prefix2(bool fa, bool fb, int& pa, int& pb, int& ta, int& tb) const {
         const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-        unsigned m = __ballot_sync(kFull, f);
-        if (lane == 0) sm[wid] = __popc(m);
+        const unsigned lt = lanemask_lt();
+        int* b = scan_buf();
+        unsigned ma = __ballot_sync(kFull, fa), mb = __ballot_sync(kFull, fb);
+        if (lane == 0) b[wid] = __popc(ma) | (__popc(mb) << 16);
         __syncthreads();
         if (wid == 0) {
-            int c = lane < kWarps ? sm[lane] : 0;
+            int c = lane < kWarps ? b[lane] : 0;
             int inc = warp_inclusive_scan(c);
-            if (lane < kWarps) sm[lane] = inc - c;
-            if (lane == kWarps - 1) sm[kWarps] = inc;
+            if (lane < kWarps) b[lane] = inc - c;
+            if (lane == kWarps - 1) b[kWarps] = inc;
         }
         __syncthreads();
-        int r = sm[wid] + __popc(m & lanemask_lt());
-        tot = sm[kWarps];
+        const int base = b[wid], tot = b[kWarps];
+        pa = (base & 0xffff) + __popc(ma & lt);
+        pb = (base >> 16) + __popc(mb & lt);
+        ta = tot & 0xffff;
+        tb = tot >> 16;
+    }
+    __device__ __forceinline__ int prefix_int(int v, int& tot) const {
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+        int* b = scan_buf();
+        int inc = warp_inclusive_scan(v);
+        if (lane == 31) b[wid] = inc;
         __syncthreads();
-        return r;
+        if (wid == 0) {
+            int c = lane < kWarps ? b[lane] : 0;
+            int ci = warp_inclusive_scan(c);
+            if (lane < kWarps) b[lane] = ci - c;
+            if (lane == kWarps - 1) b[kWarps] = ci;
+        }
+        __syncthreads();
+        tot = b[kWarps];
+        return b[wid] + inc - v;
     }
     __device__ __forceinline__ int sum(int v) const {
         const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+        int* b = scan_buf();
         int w = warp_sum(v);
-        if (lane == 0) sm[wid] = w;
+        if (lane == 0) b[wid] = w;
         __syncthreads();
         if (wid == 0) {
-            int c = lane < kWarps ? sm[lane] : 0;
+            int c = lane < kWarps ? b[lane] : 0;
             c = warp_sum(c);
-            if (lane == 0) sm[kWarps] = c;
+            if (lane == 0) b[kWarps] = c;
         }
         __syncthreads();
-        int r = sm[kWarps];
-        __syncthreads();
-        return r;
+        return b[kWarps];
     }
 };
 
 // --------------------------------------------------------------- list ops
-__device__ __forceinline__ int ldv(const int32_t* p, bool global) { return global ? __ldcg(p) : *p; }
+// List loads: shared-memory lists with ld.shared, arena lists through L2
+// (ld.global.cg: arena slots written by other SMs must not be served from a
+// stale L1 line).  The space of each list is a template parameter, so no load
+// carries a runtime branch or generic addressing.
+__device__ __forceinline__ int lds(const int32_t* p) {
+    int v;
+    asm volatile("ld.shared.b32 %0, [%1];" : "=r"(v) : "r"(unsigned(__cvta_generic_to_shared(p))));
+    return v;
+}
+template <bool GL>
+__device__ __forceinline__ int ld(const int32_t* p) {
+    if constexpr (GL) return __ldcg(p);
+    else return lds(p);
+}
+__device__ __forceinline__ int ldv(const int32_t* p, bool global) { return global ? __ldcg(p) : lds(p); }
+
+// calls F<ga, gb>(...) with the spaces known at compile time
+#define SSPP_DISPATCH2(ga, gb, CALL) \
+    ((ga) ? ((gb) ? CALL(true, true) : CALL(true, false)) : ((gb) ? CALL(false, true) : CALL(false, false)))
 
 // first index k in [0, n) with a[k] >= x
-__device__ __forceinline__ int lower_bound_v(const int32_t* a, int n, int x, bool g) {
+template <bool GL>
+__device__ __forceinline__ int lower_bound_t(const int32_t* a, int n, int x) {
     int lo = 0, hi = n;
     while (lo < hi) {
         int mid = (lo + hi) >> 1;
-        if (ldv(a + mid, g) < x) lo = mid + 1;
+        if (ld<GL>(a + mid) < x) lo = mid + 1;
         else hi = mid;
     }
     return lo;
 }
 
-// number of indices common to sorted lists a and b
+// number of indices common to sorted lists a and b (b is searched)
+template <class G, bool GA, bool GB>
+__device__ int count_common_t(const G& g, const int32_t* a, int na, const int32_t* b, int nb) {
+    int e = 0;
+    for (int i = g.rank(); i < na; i += G::kSize) {
+        int x = ld<GA>(a + i);
+        int r = lower_bound_t<GB>(b, nb, x);
+        e += (r < nb && ld<GB>(b + r) == x);
+    }
+    return g.sum(e);
+}
+
 template <class G>
 __device__ int count_common(const G& g, const int32_t* a, int na, bool ga, const int32_t* b, int nb, bool gb) {
     if (na > nb) {  // search the shorter list's elements in the longer one
@@ -152,60 +252,199 @@ __device__ int count_common(const G& g, const int32_t* a, int na, bool ga, const
         int tn = na; na = nb; nb = tn;
         bool tg = ga; ga = gb; gb = tg;
     }
-    int e = 0;
-    for (int i = g.rank(); i < na; i += G::kSize) {
-        int x = ldv(a + i, ga);
-        int r = lower_bound_v(b, nb, x, gb);
-        e += (r < nb && ldv(b + r, gb) == x);
-    }
-    return g.sum(e);
+#define SSPP_CC(A_, B_) count_common_t<G, A_, B_>(g, a, na, b, nb)
+    return SSPP_DISPATCH2(ga, gb, SSPP_CC);
+#undef SSPP_CC
 }
 
-// survivors of a (those not in b) go to out[i + rank_b(x) - 2 * cancelled_before(i)]
-template <class G>
-__device__ void scatter_side(const G& g, const int32_t* a, int na, bool ga, const int32_t* b, int nb, bool gb,
-                             int32_t* out, int out_len, int* err) {
-    int carry = 0;
-    for (int base = 0; base < na; base += G::kSize) {
-        int i = base + g.rank();
-        bool valid = i < na;
-        int x = valid ? ldv(a + i, ga) : 0;
-        int r = valid ? lower_bound_v(b, nb, x, gb) : 0;
-        bool eq = valid && r < nb && ldv(b + r, gb) == x;
-        int tot;
-        int before = carry + g.prefix(eq, tot);
-        if (valid && !eq) {
-            int pos = i + r - 2 * before;
-            if (pos >= 0 && pos < out_len) out[pos] = x;
+// out = a xor b (as index sets) in one pass over both lists.  Element a[i]
+// survives unless it is in b; it lands at i + rank_b(a[i]) - 2 * (cancelled
+// a's before i), symmetrically for b.  Writes stay below out_cap.  Returns the
+// output length and pads it to a multiple of four with INT_MAX.
+// Two lower-bound searches in lockstep (x in b, y in a): two independent load
+// chains per step.  Equality comes from the probe that last moved `hi` (the
+// final position was probed then), so no extra dependent load is needed.
+template <bool GA, bool GB>
+__device__ __forceinline__ void rank2(const int32_t* a, int na, const int32_t* b, int nb, int x, bool vx, int y, bool vy,
+                                      int& rx, bool& ex, int& ry, bool& ey) {
+    int lo1 = 0, hi1 = vx ? nb : 0, lo2 = 0, hi2 = vy ? na : 0;
+    int h1 = INT_MIN, h2 = INT_MIN;
+    while (lo1 < hi1 || lo2 < hi2) {
+        const bool s1 = lo1 < hi1, s2 = lo2 < hi2;
+        const int m1 = (lo1 + hi1) >> 1, m2 = (lo2 + hi2) >> 1;
+        const int v1 = s1 ? ld<GB>(b + m1) : 0;
+        const int v2 = s2 ? ld<GA>(a + m2) : 0;
+        if (s1) {
+            if (v1 < x) lo1 = m1 + 1;
+            else { hi1 = m1; h1 = v1; }
+        }
+        if (s2) {
+            if (v2 < y) lo2 = m2 + 1;
+            else { hi2 = m2; h2 = v2; }
+        }
+    }
+    rx = lo1;
+    ex = vx && lo1 < nb && h1 == x;
+    ry = lo2;
+    ey = vy && lo2 < na && h2 == y;
+}
+
+template <class G, bool GA, bool GB>
+__device__ int xor_merge(const G& g, const int32_t* a, int na, const int32_t* b, int nb, int32_t* out, int out_cap,
+                         int* err) {
+    int carry_a = 0, carry_b = 0;
+    const int n = na > nb ? na : nb;
+    for (int base = 0; base < n; base += G::kSize) {
+        const int i = base + g.rank();
+        const bool va = i < na, vb = i < nb;
+        const int x = va ? ld<GA>(a + i) : 0;
+        const int y = vb ? ld<GB>(b + i) : 0;
+        int ra, rb;
+        bool ea, eb;
+        rank2<GA, GB>(a, na, b, nb, x, va, y, vb, ra, ea, rb, eb);
+        int pa, pb, ta, tb;
+        g.prefix2(ea, eb, pa, pb, ta, tb);
+        if (va && !ea) {
+            int pos = i + ra - 2 * (carry_a + pa);
+            if (pos >= 0 && pos < out_cap) out[pos] = x;
             else atomicOr(err, ERRB_BAD_INPUT);  // inputs were not strictly increasing
         }
-        carry += tot;
+        if (vb && !eb) {
+            int pos = i + rb - 2 * (carry_b + pb);
+            if (pos >= 0 && pos < out_cap) out[pos] = y;
+            else atomicOr(err, ERRB_BAD_INPUT);
+        }
+        carry_a += ta;
+        carry_b += tb;
     }
-}
-
-template <class G>
-__device__ void xor_merge(const G& g, const int32_t* a, int na, bool ga, const int32_t* b, int nb, bool gb,
-                          int32_t* out, int out_len, int* err) {
-    scatter_side(g, a, na, ga, b, nb, gb, out, out_len, err);
-    scatter_side(g, b, nb, gb, a, na, ga, out, out_len, err);
-    // pad to a multiple of four with INT_MAX (keeps 16-byte vector loads in bounds)
-    if (g.rank() < int(pad4(out_len) - out_len)) out[out_len + g.rank()] = INT_MAX;
+    const int out_len = na + nb - 2 * carry_a;
+    const int padn = int(pad4(out_len) - out_len);
+    if (g.rank() < padn && out_len + g.rank() < out_cap) out[out_len + g.rank()] = INT_MAX;
     g.sync();
+    return out_len;
 }
 
-// global -> shared copy of a padded column (16-byte aligned on both sides)
+// Merge-path form of the same merge.  M = merge(a, b), a first on ties, so
+// every equal pair is adjacent in M as (a[i], b[j]).  Thread t owns positions
+// [tK, tK + K) of M per round: one binary search finds its split (i, j), a
+// short walk emits the elements of its positions that have no equal partner
+// (a pair cut by a slice boundary is dropped on both sides), and a group
+// prefix sum of the per-thread counts places them.  The walk runs twice
+// (count, then write) so nothing is held in registers.
+template <int K, bool GA, bool GB>
+__device__ __forceinline__ int path_walk(const int32_t* a, int na, const int32_t* b, int nb, int d0, int total,
+                                         int32_t* out, int out_off, int out_cap, bool emit, int* err) {
+    int lo = d0 - nb > 0 ? d0 - nb : 0, hi = d0 < na ? d0 : na;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (ld<GA>(a + mid - 1) <= ld<GB>(b + d0 - mid)) lo = mid;
+        else hi = mid - 1;
+    }
+    int i = lo, j = d0 - lo, pos = d0, cnt = 0;
+    const int end = d0 + K < total ? d0 + K : total;
+    // b[j] partners the element just before this slice (a[i-1])
+    if (pos < end && i > 0 && j < nb && ld<GA>(a + i - 1) == ld<GB>(b + j)) { j++; pos++; }
+    while (pos < end) {
+        const int x = i < na ? ld<GA>(a + i) : INT_MAX;
+        const int y = j < nb ? ld<GB>(b + j) : INT_MAX;
+        if (i < na && (j >= nb || x <= y)) {
+            if (j < nb && x == y) {  // equal pair: drop both (the partner may open the next slice)
+                i++;
+                pos++;
+                if (pos < end) { j++; pos++; }
+                continue;
+            }
+            if (emit) {
+                if (out_off + cnt < out_cap) out[out_off + cnt] = x;
+                else atomicOr(err, ERRB_BAD_INPUT);
+            }
+            cnt++;
+            i++;
+        } else {
+            if (emit) {
+                if (out_off + cnt < out_cap) out[out_off + cnt] = y;
+                else atomicOr(err, ERRB_BAD_INPUT);
+            }
+            cnt++;
+            j++;
+        }
+        pos++;
+    }
+    return cnt;
+}
+
+template <class G, int K, bool GA, bool GB>
+__device__ int xor_merge_path(const G& g, const int32_t* a, int na, const int32_t* b, int nb, int32_t* out,
+                              int out_cap, int* err) {
+    const int total = na + nb;
+    int written = 0;
+    for (int base = 0; base < total; base += G::kSize * K) {
+        const int d0 = base + g.rank() * K;
+        int cnt = d0 < total ? path_walk<K, GA, GB>(a, na, b, nb, d0, total, out, 0, out_cap, false, err) : 0;
+        int tot;
+        const int off = g.prefix_int(cnt, tot);
+        if (cnt) path_walk<K, GA, GB>(a, na, b, nb, d0, total, out, written + off, out_cap, true, err);
+        written += tot;
+    }
+    const int padn = int(pad4(written) - written);
+    if (g.rank() < padn && written + g.rank() < out_cap) out[written + g.rank()] = INT_MAX;
+    g.sync();
+    return written;
+}
+
 template <class G>
-__device__ __forceinline__ void stage(const G& g, int32_t* dst, const int32_t* src, int len) {
-    const int n4 = int(pad4(len)) >> 2;
+struct PathK;
+template <>
+struct PathK<WarpG> {
+    static constexpr int K = 4;
+};
+template <int T>
+struct PathK<BlockG<T>> {
+    static constexpr int K = 8;
+};
+
+// Rank form while both lists fit in two rounds of the group (one binary
+// search per element, all independent); merge-path beyond that, where the
+// per-element searches would take many rounds.
+template <class G, bool GA, bool GB>
+__device__ __forceinline__ int merge_t(const G& g, const int32_t* a, int na, const int32_t* b, int nb, int32_t* out,
+                                       int out_cap, int* err) {
+    if ((na > nb ? na : nb) <= 2 * G::kSize) return xor_merge<G, GA, GB>(g, a, na, b, nb, out, out_cap, err);
+    return xor_merge_path<G, PathK<G>::K, GA, GB>(g, a, na, b, nb, out, out_cap, err);
+}
+
+template <class G>
+__device__ int merge(const G& g, const int32_t* a, int na, bool ga, const int32_t* b, int nb, bool gb, int32_t* out,
+                     int out_cap, int* err) {
+#define SSPP_MG(A_, B_) merge_t<G, A_, B_>(g, a, na, b, nb, out, out_cap, err)
+    return SSPP_DISPATCH2(ga, gb, SSPP_MG);
+#undef SSPP_MG
+}
+
+// largest index of a xor b below their common top a[na-1] == b[nb-1]; -1 if none
+__device__ __forceinline__ int next_low(const int32_t* a, int na, bool ga, const int32_t* b, int nb, bool gb) {
+    int i = na - 2, j = nb - 2;
+    while (i >= 0 && j >= 0) {
+        int x = ldv(a + i, ga), y = ldv(b + j, gb);
+        if (x != y) return x > y ? x : y;
+        i--;
+        j--;
+    }
+    if (i >= 0) return ldv(a + i, ga);
+    if (j >= 0) return ldv(b + j, gb);
+    return -1;
+}
+
+// global -> shared copy of int4 units [k0, k1) of a slot
+template <class G>
+__device__ __forceinline__ void copy4(const G& g, int32_t* dst, const int32_t* src, int k0, int k1) {
     const int4* s4 = reinterpret_cast<const int4*>(src);
     int4* d4 = reinterpret_cast<int4*>(dst);
-    for (int k = g.rank(); k < n4; k += G::kSize) d4[k] = __ldcg(s4 + k);
-    g.sync();
+    for (int k = k0 + g.rank(); k < k1; k += G::kSize) d4[k] = __ldcg(s4 + k);
 }
 
 template <class G>
-__device__ __forceinline__ void store(const G& g, int32_t* dst, const int32_t* src, int len) {
-    const int n4 = int(pad4(len)) >> 2;
+__device__ __forceinline__ void store4(const G& g, int32_t* dst, const int32_t* src, int n4) {
     const int4* s4 = reinterpret_cast<const int4*>(src);
     int4* d4 = reinterpret_cast<int4*>(dst);
     for (int k = g.rank(); k < n4; k += G::kSize) d4[k] = s4[k];
@@ -228,10 +467,11 @@ __device__ __forceinline__ int64_t alloc(const G& g, const ReduceArgs& A, int64_
 
 // Working column of one group.
 struct Work {
-    int32_t* buf;      // current entries (shared or arena)
+    int32_t* buf;      // current entries (shared memory, or the data part of an arena slot)
     int len;
-    bool global;       // buf is an arena buffer
-    int64_t goff;      // arena offset of buf when global
+    bool global;       // buf lives in the arena
+    int64_t gslot;     // arena slot of buf when global
+    int64_t slot;      // arena slot of the published version
     bool dirty;        // differs from the published version
 };
 
@@ -239,21 +479,22 @@ struct Work {
 // arena is exhausted.
 template <class G>
 __device__ bool publish(const G& g, const ReduceArgs& A, int col, Work& w) {
-    int64_t off;
+    int64_t so;
     if (w.global) {
-        off = w.goff;
+        so = w.gslot;
     } else {
-        off = alloc(g, A, pad4(w.len));
-        if (off < 0) return false;
-        store(g, A.arena + off, w.buf, w.len);
-        if (g.leader()) cnt_add(&A.counters[CNT_PUBLISHED], (long long)pad4(w.len));
+        so = alloc(g, A, slot_ints(w.len));
+        if (so < 0) return false;
+        store4(g, A.arena + so + kHdr, w.buf, int(pad4(w.len)) >> 2);
+        if (g.leader()) cnt_add(&A.counters[CNT_PUBLISHED], (long long)slot_ints(w.len));
     }
+    if (g.leader()) *reinterpret_cast<int4*>(A.arena + so) = make_int4(w.len, col, 0, 0);
     g.sync();
     if (g.leader()) {
         __threadfence();
-        A.desc[col] = pack_desc(uint64_t(off), uint32_t(w.len));
+        A.desc[col] = pack_desc(uint64_t(so), uint32_t(w.len));
     }
-    g.sync();
+    w.slot = so;
     w.dirty = false;
     return true;
 }
@@ -265,7 +506,7 @@ enum Outcome { OUT_OWNER, OUT_ZERO, OUT_PARKED, OUT_DEFERRED, OUT_FAIL };
 // whose next addend or sum) exceed the shared capacity is published and
 // returned as OUT_DEFERRED for the heavy tier; without it such columns continue
 // in arena buffers.  *displaced receives the owner this column displaced (-1
-// if none).
+// if none).  sp holds kHdr + cap ints (staged addend with its header).
 template <class G>
 __device__ Outcome reduce_column(const G& g, const ReduceArgs& A, int col, int32_t* sw0, int32_t* sw1, int32_t* sp,
                                  bool defer, int* displaced) {
@@ -275,21 +516,39 @@ __device__ Outcome reduce_column(const G& g, const ReduceArgs& A, int col, int32
     d = g.bcast64(d);
     Work w;
     w.len = int(desc_len(d));
+    w.slot = int64_t(desc_off(d));
     w.dirty = false;
+    if (w.slot + slot_ints(w.len) > A.arena_cap) {  // self-check: descriptor inside the arena
+        if (g.leader()) atomicOr(A.err, ERRB_CHECK);
+        return OUT_FAIL;
+    }
     if (w.len <= A.cap) {
-        stage(g, sw0, A.arena + desc_off(d), w.len);
+        copy4(g, sw0, A.arena + w.slot + kHdr, 0, int(pad4(w.len)) >> 2);
+        g.sync();
         w.buf = sw0;
         w.global = false;
-        w.goff = 0;
+        w.gslot = 0;
     } else if (defer) {
         return OUT_DEFERRED;
     } else {
-        w.buf = A.arena + desc_off(d);
+        w.buf = A.arena + w.slot + kHdr;
         w.global = true;
-        w.goff = int64_t(desc_off(d));
+        w.gslot = w.slot;
     }
     long long adds = 0, add_ints = 0;
     Outcome res = OUT_FAIL;
+    int L = w.len ? ldv(w.buf + w.len - 1, w.global) : -1;
+    uint64_t e = kNoOwner;
+    if (L >= A.ncols) {  // self-check: row index in range
+        if (g.leader()) atomicOr(A.err, ERRB_CHECK);
+        return OUT_FAIL;
+    }
+    if (L >= A.minrow) {
+        if (g.leader()) e = ld_acquire_u64(A.pivot + L);
+        e = g.bcast64(e);
+    }
+    // speculative first staging round: header + as many entries as one pass of the group reads
+    const int first4 = min(G::kSize, (kHdr + A.cap) >> 2);
     for (int iter = 0;; iter++) {
         if (w.len == 0) {
             if (g.leader()) {
@@ -303,85 +562,117 @@ __device__ Outcome reduce_column(const G& g, const ReduceArgs& A, int col, int32
             if (g.leader()) atomicOr(A.err, ERRB_TIMEOUT);
             break;
         }
-        const int L = ldv(w.buf + w.len - 1, w.global);
         if (L < A.minrow) {
             if (w.dirty && !publish(g, A, col, w)) break;
             if (g.leader()) A.low[col] = L;
             res = OUT_PARKED;
             break;
         }
-        int p = 0;
-        if (g.leader()) p = ld_acquire(A.pivot + L);
-        p = g.bcast(p);
-        if (p < 0 || p > col) {
+        const int p = pv_col(e);
+        if (p > col) {  // no owner, or a larger one: claim the row
             if (w.dirty && !publish(g, A, col, w)) break;
-            int old = 0;
+            uint64_t old = 0;
             if (g.leader()) {
                 A.low[col] = L;
                 __threadfence();
-                old = atomicCAS(A.pivot + L, p, col);
+                old = atomicCAS(reinterpret_cast<unsigned long long*>(A.pivot + L), (unsigned long long)e,
+                                (unsigned long long)pv_pack(col, uint64_t(w.slot)));
             }
-            old = g.bcast(old);
-            if (old == p) {
+            old = g.bcast64(old);
+            if (old == e) {
                 if (g.leader()) {
-                    if (p < 0) A.cleared[L] = 1;  // twist clearing of the positive row column
+                    if (e == kNoOwner) A.cleared[L] = 1;  // twist clearing of the positive row column
                     else cnt_add(&A.counters[CNT_DISPLACED], 1ll);
                 }
-                *displaced = p;
+                *displaced = (e == kNoOwner) ? -1 : p;
                 res = OUT_OWNER;
                 break;
             }
-            continue;  // someone else changed the owner; look again
+            e = old;  // someone else changed the owner; look again
+            continue;
         }
-        // add column p (p < col, same lowest row)
+        // add the owner's version (p < col, same lowest row): stage header + entries
+        if (pv_slot(e) + kHdr > uint64_t(A.arena_cap)) {  // self-check: entry inside the arena
+            if (g.leader()) atomicOr(A.err, ERRB_CHECK);
+            break;
+        }
+        const int32_t* src = A.arena + pv_slot(e);
+        copy4(g, sp, src, 0, first4);
         g.sync();
-        uint64_t dp = 0;
-        if (g.leader()) dp = ld_cg_u64(A.desc + p);
-        dp = g.bcast64(dp);
-        const int plen = int(desc_len(dp));
+        const int plen = sp[0];
+        if (plen < 1 || plen > int(kMaxColLen) || sp[1] != p ||
+            int64_t(pv_slot(e)) + slot_ints(plen) > A.arena_cap) {  // self-check: header of the owner's version
+            if (g.leader()) atomicOr(A.err, ERRB_CHECK);
+            break;
+        }
         const int32_t* pb;
         bool pg;
         if (plen <= A.cap) {
-            stage(g, sp, A.arena + desc_off(dp), plen);
-            pb = sp;
+            const int n4 = (kHdr + int(pad4(plen))) >> 2;
+            if (n4 > first4) {
+                copy4(g, sp, src, first4, n4);
+                g.sync();
+            }
+            pb = sp + kHdr;
             pg = false;
         } else if (defer) {
             if (w.dirty && !publish(g, A, col, w)) break;
             res = OUT_DEFERRED;
             break;
         } else {
-            pb = A.arena + desc_off(dp);
+            pb = src + kHdr;
             pg = true;
         }
-        const int common = count_common(g, w.buf, w.len, w.global, pb, plen, pg);
-        const int out_len = w.len + plen - 2 * common;
-        if (out_len > int(kMaxColLen)) {
-            if (g.leader()) atomicOr(A.err, ERRB_LEN);
+        if (g.leader() && (plen == 0 || ldv(pb + plen - 1, pg) != L)) atomicOr(A.err, ERRB_BAD_INPUT);
+        // the next lowest row is known before the merge: request its pivot entry now
+        const int L2 = next_low(w.buf, w.len, w.global, pb, plen, pg);
+        if (L2 >= A.ncols) {  // self-check: row index in range
+            if (g.leader()) atomicOr(A.err, ERRB_CHECK);
             break;
         }
-        if (out_len > A.cap && defer) {
-            if (w.dirty && !publish(g, A, col, w)) break;
-            res = OUT_DEFERRED;
-            break;
-        }
-        adds++;
-        add_ints += w.len + plen + out_len;
-        if (out_len <= A.cap) {
+        // the group's last thread takes the entry: in short merges it holds no
+        // element, so its acquire load completes while the others merge
+        uint64_t pref = kNoOwner;
+        if (g.rank() == G::kSize - 1 && L2 >= A.minrow && L2 >= 0) pref = ld_acquire_u64(A.pivot + L2);
+        int out_len;
+        const int bound = w.len + plen - 2;
+        if (bound <= A.cap) {
             int32_t* dst = (w.global || w.buf == sw1) ? sw0 : sw1;
-            xor_merge(g, w.buf, w.len, w.global, pb, plen, pg, dst, out_len, A.err);
+            out_len = merge(g, w.buf, w.len, w.global, pb, plen, pg, dst, A.cap, A.err);
             w.buf = dst;
             w.global = false;
         } else {
-            int64_t off = alloc(g, A, pad4(out_len));
-            if (off < 0) break;
-            xor_merge(g, w.buf, w.len, w.global, pb, plen, pg, A.arena + off, out_len, A.err);
-            if (g.leader()) cnt_add(&A.counters[CNT_PUBLISHED], (long long)pad4(out_len));
-            w.buf = A.arena + off;
-            w.global = true;
-            w.goff = off;
+            const int common = count_common(g, w.buf, w.len, w.global, pb, plen, pg);
+            out_len = w.len + plen - 2 * common;
+            if (out_len > int(kMaxColLen)) {
+                if (g.leader()) atomicOr(A.err, ERRB_LEN);
+                break;
+            }
+            if (out_len <= A.cap) {
+                int32_t* dst = (w.global || w.buf == sw1) ? sw0 : sw1;
+                merge(g, w.buf, w.len, w.global, pb, plen, pg, dst, A.cap, A.err);
+                w.buf = dst;
+                w.global = false;
+            } else if (defer) {
+                if (w.dirty && !publish(g, A, col, w)) break;
+                res = OUT_DEFERRED;
+                break;
+            } else {
+                int64_t so = alloc(g, A, slot_ints(out_len));
+                if (so < 0) break;
+                merge(g, w.buf, w.len, w.global, pb, plen, pg, A.arena + so + kHdr, int(pad4(out_len)), A.err);
+                if (g.leader()) cnt_add(&A.counters[CNT_PUBLISHED], (long long)slot_ints(out_len));
+                w.buf = A.arena + so + kHdr;
+                w.global = true;
+                w.gslot = so;
+            }
         }
+        adds++;
+        add_ints += w.len + plen + out_len;
         w.len = out_len;
         w.dirty = true;
+        L = L2;
+        e = g.bcast64_last(pref);
     }
     if (g.leader() && adds) {
         cnt_add(&A.counters[CNT_ADDITIONS], adds);
@@ -397,10 +688,13 @@ __device__ __forceinline__ bool settle(const G& g, const ReduceArgs& A, int col,
         switch (o) {
             case OUT_OWNER: A.state[col] = ST_OWNER; break;
             case OUT_ZERO: A.state[col] = ST_ZERO; break;
-            case OUT_DEFERRED:
+            case OUT_DEFERRED: {
                 A.state[col] = ST_HEAVY;
-                A.heavy[atomicAdd(A.ctr + 1, 1)] = col;
+                int i = atomicAdd(A.pool_tail, 1);
+                if (i < A.pool_cap) A.heavy[i] = col;
+                else atomicOr(A.err, ERRB_CAPACITY);  // pool full: the run is repeated with a larger one
                 break;
+            }
             default: __threadfence(); st_release_u8(A.state + col, ST_ACTIVE); break;  // parked / failed
         }
     }
@@ -408,25 +702,26 @@ __device__ __forceinline__ bool settle(const G& g, const ReduceArgs& A, int col,
     return o != OUT_FAIL;
 }
 
-// Light tier: warps take chunks of 32 window entries and reduce the runnable
-// ones (active, not cleared, lowest row inside the band) one after another.
+// Light tier: warps take `chunk` window entries at a time and reduce the
+// runnable ones (active, not cleared, lowest row inside the band).
 __global__ void __launch_bounds__(128) k_reduce_light(ReduceArgs A) {
     extern __shared__ __align__(16) int32_t smem[];
     WarpG g;
     const int lane = g.rank();
-    int32_t* sw0 = smem + size_t(threadIdx.x >> 5) * 3 * A.cap;
+    int32_t* sw0 = smem + size_t(threadIdx.x >> 5) * (3 * A.cap + kHdr);
     int32_t* sw1 = sw0 + A.cap;
     int32_t* sp = sw1 + A.cap;
     const int count = A.end - A.beg;
+    const int chunk = A.chunk;
     while (true) {
         int base = 0;
-        if (lane == 0) base = atomicAdd(A.ctr, 32);
+        if (lane == 0) base = atomicAdd(A.ctr, chunk);
         base = g.bcast(base);
         if (base >= count) break;
         const int idx = A.beg + base + lane;
         int c = -1;
         bool run = false;
-        if (idx < A.end) {
+        if (lane < chunk && idx < A.end) {
             c = A.active[idx];
             run = ld_acquire_u8(A.state + c) == ST_ACTIVE && !ld_acquire_u8(A.cleared + c) &&
                   __ldcg(A.low + c) >= A.minrow;
@@ -447,23 +742,26 @@ __global__ void __launch_bounds__(128) k_reduce_light(ReduceArgs A) {
 }
 
 // Heavy tier: one CTA per deferred column, buffers of the level-2 capacity.
+// Like the reference's block phase (include/kernel.h:966-1060) it does not
+// stop at the band: a column handed over is reduced until it owns its lowest
+// row or becomes zero.
 template <int T>
-__global__ void __launch_bounds__(T) k_reduce_heavy(ReduceArgs A) {
+__global__ void __launch_bounds__(T, 1) k_reduce_heavy(ReduceArgs A) {
     extern __shared__ __align__(16) int32_t smem[];
-    __shared__ int gsm[T / 32 + 2];
-    __shared__ unsigned long long gsb;
+    __shared__ int gsm[2 * (T / 32 + 2)];
+    __shared__ unsigned long long gsb[2];
     BlockG<T> g;
     g.sm = gsm;
-    g.sb = &gsb;
+    g.sb = gsb;
     int32_t* sw0 = smem;
     int32_t* sw1 = sw0 + A.cap;
     int32_t* sp = sw1 + A.cap;
-    const int nheavy = __ldcg(A.ctr + 1);
+    const int hb = __ldcg(A.ctr + 1), he = __ldcg(A.ctr + 2);
     while (true) {
         int k = 0;
-        if (g.leader()) k = atomicAdd(A.ctr + 2, 1);
+        if (g.leader()) k = hb + atomicAdd(A.ctr + 3, 1);
         k = g.bcast(k);
-        if (k >= nheavy) break;
+        if (k >= he) break;
         int col = __ldcg(A.heavy + k);
         while (col >= 0) {
             int next = -1;
@@ -474,19 +772,19 @@ __global__ void __launch_bounds__(T) k_reduce_heavy(ReduceArgs A) {
     }
 }
 
-constexpr int kHeavyThreads = 256;
-
-int light_smem_bytes(int cap) { return 4 * 3 * cap * 4; }
-int heavy_smem_bytes(int cap) { return 3 * cap * 4; }
+int light_smem_bytes(int cap) { return 4 * (3 * cap + kHdr) * 4; }
+int heavy_smem_bytes(int cap) { return (3 * cap + kHdr) * 4; }
 
 static ReduceArgs make_args(const Device& D, const int32_t* active, int32_t beg, int32_t end, int32_t minrow, int cap,
-                            int* ctr) {
+                            int chunk, int* ctr) {
     ReduceArgs A;
+    A.ncols = int32_t(D.n);
     A.active = active;
     A.beg = beg;
     A.end = end;
     A.minrow = minrow;
     A.cap = cap;
+    A.chunk = chunk;
     A.arena = D.arena;
     A.arena_cap = D.arena_cap;
     A.arena_top = D.arena_top;
@@ -497,32 +795,53 @@ static ReduceArgs make_args(const Device& D, const int32_t* active, int32_t beg,
     A.cleared = D.cleared;
     A.ctr = ctr;
     A.heavy = D.heavy;
+    A.pool_tail = D.pool_tail;
+    A.pool_cap = D.pool_cap;
     A.err = D.err;
     A.counters = D.counters;
     return A;
 }
 
 void reduce_light_launch(const Device& D, const int32_t* active, int32_t beg, int32_t end, int32_t minrow, int cap,
-                         int* ctr, int grid, cudaStream_t s) {
-    k_reduce_light<<<grid, 128, light_smem_bytes(cap), s>>>(make_args(D, active, beg, end, minrow, cap, ctr));
+                         int chunk, int* ctr, int grid, cudaStream_t s) {
+    k_reduce_light<<<grid, 128, light_smem_bytes(cap), s>>>(make_args(D, active, beg, end, minrow, cap, chunk, ctr));
 }
 
-void reduce_heavy_launch(const Device& D, int32_t minrow, int cap, int* ctr, int grid, cudaStream_t s) {
-    k_reduce_heavy<kHeavyThreads><<<grid, kHeavyThreads, heavy_smem_bytes(cap), s>>>(
-        make_args(D, nullptr, 0, 0, minrow, cap, ctr));
+// step k's slice of the heavy pool ends where the pool tail is now; the next step's slice starts there
+__global__ void k_pool_mark(const int* pool_tail, int* ctr_k, int* ctr_next) {
+    int t = *pool_tail;
+    ctr_k[2] = t;
+    if (ctr_next) ctr_next[1] = t;
 }
 
-cudaError_t reduce_configure(int cap1, int cap2, int* light_blocks_per_sm, int* heavy_blocks_per_sm) {
+void heavy_slice_mark(const Device& D, int* ctr_k, int* ctr_next, cudaStream_t s) {
+    k_pool_mark<<<1, 1, 0, s>>>(D.pool_tail, ctr_k, ctr_next);
+}
+
+void reduce_heavy_launch(const Device& D, int cap, int threads, int* ctr, int grid, cudaStream_t s) {
+    ReduceArgs A = make_args(D, nullptr, 0, 0, INT32_MIN, cap, 1, ctr);
+    if (threads == 256) k_reduce_heavy<256><<<grid, 256, heavy_smem_bytes(cap), s>>>(A);
+    else k_reduce_heavy<128><<<grid, 128, heavy_smem_bytes(cap), s>>>(A);
+}
+
+cudaError_t reduce_configure(int cap1, int cap2, int heavy_threads, int* light_blocks_per_sm,
+                             int* heavy_blocks_per_sm) {
     cudaError_t e = cudaFuncSetAttribute(k_reduce_light, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          light_smem_bytes(cap1));
     if (e != cudaSuccess) return e;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(light_blocks_per_sm, k_reduce_light, 128, light_smem_bytes(cap1));
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k_reduce_heavy<kHeavyThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             heavy_smem_bytes(cap2));
+    if (heavy_threads == 256) {
+        e = cudaFuncSetAttribute(k_reduce_heavy<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 heavy_smem_bytes(cap2));
+        if (e != cudaSuccess) return e;
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(heavy_blocks_per_sm, k_reduce_heavy<256>, 256,
+                                                             heavy_smem_bytes(cap2));
+    }
+    e = cudaFuncSetAttribute(k_reduce_heavy<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, heavy_smem_bytes(cap2));
     if (e != cudaSuccess) return e;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(heavy_blocks_per_sm, k_reduce_heavy<kHeavyThreads>,
-                                                         kHeavyThreads, heavy_smem_bytes(cap2));
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(heavy_blocks_per_sm, k_reduce_heavy<128>, 128,
+                                                         heavy_smem_bytes(cap2));
 }
 
 }  // namespace sspp

@@ -38,7 +38,7 @@ class _Params(ctypes.Structure):
     _fields_ = [("dualize", ctypes.c_int32), ("model", ctypes.c_int32), ("max_iteration", ctypes.c_int32),
                 ("ss_block_size", ctypes.c_int32), ("growth", ctypes.c_float), ("queue_size", ctypes.c_int32),
                 ("level1_capacity", ctypes.c_int32), ("level2_capacity", ctypes.c_int32),
-                ("autotune", ctypes.c_int32)]
+                ("autotune", ctypes.c_int32), ("heavy_threads", ctypes.c_int32)]
 
 
 class _Stats(ctypes.Structure):
@@ -63,6 +63,7 @@ class Params:
     level1_capacity: int = 1000
     level2_capacity: int = 8000
     autotune: int = 0
+    heavy_threads: int = 0
 
     def _c(self) -> _Params:
         return _Params(*(getattr(self, f.name) for f in fields(self)))
