@@ -138,6 +138,23 @@ int32_t sspp_write_pairs(sspp_ctx* ctx, const char* path, int32_t fmt);
 
 int32_t sspp_get_stats(const sspp_ctx* ctx, sspp_stats* out);
 
+/* No counterpart in the reference.  Allocation-free reduction for callers that
+ * cannot have a library allocate device memory (a server that reserves all of
+ * its GPU memory up front; a multi-stream pipeline that cannot afford the
+ * device-wide synchronisation of cudaMalloc/cudaFree).  All working memory is
+ * one 64 MiB file-scope device array that every GPU loading this library holds
+ * until exit.  Inputs (filtration order, as sspp_load_csc) and outputs are
+ * device pointers: d_pairs receives up to ncols (birth, death) int64 pairs
+ * sorted by birth (room for 2 * ncols int64), *d_npairs their number.  Limits:
+ * ncols <= 1048576 and 3 * ncols + nnz <= 12582896, else SSPP_ERR_BAD_INPUT;
+ * fill-in beyond the array gives SSPP_ERR_CAPACITY.  The first call on a device
+ * looks up the array's address (make it before any stream capture); calls that
+ * overlap on the GPU share the array and race, so serialise them.  Blocks until
+ * done; a message is written to err_msg (may be NULL) when it fails. */
+int32_t sspp_reduce_noalloc(int64_t ncols, int64_t nnz, const int32_t* d_dims, const int64_t* d_col_ptr,
+                            const int32_t* d_rows, int64_t* d_pairs, int64_t* d_npairs, void* stream, char* err_msg,
+                            int32_t err_cap);
+
 #ifdef __cplusplus
 }
 #endif

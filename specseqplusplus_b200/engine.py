@@ -98,6 +98,7 @@ def load_library():
         "sspp_essentials": (i64, [vp, vp, i64]),
         "sspp_write_pairs": (i32, [vp, ctypes.c_char_p, i32]),
         "sspp_get_stats": (i32, [vp, ctypes.POINTER(_Stats)]),
+        "sspp_reduce_noalloc": (i32, [i64, i64, vp, vp, vp, vp, vp, vp, ctypes.c_char_p, i32]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -109,7 +110,8 @@ def load_library():
 
 EXPORTED = ("sspp_create", "sspp_destroy", "sspp_last_error", "sspp_default_params", "sspp_load_phat",
             "sspp_load_csc", "sspp_load_csc_device", "sspp_init", "sspp_compute", "sspp_reduce", "sspp_num_pairs",
-            "sspp_pairs", "sspp_num_essential", "sspp_essentials", "sspp_write_pairs", "sspp_get_stats")
+            "sspp_pairs", "sspp_num_essential", "sspp_essentials", "sspp_write_pairs", "sspp_get_stats",
+            "sspp_reduce_noalloc")
 
 
 class Engine:
@@ -200,6 +202,21 @@ class Engine:
         st = _Stats()
         self._check(self._lib.sspp_get_stats(self._h, ctypes.byref(st)))
         return {k: getattr(st, k) for k, _ in _Stats._fields_}
+
+
+def reduce_noalloc(ncols: int, nnz: int, d_dims: int, d_col_ptr: int, d_rows: int, d_pairs: int, d_npairs: int,
+                   stream: int = 0) -> None:
+    """Allocation-free reduction on device buffers (sspp_reduce_noalloc in include/sspp.h).
+
+    For callers that must not have the library allocate device memory: all
+    working memory is a fixed 64 MiB device array owned by the library.  All
+    pointers are device addresses; d_pairs needs room for 2 * ncols int64.
+    """
+    lib = load_library()
+    msg = ctypes.create_string_buffer(256)
+    rc = lib.sspp_reduce_noalloc(ncols, nnz, d_dims, d_col_ptr, d_rows, d_pairs, d_npairs, stream or None, msg, 256)
+    if rc != OK:
+        raise SsppError(rc, msg.value.decode(errors="replace"))
 
 
 def compute_persistence_pairs(m, params: Params | None = None, device: int = 0):
