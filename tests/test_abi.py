@@ -55,3 +55,13 @@ def test_no_oracle_on_product_path():
             if f.endswith((".py", ".cu", ".cpp", ".h", ".cuh")):
                 text = open(os.path.join(dirpath, f)).read()
                 assert "import oracle" not in text and "liboracle" not in text, f
+
+
+def test_cpp_mirror_header_compiles(tmp_path):
+    # the reference-side swap: a main in the reference's style against include/specseq_b200.hpp
+    out = tmp_path / "mirror"
+    r = subprocess.run(["g++", "-std=c++17", "-O1", "-I", os.path.join(ROOT, "include"),
+                        os.path.join(ROOT, "tests", "cpp", "mirror_main.cpp"), "-o", str(out),
+                        "-L", os.path.dirname(LIB), "-lsspp", "-Wl,-rpath," + os.path.dirname(LIB)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr

@@ -209,3 +209,15 @@ def test_highclear_lowerstar_and_2d():
         pairs, ess, st = run(m, Params(model=1, max_iteration=10))
         assert st["highclear_cleared"] == ref.stats["highclear"]
         assert np.array_equal(pairs, ref.pairs)
+
+
+def test_cpp_mirror_class_end_to_end(tmp_path):
+    exe = tmp_path / "mirror"
+    r = subprocess.run(["g++", "-std=c++17", "-O1", "-I", os.path.join(ROOT, "include"),
+                        os.path.join(ROOT, "tests", "cpp", "mirror_main.cpp"), "-o", str(exe),
+                        "-L", os.path.join(ROOT, "specseqplusplus_b200"), "-lsspp",
+                        "-Wl,-rpath," + os.path.join(ROOT, "specseqplusplus_b200")], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([str(exe), os.path.join(GOLD, "single_triangle.dat")], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    assert r.stdout == open(os.path.join(GOLD, "single_triangle_pairs.dat")).read()
