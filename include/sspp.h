@@ -133,6 +133,22 @@ int64_t sspp_pairs(sspp_ctx* ctx, int64_t* out_birth_death, int64_t cap);
 int64_t sspp_num_essential(sspp_ctx* ctx);
 int64_t sspp_essentials(sspp_ctx* ctx, int64_t* out, int64_t cap);
 
+/* Batching (no counterpart in the reference, which reduces one file per
+ * process).  k independent complexes, each with its own 0-based face indices,
+ * are loaded as one block-diagonal matrix: columns of different complexes
+ * never share rows, so one reduction yields every complex's pairs and all
+ * kernels drain the columns of all complexes from the same work counters.
+ * sspp_load_batch takes host arrays per complex; sspp_load_batch_device takes
+ * one device-resident concatenation whose face indices are already offset by
+ * the columns of the complexes before them.  After sspp_reduce, per-complex
+ * results come back in the complex's own indices. */
+int32_t sspp_load_batch(sspp_ctx* ctx, int32_t k, const int64_t* ncols, const int32_t* const* dims,
+                        const int64_t* const* col_ptr, const int32_t* const* rows);
+int32_t sspp_load_batch_device(sspp_ctx* ctx, int32_t k, const int64_t* ncols, const int32_t* d_dims,
+                               const int64_t* d_col_ptr, const int32_t* d_rows);
+int64_t sspp_batch_num_pairs(sspp_ctx* ctx, int32_t i);
+int64_t sspp_batch_pairs(sspp_ctx* ctx, int32_t i, int64_t* out_birth_death, int64_t cap);
+
 /* Replaces: writeVectorToFile (src/main.cu:191-229). */
 int32_t sspp_write_pairs(sspp_ctx* ctx, const char* path, int32_t fmt);
 

@@ -87,6 +87,11 @@ struct sspp_ctx {
     HighclearScratch hc;
     Prof prof;
     double ph_ms[PH_NUM] = {};
+    // batch: column range of each complex in the concatenated input, and the
+    // sorted pairs copied back once for slicing
+    std::vector<int64_t> batch_start;   // k + 1 entries (empty when not a batch)
+    std::vector<int64_t> host_pairs;
+    bool host_pairs_valid = false;
     int64_t launches = 0, light_launches = 0, heavy_launches = 0;
 };
 
@@ -358,6 +363,7 @@ int run_init(sspp_ctx* ctx) {
 
 int run_compute(sspp_ctx* ctx) {
     ctx->err.clear();
+    ctx->host_pairs_valid = false;
     Device& D = ctx->D;
     cudaStream_t s = ctx->stream;
     auto t0 = std::chrono::steady_clock::now();
@@ -483,6 +489,8 @@ int run_compute(sspp_ctx* ctx) {
 
 int load_common(sspp_ctx* ctx, int64_t n, int64_t nnz) {
     ctx->loaded = ctx->inited = ctx->computed = false;
+    ctx->batch_start.clear();
+    ctx->host_pairs_valid = false;
     int rc = ensure_columns(ctx, std::max<int64_t>(n, 1), std::max<int64_t>(nnz, 1));
     if (rc) return rc;
     ctx->D.n = n;
@@ -634,6 +642,107 @@ int32_t sspp_load_csc_device(sspp_ctx* ctx, int64_t ncols, const int32_t* d_dims
     ctx->D.in_rows = const_cast<int32_t*>(d_rows);
     ctx->loaded = true;
     return SSPP_OK;
+}
+
+int32_t sspp_load_batch(sspp_ctx* ctx, int32_t k, const int64_t* ncols, const int32_t* const* dims,
+                        const int64_t* const* col_ptr, const int32_t* const* rows) {
+    if (!ctx) return SSPP_ERR_BAD_INPUT;
+    if (k < 0 || (k > 0 && (!ncols || !dims || !col_ptr || !rows)))
+        return set_err(ctx, SSPP_ERR_BAD_INPUT, "null batch arrays");
+    int64_t n = 0, nnz = 0;
+    for (int32_t i = 0; i < k; i++) {
+        if (ncols[i] < 0 || !col_ptr[i] || (ncols[i] > 0 && !dims[i]))
+            return set_err(ctx, SSPP_ERR_BAD_INPUT, "bad batch member");
+        if (!validate_colptr(col_ptr[i], ncols[i]))
+            return set_err(ctx, SSPP_ERR_BAD_INPUT, "col_ptr must start at 0 and be non-decreasing");
+        n += ncols[i];
+        nnz += col_ptr[i][ncols[i]];
+    }
+    std::vector<int32_t> cd(size_t(std::max<int64_t>(n, 1)));
+    std::vector<int64_t> cp(size_t(n) + 1, 0);
+    std::vector<int32_t> cr(size_t(std::max<int64_t>(nnz, 1)));
+    std::vector<int64_t> starts(size_t(k) + 1, 0);
+    int64_t c0 = 0, e0 = 0;
+    for (int32_t i = 0; i < k; i++) {
+        const int64_t ni = ncols[i], ei = col_ptr[i][ni];
+        for (int64_t j = 0; j < ni; j++) {
+            cd[size_t(c0 + j)] = dims[i][j];
+            cp[size_t(c0 + j + 1)] = e0 + col_ptr[i][j + 1];
+        }
+        for (int64_t t = 0; t < ei; t++) cr[size_t(e0 + t)] = rows[i][t] + int32_t(c0);
+        c0 += ni;
+        e0 += ei;
+        starts[size_t(i) + 1] = c0;
+    }
+    int rc = sspp_load_csc(ctx, n, cd.data(), cp.data(), cr.data());
+    if (rc) return rc;
+    ctx->batch_start = starts;
+    return SSPP_OK;
+}
+
+int32_t sspp_load_batch_device(sspp_ctx* ctx, int32_t k, const int64_t* ncols, const int32_t* d_dims,
+                               const int64_t* d_col_ptr, const int32_t* d_rows) {
+    if (!ctx) return SSPP_ERR_BAD_INPUT;
+    if (k < 0 || (k > 0 && !ncols)) return set_err(ctx, SSPP_ERR_BAD_INPUT, "null batch sizes");
+    std::vector<int64_t> starts(size_t(k) + 1, 0);
+    for (int32_t i = 0; i < k; i++) {
+        if (ncols[i] < 0) return set_err(ctx, SSPP_ERR_BAD_INPUT, "negative batch member size");
+        starts[size_t(i) + 1] = starts[size_t(i)] + ncols[i];
+    }
+    int rc = sspp_load_csc_device(ctx, starts[size_t(k)], d_dims, d_col_ptr, d_rows);
+    if (rc) return rc;
+    ctx->batch_start = starts;
+    return SSPP_OK;
+}
+
+// pairs of complex i, in its own indices (the sorted global pairs are copied once)
+static int batch_slice(sspp_ctx* ctx, int32_t i, int64_t& b, int64_t& e) {
+    if (!ctx->computed || ctx->batch_start.empty() || i < 0 || i + 1 >= int32_t(ctx->batch_start.size()))
+        return SSPP_ERR_STATE;
+    if (!ctx->host_pairs_valid) {
+        const int64_t k = ctx->hcounters[CNT_NPAIRS];
+        ctx->host_pairs.resize(size_t(2 * k));
+        if (k > 0 && cudaMemcpy(ctx->host_pairs.data(), ctx->D.pairs, sizeof(int64_t) * 2 * k,
+                                cudaMemcpyDeviceToHost) != cudaSuccess)
+            return SSPP_ERR_CUDA;
+        ctx->host_pairs_valid = true;
+    }
+    const int64_t npairs = int64_t(ctx->host_pairs.size() / 2);
+    const int64_t lo = ctx->batch_start[size_t(i)], hi = ctx->batch_start[size_t(i) + 1];
+    auto first_at_least = [&](int64_t x) {  // first pair whose birth >= x
+        int64_t l = 0, h = npairs;
+        while (l < h) {
+            int64_t m = (l + h) / 2;
+            if (ctx->host_pairs[size_t(2 * m)] < x) l = m + 1;
+            else h = m;
+        }
+        return l;
+    };
+    b = first_at_least(lo);
+    e = first_at_least(hi);
+    return SSPP_OK;
+}
+
+int64_t sspp_batch_num_pairs(sspp_ctx* ctx, int32_t i) {
+    if (!ctx) return -1;
+    cudaSetDevice(ctx->cfg.device);
+    int64_t b, e;
+    if (batch_slice(ctx, i, b, e)) return -1;
+    return e - b;
+}
+
+int64_t sspp_batch_pairs(sspp_ctx* ctx, int32_t i, int64_t* out, int64_t cap) {
+    if (!ctx || cap < 0 || (!out && cap > 0)) return -1;
+    cudaSetDevice(ctx->cfg.device);
+    int64_t b, e;
+    if (batch_slice(ctx, i, b, e)) return -1;
+    const int64_t off = ctx->batch_start[size_t(i)];
+    const int64_t n = std::min(cap, e - b);
+    for (int64_t t = 0; t < n; t++) {
+        out[2 * t] = ctx->host_pairs[size_t(2 * (b + t))] - off;
+        out[2 * t + 1] = ctx->host_pairs[size_t(2 * (b + t) + 1)] - off;
+    }
+    return n;
 }
 
 int32_t sspp_load_phat(sspp_ctx* ctx, const char* path, int32_t fmt) {

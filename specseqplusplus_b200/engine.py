@@ -99,6 +99,10 @@ def load_library():
         "sspp_write_pairs": (i32, [vp, ctypes.c_char_p, i32]),
         "sspp_get_stats": (i32, [vp, ctypes.POINTER(_Stats)]),
         "sspp_reduce_noalloc": (i32, [i64, i64, vp, vp, vp, vp, vp, vp, ctypes.c_char_p, i32]),
+        "sspp_load_batch": (i32, [vp, i32, vp, vp, vp, vp]),
+        "sspp_load_batch_device": (i32, [vp, i32, vp, vp, vp, vp]),
+        "sspp_batch_num_pairs": (i64, [vp, i32]),
+        "sspp_batch_pairs": (i64, [vp, i32, vp, i64]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -111,7 +115,8 @@ def load_library():
 EXPORTED = ("sspp_create", "sspp_destroy", "sspp_last_error", "sspp_default_params", "sspp_load_phat",
             "sspp_load_csc", "sspp_load_csc_device", "sspp_init", "sspp_compute", "sspp_reduce", "sspp_num_pairs",
             "sspp_pairs", "sspp_num_essential", "sspp_essentials", "sspp_write_pairs", "sspp_get_stats",
-            "sspp_reduce_noalloc")
+            "sspp_reduce_noalloc", "sspp_load_batch", "sspp_load_batch_device", "sspp_batch_num_pairs",
+            "sspp_batch_pairs")
 
 
 class Engine:
@@ -151,6 +156,29 @@ class Engine:
 
     def load_csc_device(self, ncols: int, d_dims: int, d_col_ptr: int, d_rows: int) -> None:
         self._check(self._lib.sspp_load_csc_device(self._h, ncols, d_dims, d_col_ptr, d_rows))
+
+    def load_batch(self, matrices) -> None:
+        """k independent complexes reduced together (block-diagonal concatenation)."""
+        ms = list(matrices)
+        k = len(ms)
+        keep = [(np.ascontiguousarray(m.dims, dtype=np.int32), np.ascontiguousarray(m.col_ptr, dtype=np.int64),
+                 np.ascontiguousarray(m.rows if m.nnz else np.zeros(1, np.int32), dtype=np.int32)) for m in ms]
+        ncols = np.array([m.ncols for m in ms], dtype=np.int64)
+        arr = lambda i: (ctypes.c_void_p * max(k, 1))(*[t[i].ctypes.data for t in keep])
+        self._check(self._lib.sspp_load_batch(self._h, k, ncols.ctypes.data, arr(0), arr(1), arr(2)))
+
+    def load_batch_device(self, ncols, d_dims: int, d_col_ptr: int, d_rows: int) -> None:
+        nc = np.ascontiguousarray(ncols, dtype=np.int64)
+        self._check(self._lib.sspp_load_batch_device(self._h, nc.shape[0], nc.ctypes.data, d_dims, d_col_ptr, d_rows))
+
+    def batch_pairs(self, i: int) -> np.ndarray:
+        n = self._lib.sspp_batch_num_pairs(self._h, i)
+        if n < 0:
+            self._check(ERR_STATE)
+        out = np.empty((n, 2), dtype=np.int64)
+        if self._lib.sspp_batch_pairs(self._h, i, out.ctypes.data, n) != n:
+            self._check(ERR_CUDA)
+        return out
 
     def load_phat(self, path: str, fmt: int = ASCII) -> None:
         self._check(self._lib.sspp_load_phat(self._h, path.encode(), fmt))

@@ -221,3 +221,37 @@ def test_cpp_mirror_class_end_to_end(tmp_path):
     r = subprocess.run([str(exe), os.path.join(GOLD, "single_triangle.dat")], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
     assert r.stdout == open(os.path.join(GOLD, "single_triangle_pairs.dat")).read()
+
+
+def test_batch_matches_individual_reductions():
+    from specseqplusplus_b200 import workloads
+
+    mats, _ = workloads.batch_of_rips(24, seed=9, n_min=100, n_max=1200)
+    mats.append(gen.lowerstar(10, 1.0, 3))
+    mats.append(gen.BoundaryMatrix.from_columns([0, 0], [[], []]))
+    with Engine(0) as e:
+        e.load_batch(mats)
+        e.reduce(Params(model=1, max_iteration=10))
+        for i, m in enumerate(mats):
+            assert np.array_equal(e.batch_pairs(i), oracle.reduce(m).pairs), i
+
+
+def test_batch_device_concatenation():
+    torch = pytest.importorskip("torch")
+    mats = [gen.rips(300, 2, s, 0.12, 2) for s in range(5)]
+    dims = np.concatenate([m.dims for m in mats])
+    cps, rows, c0, e0 = [np.zeros(1, np.int64)], [], 0, 0
+    for m in mats:
+        cps.append(m.col_ptr[1:] + e0)
+        rows.append(m.rows + c0)
+        c0 += m.ncols
+        e0 += m.nnz
+    dev = torch.device("cuda", 0)
+    d_d = torch.from_numpy(dims).to(dev)
+    d_c = torch.from_numpy(np.concatenate(cps)).to(dev)
+    d_r = torch.from_numpy(np.concatenate(rows).astype(np.int32)).to(dev)
+    with Engine(0) as e:
+        e.load_batch_device([m.ncols for m in mats], d_d.data_ptr(), d_c.data_ptr(), d_r.data_ptr())
+        e.reduce(Params())
+        for i, m in enumerate(mats):
+            assert np.array_equal(e.batch_pairs(i), oracle.reduce(m).pairs)
