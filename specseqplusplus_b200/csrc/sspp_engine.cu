@@ -22,6 +22,7 @@
 #include "sspp_internal.h"
 #include "sspp_io.h"
 #include "sspp_launch.h"
+#include "sspp_xfer.h"
 
 using namespace sspp;
 
@@ -84,6 +85,9 @@ struct sspp_ctx {
     int64_t* own_colptr = nullptr;
     int32_t* own_rows = nullptr;
     int64_t cap_own_n = 0, cap_own_nnz = 0;
+    int64_t* d_batch = nullptr;    // batch column and entry starts (2 * (k + 1))
+    int64_t cap_d_batch = 0;
+    Xfer xfer;                     // staged copies from and to caller memory
     HighclearScratch hc;
     Prof prof;
     double ph_ms[PH_NUM] = {};
@@ -124,7 +128,7 @@ cudaError_t grow(T*& p, int64_t& cap, int64_t want) {
 void free_device(Device& D) {
     void* ptrs[] = {D.dim, D.perm, D.newidx, D.scratch64, D.arena, D.arena_top,
                     D.desc, D.low, D.pivot, D.state, D.cleared, D.negative, D.leftmost, D.active, D.blk, D.dimcnt,
-                    D.diminfo, D.err, D.counters, D.step_ctr, D.heavy, D.pool_tail, D.death_of, D.pairs, D.ess};
+                    D.diminfo, D.err, D.counters, D.step_ctr, D.heavy, D.pool_tail, D.death_of, D.pairs, D.ess, D.misc};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     D = Device();
@@ -169,6 +173,7 @@ int ensure_columns(sspp_ctx* ctx, int64_t n, int64_t nnz) {
         CK(cudaMalloc(&D.counters, sizeof(long long) * CNT_NUM));
         CK(cudaMalloc(&D.arena_top, sizeof(unsigned long long)));
         CK(cudaMalloc(&D.pool_tail, sizeof(int)));
+        CK(cudaMalloc(&D.misc, sizeof(int64_t) * 8));
     }
     return SSPP_OK;
 }
@@ -191,6 +196,7 @@ int ensure_arena(sspp_ctx* ctx, int64_t ints) {
 int64_t arena_need(const sspp_ctx* ctx) {
     const int64_t base = ctx->D.nnz + (kHdr + 3) * ctx->D.n + 4;
     int64_t want = base + std::max<int64_t>(2 * base, int64_t(16) << 20);
+    if (ctx->params.dualize) want += base;  // the dual columns are built behind the primal ones
     if (ctx->cfg.arena_bytes > 0) want = std::max<int64_t>(want, ctx->cfg.arena_bytes / 4);
     return std::max(want, ctx->arena_request);
 }
@@ -237,7 +243,6 @@ int check_params(sspp_ctx* ctx, const sspp_params* p) {
         return set_err(ctx, SSPP_ERR_BAD_INPUT, "heavy_threads must be 0, 128 or 256");
     if (p->level1_capacity < 0 || p->level2_capacity < 0)
         return set_err(ctx, SSPP_ERR_BAD_INPUT, "level capacities must be >= 0");
-    if (p->dualize) return set_err(ctx, SSPP_ERR_BAD_INPUT, "dualize is not available in this build");
     if (p->model & 2) return set_err(ctx, SSPP_ERR_BAD_INPUT, "edge collapse is not available in this build");
     return SSPP_OK;
 }
@@ -340,6 +345,7 @@ int run_init(sspp_ctx* ctx) {
         if (rc2) return rc2;
     }
     ctx->launches += init_compress(D, nullptr, s);
+    if (ctx->params.dualize) ctx->launches += dualize(D, s);
     ctx->launches += active_list(D, s);
     span_end(ctx, PH_INIT, ev0);
     CK(cudaGetLastError());
@@ -355,6 +361,7 @@ int run_init(sspp_ctx* ctx) {
         return set_err(ctx, SSPP_ERR_BAD_INPUT,
                        "malformed boundary matrix (a face index out of range, unsorted, duplicated, or of the "
                        "wrong dimension)");
+    if (*ctx->h_err & ERRB_CHECK) return set_err(ctx, SSPP_ERR_BAD_INPUT, "dualization self-check failed");
     if (*ctx->h_err) return set_err(ctx, SSPP_ERR_CAPACITY, "init pass overflow");
     ctx->inited = true;
     ctx->computed = false;
@@ -385,11 +392,14 @@ int run_compute(sspp_ctx* ctx) {
         if (ctx->light_blocks_per_sm < 1 || ctx->heavy_blocks_per_sm < 1)
             return set_err(ctx, SSPP_ERR_CAPACITY, "level capacities too large for shared memory");
     }
-    // schedule (dimensions high to low)
+    // schedule: dimensions high to low, or low to high for the dual matrix
+    // (include/specseq.h:598-600)
     std::vector<Step> steps;
     const DimInfo& I = ctx->hinfo;
-    for (int d = kMaxDim; d >= 1; d--)
+    for (int k = 0; k <= kMaxDim; k++) {
+        const int d = P.dualize ? k : kMaxDim - k;
         ss_schedule(P, I.act_begin[d], I.act_end[d], I.min_row[d] == INT_MAX ? 0 : I.min_row[d], I.max_row[d], steps);
+    }
     if (4 * int64_t(steps.size()) > D.cap_steps) {
         if (D.step_ctr) cudaFree(D.step_ctr);
         D.step_ctr = nullptr;
@@ -468,7 +478,7 @@ int run_compute(sspp_ctx* ctx) {
     ctx->ss_steps = int64_t(steps.size());
     cudaEvent_t ep = nullptr;
     span_begin(ctx, ep);
-    ctx->launches += extract_pairs(D, 0, nullptr, s);
+    ctx->launches += extract_pairs(D, P.dualize, nullptr, s);
     span_end(ctx, PH_PAIRS, ep);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(ctx->h_err, D.err, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -499,11 +509,28 @@ int load_common(sspp_ctx* ctx, int64_t n, int64_t nnz) {
     return SSPP_OK;
 }
 
-bool validate_colptr(const int64_t* cp, int64_t n) {
-    if (cp[0] != 0) return false;
-    for (int64_t j = 0; j < n; j++)
-        if (cp[j + 1] < cp[j] || cp[j + 1] - cp[j] > kMaxColLen) return false;
-    return true;
+// Device buffers for inputs copied from the host (grown, never shrunk).
+int ensure_own(sspp_ctx* ctx, int64_t n, int64_t nnz) {
+    if (n + 1 > ctx->cap_own_n) {
+        if (ctx->own_dims) cudaFree(ctx->own_dims);
+        if (ctx->own_colptr) cudaFree(ctx->own_colptr);
+        ctx->own_dims = nullptr;
+        ctx->own_colptr = nullptr;
+        ctx->cap_own_n = 0;
+        int64_t c1 = 0, c2 = 0;
+        CK(grow(ctx->own_dims, c1, n + 1));
+        CK(grow(ctx->own_colptr, c2, n + 1));
+        ctx->cap_own_n = n + 1;
+    }
+    if (nnz > ctx->cap_own_nnz || !ctx->own_rows) {
+        if (ctx->own_rows) cudaFree(ctx->own_rows);
+        ctx->own_rows = nullptr;
+        ctx->cap_own_nnz = 0;
+        int64_t c3 = 0;
+        CK(grow(ctx->own_rows, c3, std::max<int64_t>(nnz, 1)));
+        ctx->cap_own_nnz = std::max<int64_t>(nnz, 1);
+    }
+    return SSPP_OK;
 }
 
 }  // namespace
@@ -559,6 +586,7 @@ void sspp_destroy(sspp_ctx* ctx) {
     if (ctx->own_dims) cudaFree(ctx->own_dims);
     if (ctx->own_colptr) cudaFree(ctx->own_colptr);
     if (ctx->own_rows) cudaFree(ctx->own_rows);
+    if (ctx->d_batch) cudaFree(ctx->d_batch);
     for (auto* t : ctx->hc.tup)
         if (t) cudaFree(t);
     if (ctx->hc.deg) cudaFree(ctx->hc.deg);
@@ -588,34 +616,20 @@ int32_t sspp_load_csc(sspp_ctx* ctx, int64_t ncols, const int32_t* dims, const i
     cudaSetDevice(ctx->cfg.device);
     if (ncols < 0 || (ncols > 0 && (!dims || !col_ptr)) || !col_ptr)
         return set_err(ctx, SSPP_ERR_BAD_INPUT, "null input array");
-    if (!validate_colptr(col_ptr, ncols)) return set_err(ctx, SSPP_ERR_BAD_INPUT, "col_ptr must start at 0 and be non-decreasing");
+    // the rest of col_ptr (non-decreasing, column lengths) is checked on the device
+    if (col_ptr[0] != 0 || col_ptr[ncols] < 0)
+        return set_err(ctx, SSPP_ERR_BAD_INPUT, "col_ptr must start at 0 and be non-decreasing");
     const int64_t nnz = col_ptr[ncols];
     if (nnz > 0 && !rows) return set_err(ctx, SSPP_ERR_BAD_INPUT, "null rows");
     int rc = load_common(ctx, ncols, nnz);
     if (rc) return rc;
-    if (ncols + 1 > ctx->cap_own_n) {
-        int64_t c1 = 0, c2 = 0;
-        if (ctx->own_dims) cudaFree(ctx->own_dims);
-        if (ctx->own_colptr) cudaFree(ctx->own_colptr);
-        ctx->own_dims = nullptr;
-        ctx->own_colptr = nullptr;
-        ctx->cap_own_n = 0;
-        CK(grow(ctx->own_dims, c1, ncols + 1));
-        CK(grow(ctx->own_colptr, c2, ncols + 1));
-        ctx->cap_own_n = ncols + 1;
-    }
-    if (nnz > ctx->cap_own_nnz || !ctx->own_rows) {
-        int64_t c3 = 0;
-        if (ctx->own_rows) cudaFree(ctx->own_rows);
-        ctx->own_rows = nullptr;
-        ctx->cap_own_nnz = 0;
-        CK(grow(ctx->own_rows, c3, std::max<int64_t>(nnz, 1)));
-        ctx->cap_own_nnz = std::max<int64_t>(nnz, 1);
-    }
+    rc = ensure_own(ctx, ncols, nnz);
+    if (rc) return rc;
     cudaStream_t s = ctx->stream;
-    if (ncols) CK(cudaMemcpyAsync(ctx->own_dims, dims, sizeof(int32_t) * ncols, cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(ctx->own_colptr, col_ptr, sizeof(int64_t) * (ncols + 1), cudaMemcpyHostToDevice, s));
-    if (nnz) CK(cudaMemcpyAsync(ctx->own_rows, rows, sizeof(int32_t) * nnz, cudaMemcpyHostToDevice, s));
+    const std::vector<Piece> pcs = {{dims, ctx->own_dims, sizeof(int32_t) * size_t(ncols)},
+                                    {col_ptr, ctx->own_colptr, sizeof(int64_t) * size_t(ncols + 1)},
+                                    {rows, ctx->own_rows, sizeof(int32_t) * size_t(nnz)}};
+    CK(ctx->xfer.h2d(pcs, s));
     CK(cudaStreamSynchronize(s));
     ctx->D.in_dims = ctx->own_dims;
     ctx->D.in_colptr = ctx->own_colptr;
@@ -647,36 +661,49 @@ int32_t sspp_load_csc_device(sspp_ctx* ctx, int64_t ncols, const int32_t* d_dims
 int32_t sspp_load_batch(sspp_ctx* ctx, int32_t k, const int64_t* ncols, const int32_t* const* dims,
                         const int64_t* const* col_ptr, const int32_t* const* rows) {
     if (!ctx) return SSPP_ERR_BAD_INPUT;
+    cudaSetDevice(ctx->cfg.device);
     if (k < 0 || (k > 0 && (!ncols || !dims || !col_ptr || !rows)))
         return set_err(ctx, SSPP_ERR_BAD_INPUT, "null batch arrays");
-    int64_t n = 0, nnz = 0;
+    std::vector<int64_t> starts(size_t(2) * (size_t(k) + 1), 0);  // column starts, then entry starts
+    int64_t* cst = starts.data();
+    int64_t* est = cst + k + 1;
     for (int32_t i = 0; i < k; i++) {
         if (ncols[i] < 0 || !col_ptr[i] || (ncols[i] > 0 && !dims[i]))
             return set_err(ctx, SSPP_ERR_BAD_INPUT, "bad batch member");
-        if (!validate_colptr(col_ptr[i], ncols[i]))
+        if (col_ptr[i][0] != 0 || col_ptr[i][ncols[i]] < 0)
             return set_err(ctx, SSPP_ERR_BAD_INPUT, "col_ptr must start at 0 and be non-decreasing");
-        n += ncols[i];
-        nnz += col_ptr[i][ncols[i]];
+        if (col_ptr[i][ncols[i]] > 0 && !rows[i]) return set_err(ctx, SSPP_ERR_BAD_INPUT, "null rows");
+        cst[i + 1] = cst[i] + ncols[i];
+        est[i + 1] = est[i] + col_ptr[i][ncols[i]];
     }
-    std::vector<int32_t> cd(size_t(std::max<int64_t>(n, 1)));
-    std::vector<int64_t> cp(size_t(n) + 1, 0);
-    std::vector<int32_t> cr(size_t(std::max<int64_t>(nnz, 1)));
-    std::vector<int64_t> starts(size_t(k) + 1, 0);
-    int64_t c0 = 0, e0 = 0;
-    for (int32_t i = 0; i < k; i++) {
-        const int64_t ni = ncols[i], ei = col_ptr[i][ni];
-        for (int64_t j = 0; j < ni; j++) {
-            cd[size_t(c0 + j)] = dims[i][j];
-            cp[size_t(c0 + j + 1)] = e0 + col_ptr[i][j + 1];
-        }
-        for (int64_t t = 0; t < ei; t++) cr[size_t(e0 + t)] = rows[i][t] + int32_t(c0);
-        c0 += ni;
-        e0 += ei;
-        starts[size_t(i) + 1] = c0;
-    }
-    int rc = sspp_load_csc(ctx, n, cd.data(), cp.data(), cr.data());
+    const int64_t n = cst[k], nnz = est[k];
+    if (n > INT32_MAX - 8) return set_err(ctx, SSPP_ERR_CAPACITY, "more than 2^31 columns");
+    int rc = load_common(ctx, n, nnz);
     if (rc) return rc;
-    ctx->batch_start = starts;
+    rc = ensure_own(ctx, n, nnz);
+    if (rc) return rc;
+    CK(grow(ctx->d_batch, ctx->cap_d_batch, int64_t(starts.size())));
+    cudaStream_t s = ctx->stream;
+    // the complexes side by side; indices are shifted on the device
+    std::vector<Piece> pcs;
+    pcs.reserve(size_t(3) * size_t(k) + 1);
+    for (int32_t i = 0; i < k; i++)
+        pcs.push_back({dims[i], ctx->own_dims + cst[i], sizeof(int32_t) * size_t(ncols[i])});
+    for (int32_t i = 0; i < k; i++)
+        pcs.push_back({col_ptr[i] + 1, ctx->own_colptr + cst[i] + 1, sizeof(int64_t) * size_t(ncols[i])});
+    for (int32_t i = 0; i < k; i++)
+        pcs.push_back({rows[i], ctx->own_rows + est[i], sizeof(int32_t) * size_t(est[i + 1] - est[i])});
+    pcs.push_back({starts.data(), ctx->d_batch, sizeof(int64_t) * starts.size()});
+    CK(cudaMemsetAsync(ctx->own_colptr, 0, sizeof(int64_t), s));
+    CK(ctx->xfer.h2d(pcs, s));
+    batch_rebase(n, nnz, k, ctx->d_batch, ctx->d_batch + k + 1, ctx->own_colptr, ctx->own_rows, s);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(s));
+    ctx->D.in_dims = ctx->own_dims;
+    ctx->D.in_colptr = ctx->own_colptr;
+    ctx->D.in_rows = ctx->own_rows;
+    ctx->loaded = true;
+    ctx->batch_start.assign(cst, cst + k + 1);
     return SSPP_OK;
 }
 
@@ -702,8 +729,8 @@ static int batch_slice(sspp_ctx* ctx, int32_t i, int64_t& b, int64_t& e) {
     if (!ctx->host_pairs_valid) {
         const int64_t k = ctx->hcounters[CNT_NPAIRS];
         ctx->host_pairs.resize(size_t(2 * k));
-        if (k > 0 && cudaMemcpy(ctx->host_pairs.data(), ctx->D.pairs, sizeof(int64_t) * 2 * k,
-                                cudaMemcpyDeviceToHost) != cudaSuccess)
+        if (k > 0 && ctx->xfer.d2h({{ctx->D.pairs, ctx->host_pairs.data(), sizeof(int64_t) * 2 * size_t(k)}},
+                                   ctx->stream) != cudaSuccess)
             return SSPP_ERR_CUDA;
         ctx->host_pairs_valid = true;
     }
@@ -797,7 +824,7 @@ int64_t sspp_pairs(sspp_ctx* ctx, int64_t* out, int64_t cap) {
     if (!ctx || !ctx->computed || cap < 0 || (!out && cap > 0)) return -1;
     cudaSetDevice(ctx->cfg.device);
     int64_t n = std::min<int64_t>(cap, ctx->hcounters[CNT_NPAIRS]);
-    if (n > 0 && cudaMemcpy(out, ctx->D.pairs, sizeof(int64_t) * 2 * n, cudaMemcpyDeviceToHost) != cudaSuccess) {
+    if (n > 0 && ctx->xfer.d2h({{ctx->D.pairs, out, sizeof(int64_t) * 2 * size_t(n)}}, ctx->stream) != cudaSuccess) {
         set_err(ctx, SSPP_ERR_CUDA, "pairs copy failed");
         return -1;
     }

@@ -82,6 +82,37 @@ int validate(Device& D, cudaStream_t s) {
     return 1;
 }
 
+// Batch of k complexes copied side by side: complex i's face indices are
+// shifted by its first column cstart[i], and its col_ptr entries (without the
+// leading 0) by its first entry estart[i].
+__device__ __forceinline__ int32_t batch_member(const int64_t* start, int32_t k, int64_t x) {
+    int32_t a = 0, b = k;  // largest a with start[a] <= x
+    while (b - a > 1) {
+        const int32_t m = (a + b) >> 1;
+        if (start[m] <= x) a = m;
+        else b = m;
+    }
+    return a;
+}
+
+__global__ void k_batch_rebase(int64_t n, int64_t nnz, int32_t k, const int64_t* cstart, const int64_t* estart,
+                               int64_t* colptr, int32_t* rows) {
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < nnz; t += stride)
+        rows[t] += int32_t(cstart[batch_member(estart, k, t)]);
+    for (int64_t j = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; j < n; j += stride)
+        colptr[j + 1] += estart[batch_member(cstart, k, j)];
+}
+
+int batch_rebase(int64_t n, int64_t nnz, int32_t k, const int64_t* d_cstart, const int64_t* d_estart,
+                 int64_t* colptr, int32_t* rows, cudaStream_t s) {
+    const int64_t m = n > nnz ? n : nnz;
+    if (m == 0 || k <= 1) return 0;
+    k_batch_rebase<<<grid_for(m, 256) > 16384 ? 16384 : grid_for(m, 256), 256, 0, s>>>(n, nnz, k, d_cstart, d_estart,
+                                                                                       colptr, rows);
+    return 1;
+}
+
 // ------------------------------------------------------------------ reorder
 constexpr int kPartThreads = 256;
 

@@ -126,6 +126,7 @@ struct Device {
     int64_t* death_of = nullptr;   // [n]
     int64_t* pairs = nullptr;      // [2n]
     int64_t* ess = nullptr;        // [n]
+    int64_t* misc = nullptr;       // [8] small device scalars of the dualization
 };
 
 }  // namespace sspp

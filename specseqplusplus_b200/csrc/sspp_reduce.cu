@@ -470,7 +470,9 @@ struct Work {
     int32_t* buf;      // current entries (shared memory, or the data part of an arena slot)
     int len;
     bool global;       // buf lives in the arena
+    bool gpriv;        // buf is a private arena buffer (never published, reusable)
     int64_t gslot;     // arena slot of buf when global
+    int64_t gcap;      // ints of that slot
     int64_t slot;      // arena slot of the published version
     bool dirty;        // differs from the published version
 };
@@ -482,6 +484,7 @@ __device__ bool publish(const G& g, const ReduceArgs& A, int col, Work& w) {
     int64_t so;
     if (w.global) {
         so = w.gslot;
+        w.gpriv = false;  // published versions are immutable
     } else {
         so = alloc(g, A, slot_ints(w.len));
         if (so < 0) return false;
@@ -535,6 +538,12 @@ __device__ Outcome reduce_column(const G& g, const ReduceArgs& A, int col, int32
         w.global = true;
         w.gslot = w.slot;
     }
+    w.gpriv = false;
+    w.gcap = 0;
+    // a private arena buffer freed by the last merge, reused by the next one
+    // that does not fit in shared memory (chains of long sums then need two
+    // buffers, not one per addition)
+    int64_t spare = -1, spare_cap = 0;
     long long adds = 0, add_ints = 0;
     Outcome res = OUT_FAIL;
     int L = w.len ? ldv(w.buf + w.len - 1, w.global) : -1;
@@ -639,6 +648,10 @@ __device__ Outcome reduce_column(const G& g, const ReduceArgs& A, int col, int32
         if (bound <= A.cap) {
             int32_t* dst = (w.global || w.buf == sw1) ? sw0 : sw1;
             out_len = merge(g, w.buf, w.len, w.global, pb, plen, pg, dst, A.cap, A.err);
+            if (w.global && w.gpriv) {
+                spare = w.gslot;
+                spare_cap = w.gcap;
+            }
             w.buf = dst;
             w.global = false;
         } else {
@@ -651,6 +664,10 @@ __device__ Outcome reduce_column(const G& g, const ReduceArgs& A, int col, int32
             if (out_len <= A.cap) {
                 int32_t* dst = (w.global || w.buf == sw1) ? sw0 : sw1;
                 merge(g, w.buf, w.len, w.global, pb, plen, pg, dst, A.cap, A.err);
+                if (w.global && w.gpriv) {
+                    spare = w.gslot;
+                    spare_cap = w.gcap;
+                }
                 w.buf = dst;
                 w.global = false;
             } else if (defer) {
@@ -658,13 +675,28 @@ __device__ Outcome reduce_column(const G& g, const ReduceArgs& A, int col, int32
                 res = OUT_DEFERRED;
                 break;
             } else {
-                int64_t so = alloc(g, A, slot_ints(out_len));
-                if (so < 0) break;
+                const int64_t need = slot_ints(out_len);
+                int64_t so, cap_so;
+                if (spare >= 0 && spare_cap >= need) {
+                    so = spare;
+                    cap_so = spare_cap;
+                    spare = -1;
+                } else {
+                    cap_so = (need + (need >> 1) + 3) & ~int64_t(3);  // slack for a growing sum
+                    so = alloc(g, A, cap_so);
+                    if (so < 0) break;
+                    if (g.leader()) cnt_add(&A.counters[CNT_PUBLISHED], (long long)cap_so);
+                }
                 merge(g, w.buf, w.len, w.global, pb, plen, pg, A.arena + so + kHdr, int(pad4(out_len)), A.err);
-                if (g.leader()) cnt_add(&A.counters[CNT_PUBLISHED], (long long)slot_ints(out_len));
+                if (w.global && w.gpriv) {
+                    spare = w.gslot;
+                    spare_cap = w.gcap;
+                }
                 w.buf = A.arena + so + kHdr;
                 w.global = true;
+                w.gpriv = true;
                 w.gslot = so;
+                w.gcap = cap_so;
             }
         }
         adds++;
