@@ -1,0 +1,523 @@
+// Flag-complex edge collapse (model bit 2).
+//
+// Reference counterparts: the graph build with edge filtration = edge order
+// (include/specseq.h:209-212), GUDHI's flag_complex_collapse_edges
+// (include/Flag_complex_edge_collapser.h:224-482, the Boissonnat-Pritam
+// collapse), the drop of every edge that is not returned (include/specseq.h:
+// 410-424) and SimplexCollapse, which empties every higher simplex with a
+// dropped facet (include/specseq.h:425-436, include/kernel.h:190-198).  The
+// reference runs the collapse single-threaded on the host.
+//
+// The collapse visits the edges in filtration order.  Edge uv is dominated at
+// time t when its common neighbourhood C (through the edges valid at t) is not
+// empty and one w in C is adjacent to every other vertex of C.  An arriving
+// edge t that is not dominated is kept (critical) and re-examines, largest id
+// first, the earlier non-critical edges that close a triangle with it; each
+// re-examined edge e that is no longer dominated at time e (edges valid at e:
+// those before e, and the critical ones after it) is kept too and re-examines
+// its own triangles.  Valid edges at the arrival of t are exactly the edges
+// before t, whatever was kept, so every arrival test is independent of the
+// others: one kernel runs all of them in parallel (one warp per edge).  The
+// re-examinations depend on their order and run in one warp, in arrival order,
+// only for the arrivals that have triangles to re-examine.  Tests are warp-
+// parallel: the shorter neighbour list is intersected with the longer one
+// lane by lane (binary search), and in the domination test each lane takes
+// one w in C and counts its valid neighbours in C.
+#include <algorithm>
+#include <climits>
+
+#include "sspp_collapse.h"
+#include "sspp_kernels.cuh"
+#include "sspp_scan.cuh"
+
+namespace sspp {
+
+namespace {
+
+constexpr int kWarpsA = 8;     // arrival kernel: warps per block
+constexpr int kCapA = 256;     // common neighbours in shared memory per warp (arrival kernel)
+constexpr int kCapB = 2048;    // common neighbours in shared memory (re-examination kernel)
+constexpr int kMiscE = 0, kMiscMaxDeg = 1, kMiscCascades = 2, kMiscSteps = 3;
+
+unsigned grid_of(int64_t n, int threads, int64_t cap = 65536) {
+    int64_t g = (n + threads - 1) / threads;
+    if (g < 1) g = 1;
+    if (g > cap) g = cap;
+    return unsigned(g);
+}
+
+__device__ __forceinline__ int32_t key_nbr(uint64_t k) { return int32_t(k >> 32); }
+__device__ __forceinline__ int32_t key_edge(uint64_t k) { return int32_t(uint32_t(k)); }
+
+// Edge x takes part in the test of edge e while edges 0..tcur have arrived:
+// it precedes e, or it is critical (crit == nullptr: an arrival test, where
+// only the edges before e have arrived).
+struct Valid {
+    int32_t e, tcur;
+    const uint8_t* crit;
+    __device__ __forceinline__ bool operator()(int32_t x) const {
+        return x < e || (crit != nullptr && x <= tcur && crit[x] != 0);
+    }
+};
+
+// Common neighbours w of u and v through valid edges, ascending.  The first
+// `cap` go to C (and the ids of edges uw, vw to ea, eb when given); returns
+// how many there are.
+__device__ int common_nbrs(const uint64_t* adj, const int64_t* off, int32_t u, int32_t v, const Valid& ok, int32_t* C,
+                           int32_t* ea, int32_t* eb, int64_t cap) {
+    const int lane = lane_id();
+    int64_t a0 = off[u], a1 = off[u + 1], b0 = off[v], b1 = off[v + 1];
+    if (a1 - a0 > b1 - b0) {  // walk the shorter list
+        int64_t x = a0; a0 = b0; b0 = x;
+        x = a1; a1 = b1; b1 = x;
+    }
+    int count = 0;
+    for (int64_t base = a0; base < a1; base += 32) {
+        const int64_t i = base + lane;
+        bool hit = false;
+        int32_t w = 0, e1 = 0, e2 = 0;
+        if (i < a1) {
+            const uint64_t k = adj[i];
+            w = key_nbr(k);
+            e1 = key_edge(k);
+            if (ok(e1)) {
+                const uint64_t target = uint64_t(uint32_t(w)) << 32;
+                int64_t lo = b0, hi = b1;
+                while (lo < hi) {
+                    const int64_t mid = (lo + hi) >> 1;
+                    if (adj[mid] < target) lo = mid + 1;
+                    else hi = mid;
+                }
+                if (lo < b1) {
+                    const uint64_t k2 = adj[lo];
+                    if (key_nbr(k2) == w) {
+                        e2 = key_edge(k2);
+                        hit = ok(e2);
+                    }
+                }
+            }
+        }
+        const unsigned m = __ballot_sync(kFull, hit);
+        if (hit) {
+            const int p = count + __popc(m & lanemask_lt());
+            if (p < cap) {
+                C[p] = w;
+                if (ea) {
+                    ea[p] = e1;
+                    eb[p] = e2;
+                }
+            }
+        }
+        count += __popc(m);
+    }
+    __syncwarp();
+    return count;
+}
+
+// Some w in C (sorted, c >= 2) is adjacent through valid edges to every other
+// vertex of C.
+__device__ bool dominated_by_one(const uint64_t* adj, const int64_t* off, const Valid& ok, const int32_t* C, int c) {
+    const int lane = lane_id();
+    bool any = false;
+    for (int base = 0; base < c && !any; base += 32) {
+        const int k = base + lane;
+        bool dom = false;
+        if (k < c) {
+            const int32_t w = C[k];
+            const int64_t s0 = off[w], s1 = off[w + 1];
+            if (s1 - s0 >= c - 1) {
+                int cnt = 0;
+                for (int64_t i = s0; i < s1; i++) {
+                    const uint64_t key = adj[i];
+                    if (!ok(key_edge(key))) continue;
+                    const int32_t x = key_nbr(key);
+                    int lo = 0, hi = c;
+                    while (lo < hi) {
+                        const int mid = (lo + hi) >> 1;
+                        if (C[mid] < x) lo = mid + 1;
+                        else hi = mid;
+                    }
+                    if (lo < c && C[lo] == x) cnt++;
+                }
+                dom = cnt >= c - 1;
+            }
+        }
+        any = __any_sync(kFull, dom);
+    }
+    return any;
+}
+
+__global__ void k_cdeg(const int32_t* misc, const int32_t* eu, const int32_t* ev, int32_t* deg) {
+    const int64_t E = misc[kMiscE];
+    for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < E; e += int64_t(gridDim.x) * blockDim.x) {
+        atomicAdd(deg + eu[e], 1);
+        atomicAdd(deg + ev[e], 1);
+    }
+}
+
+__global__ void k_cfill(const int32_t* misc, const int32_t* eu, const int32_t* ev, const int64_t* off, int32_t* cur,
+                        uint64_t* adj) {
+    const int64_t E = misc[kMiscE];
+    for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < E; e += int64_t(gridDim.x) * blockDim.x) {
+        const int32_t u = eu[e], v = ev[e];
+        adj[off[u] + atomicAdd(cur + u, 1)] = (uint64_t(uint32_t(v)) << 32) | uint32_t(e);
+        adj[off[v] + atomicAdd(cur + v, 1)] = (uint64_t(uint32_t(u)) << 32) | uint32_t(e);
+    }
+}
+
+__device__ void heap_sort_u64(uint64_t* a, int64_t n) {
+    auto sift = [&](int64_t root, int64_t end) {
+        while (2 * root + 1 < end) {
+            int64_t c = 2 * root + 1;
+            if (c + 1 < end && a[c] < a[c + 1]) c++;
+            if (a[root] >= a[c]) return;
+            const uint64_t t = a[root];
+            a[root] = a[c];
+            a[c] = t;
+            root = c;
+        }
+    };
+    for (int64_t s = n / 2 - 1; s >= 0; s--) sift(s, n);
+    for (int64_t e = n - 1; e > 0; e--) {
+        const uint64_t t = a[0];
+        a[0] = a[e];
+        a[e] = t;
+        sift(0, e);
+    }
+}
+
+// sorts every neighbour list; misc[kMiscMaxDeg] = largest degree
+__global__ void k_csort(int64_t nv, const int64_t* off, uint64_t* adj, int32_t* misc) {
+    int32_t mx = 0;
+    for (int64_t v = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; v < nv; v += int64_t(gridDim.x) * blockDim.x) {
+        uint64_t* a = adj + off[v];
+        const int64_t n = off[v + 1] - off[v];
+        mx = n > mx ? int32_t(n) : mx;
+        if (n <= 32) {
+            for (int64_t i = 1; i < n; i++) {
+                const uint64_t x = a[i];
+                int64_t j = i - 1;
+                while (j >= 0 && a[j] > x) {
+                    a[j + 1] = a[j];
+                    j--;
+                }
+                a[j + 1] = x;
+            }
+        } else {
+            heap_sort_u64(a, n);
+        }
+    }
+    mx = warp_max(mx);
+    if ((threadIdx.x & 31) == 0 && mx) atomicMax(misc + kMiscMaxDeg, mx);
+}
+
+// arrival test of every edge: arr 0 = dominated, 1 = kept, 2 = kept with
+// triangles to re-examine
+__global__ void __launch_bounds__(kWarpsA * 32) k_arrival(const int32_t* misc, const int32_t* eu, const int32_t* ev,
+                                                         const uint64_t* adj, const int64_t* off, uint8_t* arr,
+                                                         uint8_t* crit, int32_t* cbuf, int64_t cbuf_per_warp) {
+    __shared__ int32_t sC[kWarpsA][kCapA];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t gw = int64_t(blockIdx.x) * kWarpsA + w, nw = int64_t(gridDim.x) * kWarpsA;
+    const int64_t E = misc[kMiscE];
+    for (int64_t t = gw; t < E; t += nw) {
+        const Valid ok{int32_t(t), int32_t(t), nullptr};
+        const int c = common_nbrs(adj, off, eu[t], ev[t], ok, sC[w], nullptr, nullptr, kCapA);
+        uint8_t r;
+        if (c == 0) {
+            r = 1;
+        } else if (c == 1) {
+            r = 0;
+        } else {
+            const int32_t* C = sC[w];
+            if (c > kCapA) {
+                int32_t* g = cbuf + gw * cbuf_per_warp;
+                common_nbrs(adj, off, eu[t], ev[t], ok, g, nullptr, nullptr, cbuf_per_warp);
+                C = g;
+            }
+            r = dominated_by_one(adj, off, ok, C, c) ? 0 : 2;
+        }
+        if (lane == 0) {
+            arr[t] = r;
+            crit[t] = r != 0;
+        }
+        __syncwarp();
+    }
+}
+
+// max-heap of edge ids (one thread)
+__device__ void heap_push(int32_t* h, int& size, int32_t x) {
+    int i = size++;
+    h[i] = x;
+    while (i > 0) {
+        const int p = (i - 1) >> 1;
+        if (h[p] >= h[i]) break;
+        const int32_t t = h[p];
+        h[p] = h[i];
+        h[i] = t;
+        i = p;
+    }
+}
+
+__device__ int32_t heap_pop(int32_t* h, int& size) {
+    const int32_t top = h[0];
+    const int32_t last = h[--size];
+    int i = 0;
+    for (;;) {
+        int c = 2 * i + 1;
+        if (c >= size) break;
+        if (c + 1 < size && h[c + 1] > h[c]) c++;
+        if (h[c] <= last) break;
+        h[i] = h[c];
+        i = c;
+    }
+    if (size > 0) h[i] = last;
+    return top;
+}
+
+// the earlier non-critical edges uw, vw of the triangles of edge th go into the set
+__device__ void push_partners(const int32_t* A, const int32_t* B, int c, int32_t th, const uint8_t* crit, uint8_t* ins,
+                              int32_t* heap, int& size) {
+    if (lane_id() == 0) {
+        for (int k = 0; k < c; k++) {
+            const int32_t ab[2] = {A[k], B[k]};
+            for (int q = 0; q < 2; q++) {
+                const int32_t x = ab[q];
+                if (x < th && !crit[x] && !ins[x]) {
+                    ins[x] = 1;
+                    heap_push(heap, size, x);
+                }
+            }
+        }
+    }
+    __syncwarp();
+}
+
+// Re-examinations, in arrival order, by one warp.
+__global__ void __launch_bounds__(32) k_cascade(const int32_t* cas, int32_t* misc, const int32_t* eu, const int32_t* ev,
+                                               const uint64_t* adj, const int64_t* off, uint8_t* crit, uint8_t* ins,
+                                               int32_t* heap, int32_t* gC, int32_t* gA, int32_t* gB, int64_t gcap,
+                                               long long max_steps, int* err) {
+    __shared__ int32_t sC[kCapB], sA[kCapB], sB[kCapB];
+    const int lane = lane_id();
+    const int ncas = misc[kMiscCascades];
+    int size = 0;  // heap size, meaningful in lane 0 and broadcast
+    long long steps = 0;
+    bool fail = false;
+    for (int i = 0; i < ncas && !fail; i++) {
+        const int32_t t = cas[i];
+        {
+            const Valid ok{t, t, nullptr};
+            int c = common_nbrs(adj, off, eu[t], ev[t], ok, sC, sA, sB, kCapB);
+            const int32_t *A = sA, *B = sB;
+            if (c > kCapB) {
+                common_nbrs(adj, off, eu[t], ev[t], ok, gC, gA, gB, gcap);
+                A = gA;
+                B = gB;
+            }
+            push_partners(A, B, c, t, crit, ins, heap, size);
+            size = __shfl_sync(kFull, size, 0);
+        }
+        while (size > 0) {
+            if (++steps > max_steps) {
+                fail = true;
+                break;
+            }
+            int32_t e = 0;
+            if (lane == 0) {
+                e = heap_pop(heap, size);
+                ins[e] = 0;
+            }
+            e = __shfl_sync(kFull, e, 0);
+            size = __shfl_sync(kFull, size, 0);
+            __syncwarp();
+            if (crit[e]) continue;
+            const Valid ok{e, t, crit};
+            int c = common_nbrs(adj, off, eu[e], ev[e], ok, sC, sA, sB, kCapB);
+            const int32_t *C = sC, *A = sA, *B = sB;
+            if (c > kCapB) {
+                common_nbrs(adj, off, eu[e], ev[e], ok, gC, gA, gB, gcap);
+                C = gC;
+                A = gA;
+                B = gB;
+            }
+            const bool dom = (c == 1) || (c >= 2 && dominated_by_one(adj, off, ok, C, c));
+            if (dom) continue;
+            if (lane == 0) crit[e] = 1;
+            __syncwarp();
+            push_partners(A, B, c, e, crit, ins, heap, size);
+            size = __shfl_sync(kFull, size, 0);
+        }
+    }
+    if (lane == 0) {
+        misc[kMiscSteps] = int32_t(steps > INT_MAX ? INT_MAX : steps);
+        if (fail) atomicOr(err, ERRB_TIMEOUT);
+    }
+}
+
+__global__ void k_drop_edges(const int32_t* misc, const uint8_t* crit, const int32_t* ecol, uint8_t* dropped) {
+    const int64_t E = misc[kMiscE];
+    for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < E; e += int64_t(gridDim.x) * blockDim.x)
+        if (!crit[e]) dropped[ecol[e]] = 1;
+}
+
+// a simplex of dimension >= 2 with a dropped facet is dropped
+__global__ void k_drop_up(int32_t cb, int32_t ce, const int32_t* arena, const uint64_t* desc, uint8_t* dropped) {
+    for (int64_t j = cb + blockIdx.x * int64_t(blockDim.x) + threadIdx.x; j < ce; j += int64_t(gridDim.x) * blockDim.x) {
+        const uint64_t d = desc[j];
+        const int32_t* c = arena + desc_off(d) + kHdr;
+        const uint32_t len = desc_len(d);
+        for (uint32_t k = 0; k < len; k++)
+            if (dropped[c[k]]) {
+                dropped[j] = 1;
+                break;
+            }
+    }
+}
+
+__global__ void k_empty_dropped(int64_t n, int32_t* arena, uint64_t* desc, const uint8_t* dropped,
+                                long long* counters) {
+    long long cnt = 0;
+    for (int64_t j = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; j < n; j += int64_t(gridDim.x) * blockDim.x) {
+        if (!dropped[j]) continue;
+        const uint64_t d = desc[j];
+        desc[j] = pack_desc(desc_off(d), 0);
+        arena[desc_off(d)] = 0;
+        cnt++;
+    }
+    cnt = warp_sum(cnt);
+    if ((threadIdx.x & 31) == 0 && cnt) cnt_add(&counters[CNT_DROPPED], cnt);
+}
+
+template <typename T>
+cudaError_t grow_buf(T*& p, int64_t want) {
+    if (p) cudaFree(p);
+    p = nullptr;
+    return cudaMalloc(&p, size_t(want > 0 ? want : 1) * sizeof(T));
+}
+
+}  // namespace
+
+void collapse_free(CollapseScratch& S) {
+    void* ptrs[] = {S.eu, S.ev, S.ecol, S.deg, S.adj_off, S.adj, S.arr, S.crit, S.ins, S.heap, S.cas, S.cbuf, S.misc};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    S = CollapseScratch();
+}
+
+int collapse(Device& D, const DimInfo& info, uint8_t* dropped, CollapseScratch& S, cudaStream_t s,
+             const char** err_msg) {
+    const int64_t n = D.n;
+    int launches = 0;
+    cudaMemsetAsync(dropped, 0, size_t(n), s);
+    const int32_t eb = info.col_begin[1], ee = info.col_end[1];
+    const int64_t nv = info.col_end[0] - info.col_begin[0];
+    const int64_t ne = ee > eb ? ee - eb : 0;
+    if (ne == 0 || nv == 0) return 0;
+    *err_msg = "edge collapse: device allocation failed";
+    if (ne > S.cap_e) {
+        if (grow_buf(S.eu, ne) || grow_buf(S.ev, ne) || grow_buf(S.ecol, ne) || grow_buf(S.adj, 2 * ne) ||
+            grow_buf(S.arr, ne) || grow_buf(S.crit, ne) || grow_buf(S.ins, ne) || grow_buf(S.heap, ne) ||
+            grow_buf(S.cas, ne))
+            return -1;
+        S.cap_e = ne;
+    }
+    if (nv + 1 > S.cap_v) {
+        if (grow_buf(S.deg, nv + 1) || grow_buf(S.adj_off, nv + 1)) return -1;
+        S.cap_v = nv + 1;
+    }
+    if (!S.misc && grow_buf(S.misc, 8)) return -1;
+    cudaMemsetAsync(S.misc, 0, 8 * sizeof(int32_t), s);
+    // edge list: the 2-row columns of dimension 1, in filtration order
+    {
+        const uint64_t* desc = D.desc;
+        const int32_t* arena = D.arena;
+        int32_t* eu = S.eu;
+        int32_t* ev = S.ev;
+        int32_t* ecol = S.ecol;
+        scan([=] __device__(int64_t i) -> int64_t { return desc_len(desc[eb + i]) == 2 ? 1 : 0; },
+             [=] __device__(int64_t i, int64_t pre, int64_t v) {
+                 if (v) {
+                     const int32_t* c = arena + desc_off(desc[eb + i]) + kHdr;
+                     eu[pre] = c[0];
+                     ev[pre] = c[1];
+                     ecol[pre] = int32_t(eb + i);
+                 }
+             },
+             ne, D.blk, s);
+        launches += 3;
+    }
+    int64_t E = 0;
+    cudaMemcpyAsync(&E, D.blk + scan_blocks(ne), sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+    // the edge count for the kernels (low 32 bits of the int64 total; E < 2^31)
+    cudaMemcpyAsync(S.misc + kMiscE, D.blk + scan_blocks(ne), sizeof(int32_t), cudaMemcpyDeviceToDevice, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) {
+        *err_msg = "edge collapse: edge count";
+        return -1;
+    }
+    if (E == 0) return launches;
+    // adjacency: (neighbour, edge id), ascending per vertex
+    cudaMemsetAsync(S.deg, 0, sizeof(int32_t) * (nv + 1), s);
+    k_cdeg<<<grid_of(E, 256), 256, 0, s>>>(S.misc, S.eu, S.ev, S.deg);
+    {
+        const int32_t* deg = S.deg;
+        int64_t* off = S.adj_off;
+        scan([=] __device__(int64_t v) -> int64_t { return v < nv ? deg[v] : 0; },
+             [=] __device__(int64_t v, int64_t pre, int64_t) { off[v] = pre; }, nv + 1, D.blk, s);
+    }
+    cudaMemsetAsync(S.deg, 0, sizeof(int32_t) * (nv + 1), s);
+    k_cfill<<<grid_of(E, 256), 256, 0, s>>>(S.misc, S.eu, S.ev, S.adj_off, S.deg, S.adj);
+    k_csort<<<grid_of(nv, 128), 128, 0, s>>>(nv, S.adj_off, S.adj, S.misc);
+    launches += 6;
+    int32_t maxdeg = 0;
+    cudaMemcpyAsync(&maxdeg, S.misc + kMiscMaxDeg, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) {
+        *err_msg = "edge collapse: adjacency build";
+        return -1;
+    }
+    // overflow buffers for common neighbourhoods larger than shared memory
+    int64_t warps_a = std::min<int64_t>(E, 148 * 64);
+    int64_t per_warp = maxdeg > kCapA ? maxdeg : 0;
+    if (per_warp > 0) warps_a = std::max<int64_t>(1, std::min<int64_t>(warps_a, (int64_t(1) << 26) / per_warp));
+    warps_a = (warps_a + kWarpsA - 1) / kWarpsA * kWarpsA;  // whole blocks, each warp with its buffer
+    const int64_t gcap = maxdeg > kCapB ? maxdeg : 0;
+    const int64_t want = std::max<int64_t>(warps_a * per_warp, 3 * gcap) + 1;
+    if (want > S.cap_cbuf) {
+        if (grow_buf(S.cbuf, want)) return -1;
+        S.cap_cbuf = want;
+    }
+    k_arrival<<<unsigned(warps_a / kWarpsA), kWarpsA * 32, 0, s>>>(
+        S.misc, S.eu, S.ev, S.adj, S.adj_off, S.arr, S.crit, S.cbuf, per_warp);
+    {
+        const uint8_t* arr = S.arr;
+        int32_t* cas = S.cas;
+        scan([=] __device__(int64_t t) -> int64_t { return arr[t] == 2 ? 1 : 0; },
+             [=] __device__(int64_t t, int64_t pre, int64_t v) {
+                 if (v) cas[pre] = int32_t(t);
+             },
+             E, D.blk, s);
+    }
+    // count of arrivals with re-examinations (fits in int32: E does)
+    cudaMemcpyAsync(S.misc + kMiscCascades, D.blk + scan_blocks(E), sizeof(int32_t), cudaMemcpyDeviceToDevice, s);
+    cudaMemsetAsync(S.ins, 0, size_t(E), s);
+    // every pop either keeps an edge (at most E times) or discards one inserted
+    // by a kept edge's triangles; the bound only guards against a corrupted set
+    const double bound = 64.0 * double(E) * double(maxdeg + 1) + double(1 << 20);
+    const long long max_steps = bound > 4.0e18 ? (long long)4e18 : (long long)bound;
+    k_cascade<<<1, 32, 0, s>>>(S.cas, S.misc, S.eu, S.ev, S.adj, S.adj_off, S.crit, S.ins, S.heap, S.cbuf,
+                               S.cbuf + gcap, S.cbuf + 2 * gcap, gcap, max_steps, D.err);
+    k_drop_edges<<<grid_of(E, 256), 256, 0, s>>>(S.misc, S.crit, S.ecol, dropped);
+    launches += 7;
+    for (int d = 2; d <= kMaxDim; d++) {
+        const int32_t cb = info.col_begin[d], ce = info.col_end[d];
+        if (ce <= cb) continue;
+        k_drop_up<<<grid_of(ce - cb, 256), 256, 0, s>>>(cb, ce, D.arena, D.desc, dropped);
+        launches++;
+    }
+    k_empty_dropped<<<grid_of(n, 256), 256, 0, s>>>(n, D.arena, D.desc, dropped, D.counters);
+    launches++;
+    *err_msg = nullptr;
+    return launches;
+}
+
+}  // namespace sspp

@@ -18,6 +18,7 @@
 #include <type_traits>
 #include <vector>
 
+#include "sspp_collapse.h"
 #include "sspp_highclear.h"
 #include "sspp_internal.h"
 #include "sspp_io.h"
@@ -89,6 +90,7 @@ struct sspp_ctx {
     int64_t cap_d_batch = 0;
     Xfer xfer;                     // staged copies from and to caller memory
     HighclearScratch hc;
+    CollapseScratch cs;
     Prof prof;
     double ph_ms[PH_NUM] = {};
     // batch: column range of each complex in the concatenated input, and the
@@ -243,7 +245,6 @@ int check_params(sspp_ctx* ctx, const sspp_params* p) {
         return set_err(ctx, SSPP_ERR_BAD_INPUT, "heavy_threads must be 0, 128 or 256");
     if (p->level1_capacity < 0 || p->level2_capacity < 0)
         return set_err(ctx, SSPP_ERR_BAD_INPUT, "level capacities must be >= 0");
-    if (p->model & 2) return set_err(ctx, SSPP_ERR_BAD_INPUT, "edge collapse is not available in this build");
     return SSPP_OK;
 }
 
@@ -282,6 +283,31 @@ void span_collect(sspp_ctx* ctx) {
     ctx->prof.reset();
 }
 
+// dropped[] of the edge collapse when it runs (model bit 2), else null
+const uint8_t* dropped_of(const sspp_ctx* ctx) { return (ctx->params.model & 2) ? ctx->dropped : nullptr; }
+
+// Edge collapse on the reordered matrix (needs host reads of the column
+// ranges, the edge count and the largest degree).
+int run_collapse(sspp_ctx* ctx) {
+    Device& D = ctx->D;
+    cudaStream_t s = ctx->stream;
+    if (D.n > ctx->cap_dropped) {
+        if (ctx->dropped) cudaFree(ctx->dropped);
+        ctx->dropped = nullptr;
+        ctx->cap_dropped = 0;
+        CK(grow(ctx->dropped, ctx->cap_dropped, D.n));
+    }
+    CK(cudaMemcpyAsync(ctx->h_info, D.diminfo, sizeof(DimInfo), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    const DimInfo info = *ctx->h_info;
+    const char* msg = nullptr;
+    const int k = collapse(D, info, ctx->dropped, ctx->cs, s, &msg);
+    if (k < 0) return set_err(ctx, SSPP_ERR_CUDA, msg ? msg : "edge collapse failed");
+    ctx->launches += k;
+    CK(cudaGetLastError());
+    return SSPP_OK;
+}
+
 // Sizes the guided-clearing scratch from the per-dimension column ranges and
 // runs it (needs one host read of the ranges).
 int run_highclear(sspp_ctx* ctx) {
@@ -307,7 +333,7 @@ int run_highclear(sspp_ctx* ctx) {
     while (slots < 2 * ntop) slots *= 2;
     CK(grow(S.table, S.cap_table, slots));
     S.mask = uint32_t(slots - 1);
-    ctx->launches += highclear(D, info, ctx->params.max_iteration, nullptr, S, s);
+    ctx->launches += highclear(D, info, ctx->params.max_iteration, dropped_of(ctx), S, s);
     return SSPP_OK;
 }
 
@@ -339,12 +365,16 @@ int run_init(sspp_ctx* ctx) {
     ctx->launches += reorder(D, s);
     CK(cudaMemcpyAsync(D.arena_top, D.blk + reorder_total_slot(D), sizeof(unsigned long long),
                        cudaMemcpyDeviceToDevice, s));
+    if (ctx->params.model & 2) {  // collapse before everything else: dropped columns are emptied
+        int rc2 = run_collapse(ctx);
+        if (rc2) return rc2;
+    }
     ctx->launches += init_passes(D, s);
     if ((ctx->params.model & 1) && ctx->params.max_iteration > 0) {
         int rc2 = run_highclear(ctx);
         if (rc2) return rc2;
     }
-    ctx->launches += init_compress(D, nullptr, s);
+    ctx->launches += init_compress(D, dropped_of(ctx), s);
     if (ctx->params.dualize) ctx->launches += dualize(D, s);
     ctx->launches += active_list(D, s);
     span_end(ctx, PH_INIT, ev0);
@@ -478,7 +508,7 @@ int run_compute(sspp_ctx* ctx) {
     ctx->ss_steps = int64_t(steps.size());
     cudaEvent_t ep = nullptr;
     span_begin(ctx, ep);
-    ctx->launches += extract_pairs(D, P.dualize, nullptr, s);
+    ctx->launches += extract_pairs(D, P.dualize, dropped_of(ctx), s);
     span_end(ctx, PH_PAIRS, ep);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(ctx->h_err, D.err, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -587,6 +617,7 @@ void sspp_destroy(sspp_ctx* ctx) {
     if (ctx->own_colptr) cudaFree(ctx->own_colptr);
     if (ctx->own_rows) cudaFree(ctx->own_rows);
     if (ctx->d_batch) cudaFree(ctx->d_batch);
+    collapse_free(ctx->cs);
     for (auto* t : ctx->hc.tup)
         if (t) cudaFree(t);
     if (ctx->hc.deg) cudaFree(ctx->hc.deg);
