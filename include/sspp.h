@@ -40,14 +40,21 @@ typedef struct sspp_config {
     int64_t arena_bytes;     /* initial column arena; 0 = sized from the input       */
     int32_t verbose;         /* 0 = silent                                           */
     int32_t profile;         /* 1 = time every device phase with CUDA events         */
+    int32_t host_threads;    /* host threads for staged copies; 0 = all cores         */
 } sspp_config;
 
 /* The reference's 12 positional CLI values (src/main.cu:281-294) minus file
- * names/formats.  `autotune` != 0 replaces ss_block_size, growth, queue_size and
- * the level capacities with the engine's tuned values for the input's size
- * class. */
+ * names/formats.  `autotune` = 1 replaces ss_block_size, growth, queue_size,
+ * the level capacities and heavy_threads with the engine's choice for the
+ * input's size class (a process-wide history of measured candidates; the
+ * reference sets these by hand); 2 also lets it choose between dualize 0 and
+ * 2, which never changes the pairs. */
 typedef struct sspp_params {
-    int32_t dualize;          /* 0/1                                                  */
+    int32_t dualize;          /* 0 boundary matrix; 1 coboundary (anti-transpose) as
+                                 the reference; 2 the 0-dimensional pairs from the
+                                 boundary matrix's edges, then the coboundary matrix
+                                 from dimension 1 up (no counterpart in the
+                                 reference); the pairs are the same in every mode   */
     int32_t model;            /* bit0 high-dimension guided clearing, bit1 collapse   */
     int32_t max_iteration;    /* candidates per simplex for guided clearing           */
     int32_t ss_block_size;    /* initial spectral-sequence block size                 */
@@ -55,7 +62,7 @@ typedef struct sspp_params {
     int32_t queue_size;       /* concurrent column workers per launch                 */
     int32_t level1_capacity;  /* per-worker on-chip column capacity (ints)            */
     int32_t level2_capacity;  /* per-block on-chip column capacity (ints)             */
-    int32_t autotune;
+    int32_t autotune;         /* 0 off, 1 launch parameters, 2 also dualization     */
     int32_t heavy_threads;    /* threads per heavy-tier column: 128 or 256 (0 = 256)  */
 } sspp_params;
 
@@ -79,6 +86,8 @@ typedef struct sspp_stats {
      * heavy-tier reduction launches, pair extraction */
     double init_gpu_ms, light_gpu_ms, heavy_gpu_ms, pairs_gpu_ms;
     int64_t light_launches, heavy_launches;
+    int64_t arena_ints_used;     /* column arena in use after the reduction (ints)  */
+    int64_t tuned_candidate;     /* autotuner candidate of the last run, or -1     */
 } sspp_stats;
 
 /* Replaces: the SpecSeqPlusPlus constructor's allocation (include/specseq.h:486-512). */
@@ -148,11 +157,85 @@ int32_t sspp_load_batch_device(sspp_ctx* ctx, int32_t k, const int64_t* ncols, c
                                const int64_t* d_col_ptr, const int32_t* d_rows);
 int64_t sspp_batch_num_pairs(sspp_ctx* ctx, int32_t i);
 int64_t sspp_batch_pairs(sspp_ctx* ctx, int32_t i, int64_t* out_birth_death, int64_t cap);
+int64_t sspp_batch_num_essential(sspp_ctx* ctx, int32_t i);
+int64_t sspp_batch_essentials(sspp_ctx* ctx, int32_t i, int64_t* out, int64_t cap);
 
 /* Replaces: writeVectorToFile (src/main.cu:191-229). */
 int32_t sspp_write_pairs(sspp_ctx* ctx, const char* path, int32_t fmt);
 
 int32_t sspp_get_stats(const sspp_ctx* ctx, sspp_stats* out);
+/* The parameters the last sspp_init ran with (autotuned values included). */
+int32_t sspp_get_params(const sspp_ctx* ctx, sspp_params* out);
+
+/* Serving (no counterpart in the reference, whose CLI reduces one file per
+ * process).  A resident request loop on one GPU: `workers` host threads, each
+ * with its own context and stream, take the requests waiting in arrival order
+ * as one batch (block-diagonal, as sspp_load_batch) as long as the batch's
+ * device-memory estimate fits the worker's share of `memory_budget`; requests
+ * that arrive while batches run join the next batch a worker forms, and the
+ * workers' batches overlap on the device (copies of one with the reduction of
+ * another).  Estimate per request: 128 bytes per column + 4 per entry + the
+ * column arena, 4 bytes x fill x (nnz + 7 ncols), with fill the largest arena
+ * fill the autotuner has seen for the request's size class (3 before any).
+ * A request whose estimate exceeds the whole budget is refused at submit.
+ * A batch that fails is re-run request by request so one bad input fails
+ * alone.  Latency = completion - submission, on the host's steady clock. */
+typedef struct sspp_server sspp_server;
+
+typedef struct sspp_server_config {
+    int32_t device;
+    int32_t workers;             /* concurrent batches (contexts, streams); 0 = 2   */
+    int64_t memory_budget;       /* bytes for all workers; 0 = 85% of free memory   */
+    int64_t max_batch_cols;      /* 0 = no limit besides memory                     */
+    int32_t max_batch_requests;  /* 0 = no limit                                    */
+    double batch_window_ms;      /* wait this long for more requests when the queue
+                                    holds fewer than max_batch_requests; 0 = none   */
+} sspp_server_config;
+
+typedef struct sspp_server_stats {
+    int64_t submitted, completed, failed, rejected, batches, columns;
+    double wall_s;               /* first submission to last completion            */
+    double cols_per_s;           /* columns of completed requests / wall_s         */
+    double p50_ms, p95_ms, p99_ms, max_ms, mean_ms;
+    double mean_batch_requests;
+} sspp_server_stats;
+
+/* request states */
+#define SSPP_REQ_QUEUED 0
+#define SSPP_REQ_RUNNING 1
+#define SSPP_REQ_DONE 2
+#define SSPP_REQ_FAILED 3
+
+/* submit flag: the caller keeps dims / col_ptr / rows valid and unmodified
+ * until the request is done (no copy at submission) */
+#define SSPP_SUBMIT_NOCOPY 1
+
+/* params: as for sspp_init (autotune applies per batch). */
+sspp_server* sspp_server_create(const sspp_server_config* cfg, const sspp_params* params);
+/* Finishes every accepted request, then stops the workers. */
+void sspp_server_destroy(sspp_server* srv);
+const char* sspp_server_last_error(sspp_server* srv);
+/* Returns the request id (>= 0), or -SSPP_ERR_* when refused. */
+int64_t sspp_server_submit(sspp_server* srv, int64_t ncols, const int32_t* dims, const int64_t* col_ptr,
+                           const int32_t* rows, int32_t flags);
+/* SSPP_OK once the request is done or failed, SSPP_ERR_TIMEOUT if timeout_ms
+ * passed first (timeout_ms < 0 waits for ever), SSPP_ERR_STATE for an unknown id. */
+int32_t sspp_server_wait(sspp_server* srv, int64_t id, double timeout_ms);
+/* SSPP_REQ_* state, or -SSPP_ERR_STATE for an unknown id. */
+int32_t sspp_server_state(sspp_server* srv, int64_t id);
+/* Status code of a finished request (SSPP_OK or the failure); its message. */
+int32_t sspp_server_result(sspp_server* srv, int64_t id, char* msg, int32_t msg_cap);
+int64_t sspp_server_num_pairs(sspp_server* srv, int64_t id);
+int64_t sspp_server_pairs(sspp_server* srv, int64_t id, int64_t* out_birth_death, int64_t cap);
+int64_t sspp_server_num_essential(sspp_server* srv, int64_t id);
+int64_t sspp_server_essentials(sspp_server* srv, int64_t id, int64_t* out, int64_t cap);
+/* Latency of a finished request (ms), -1 otherwise. */
+double sspp_server_latency_ms(sspp_server* srv, int64_t id);
+/* Frees a finished request's results and forgets the id. */
+int32_t sspp_server_release(sspp_server* srv, int64_t id);
+int32_t sspp_server_get_stats(sspp_server* srv, sspp_server_stats* out);
+/* Clears the latency record and counters (not the autotuner history). */
+int32_t sspp_server_reset_stats(sspp_server* srv);
 
 /* No counterpart in the reference.  Allocation-free reduction for callers that
  * cannot have a library allocate device memory (a server that reserves all of

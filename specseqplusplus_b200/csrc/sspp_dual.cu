@@ -16,6 +16,15 @@
 // per-column sort is one warp per column (registers up to 32 entries, shared
 // memory up to 1024), and the rare longer columns are sorted by one CTA with
 // shared-memory chunk sorts and merge-path merges in global memory.
+//
+// Mode 2 (no counterpart in the reference) dualizes after the boundary
+// matrix's edge columns have been reduced: the 0-dimensional pairs are known,
+// the dual columns of vertices are left alone, and the dual columns of the
+// edges those pairs kill are cleared.  The dual columns of dimension >= 1 only
+// hold cofaces of dimension >= 2, whose columns that reduction never touched.
+// On lower-star grids the dual columns of vertices carry addition chains of
+// tens of thousands of steps; mode 2 avoids them while keeping the short dual
+// chains of dimensions >= 1 on Rips complexes.
 #include <climits>
 
 #include "sspp_launch.h"
@@ -232,9 +241,12 @@ __global__ void __launch_bounds__(kLongThreads) k_dual_sort_long(const int64_t* 
     }
 }
 
-// dual descriptors, lows and states; primal `state` is read at n-1-c
+// dual descriptors, lows and states; primal `state` and `pdim` are read at
+// n-1-c.  h0_done: the 0-dimensional pairs came from the boundary matrix, so
+// the dual columns of vertices are never reduced.
 __global__ void k_dual_finish(int64_t n, const int64_t* off, const int64_t* misc, const int32_t* arena,
-                              uint64_t* desc, int32_t* low, const uint8_t* pstate, uint8_t* nstate) {
+                              uint64_t* desc, int32_t* low, const uint8_t* pstate, const int32_t* pdim, int h0_done,
+                              uint8_t* nstate) {
     const int64_t base = misc[0];
     if (base < 0) return;
     for (int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; c < n; c += int64_t(gridDim.x) * blockDim.x) {
@@ -243,25 +255,32 @@ __global__ void k_dual_finish(int64_t n, const int64_t* off, const int64_t* misc
         desc[c] = pack_desc(uint64_t(o), uint32_t(len));
         low[c] = len ? arena[o + kHdr + len - 1] : -1;
         const uint8_t ps = pstate[n - 1 - c];
-        nstate[c] = ps == ST_DROPPED ? ST_DROPPED : (len ? ST_ACTIVE : ST_ZERO);
+        nstate[c] = ps == ST_DROPPED ? ST_DROPPED : ((len && !(h0_done && pdim[n - 1 - c] == 0)) ? ST_ACTIVE : ST_ZERO);
     }
 }
 
-// primal apparent pairs (low l, column c) -> dual (low n-1-c, column n-1-l)
+// primal pairs (low l, column c) -> dual (low n-1-c, column n-1-l); the dual
+// column n-1-c of the negative simplex c is cleared (twist clearing of the
+// dual).  With h0_done the pairs of vertices came from reducing the boundary
+// matrix's edges, so their dual owners (vertex columns) are not checked.
 __global__ void k_dual_pivots(int64_t n, const uint64_t* pivot, const int64_t* off, const int64_t* misc,
-                              const int32_t* low, uint64_t* npivot, uint8_t* nstate, int* err) {
+                              const int32_t* low, const int32_t* pdim, int h0_done, uint64_t* npivot, uint8_t* nstate,
+                              uint8_t* cleared, int* err) {
     const int64_t base = misc[0];
     if (base < 0) return;
     for (int64_t l = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; l < n; l += int64_t(gridDim.x) * blockDim.x) {
         const uint64_t e = pivot[l];
         if (e == kNoOwner) continue;
         const int64_t dc = n - 1 - l, dr = n - 1 - pv_col(e);
-        if (low[dc] != dr) {  // self-check: the dual owner's lowest row
+        const bool vertex_owner = h0_done && pdim[l] == 0;
+        if (!vertex_owner && low[dc] != dr) {  // self-check: the dual owner's lowest row
             atomicOr(err, ERRB_CHECK);
             continue;
         }
         npivot[dr] = pv_pack(int32_t(dc), uint64_t(base + off[dc]));
-        nstate[dc] = ST_OWNER;
+        nstate[dc] = vertex_owner ? ST_ZERO : ST_OWNER;
+        nstate[dr] = ST_CLEARED;
+        cleared[dr] = 1;
     }
 }
 
@@ -284,7 +303,8 @@ __global__ void k_dual_diminfo(int64_t n, DimInfo* info) {
 
 }  // namespace
 
-int dualize(Device& D, cudaStream_t s) {
+int dualize(Device& D, int mode, cudaStream_t s) {
+    const int h0_done = mode == 2;
     const int64_t n = D.n;
     const unsigned g = grid_of(n, 256, 65536);
     int32_t* cnt = D.leftmost;  // free after the init passes
@@ -299,13 +319,13 @@ int dualize(Device& D, cudaStream_t s) {
     k_dual_sort<<<grid_of(n, kSortWarps, 16384), kSortWarps * 32, 0, s>>>(n, off, D.misc, D.arena, D.active);
     // the pairs buffer (4n ints) is free until the pairs are extracted
     k_dual_sort_long<<<1, kLongThreads, 0, s>>>(off, D.misc, D.arena, D.active, reinterpret_cast<int32_t*>(D.pairs));
-    k_dual_finish<<<g, 256, 0, s>>>(n, off, D.misc, D.arena, D.desc, D.low, D.state, D.negative);
+    k_dual_finish<<<g, 256, 0, s>>>(n, off, D.misc, D.arena, D.desc, D.low, D.state, D.dim, h0_done, D.negative);
     fill_i64(reinterpret_cast<int64_t*>(D.death_of), -1, n, s);  // kNoOwner
-    k_dual_pivots<<<g, 256, 0, s>>>(n, D.pivot, off, D.misc, D.low, reinterpret_cast<uint64_t*>(D.death_of),
-                                    D.negative, D.err);
+    cudaMemsetAsync(D.cleared, 0, n, s);
+    k_dual_pivots<<<g, 256, 0, s>>>(n, D.pivot, off, D.misc, D.low, D.dim, h0_done,
+                                    reinterpret_cast<uint64_t*>(D.death_of), D.negative, D.cleared, D.err);
     cudaMemcpyAsync(D.pivot, D.death_of, sizeof(uint64_t) * n, cudaMemcpyDeviceToDevice, s);
     cudaMemcpyAsync(D.state, D.negative, n, cudaMemcpyDeviceToDevice, s);
-    cudaMemsetAsync(D.cleared, 0, n, s);
     k_reverse_i32<<<g, 256, 0, s>>>(D.dim, n);
     k_dual_diminfo<<<1, 32, 0, s>>>(n, D.diminfo);
     return 16;

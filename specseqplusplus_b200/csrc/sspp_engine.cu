@@ -23,6 +23,7 @@
 #include "sspp_internal.h"
 #include "sspp_io.h"
 #include "sspp_launch.h"
+#include "sspp_tune.h"
 #include "sspp_xfer.h"
 
 using namespace sspp;
@@ -63,7 +64,10 @@ struct sspp_ctx {
     std::vector<cudaEvent_t> step_ev;  // light step k done
     cudaEvent_t join_ev[kSide] = {};   // side stream joins
     Device D;
-    sspp_params params{};
+    sspp_params params{};          // effective parameters (after autotuning)
+    sspp_params user_params{};     // as passed to sspp_init
+    int tune_cand = -1;            // autotuner candidate of this run, -1 without autotune
+    int64_t arena_used = 0;        // arena ints in use after the last reduction
     bool loaded = false, inited = false, computed = false;
     DimInfo hinfo{};
     long long hcounters[CNT_NUM] = {};
@@ -98,6 +102,8 @@ struct sspp_ctx {
     std::vector<int64_t> batch_start;   // k + 1 entries (empty when not a batch)
     std::vector<int64_t> host_pairs;
     bool host_pairs_valid = false;
+    std::vector<int64_t> host_ess;     // essentials, copied back once for slicing
+    bool host_ess_valid = false;
     int64_t launches = 0, light_launches = 0, heavy_launches = 0;
 };
 
@@ -234,7 +240,7 @@ void ss_schedule(const sspp_params& P, int32_t ab, int32_t ae, int32_t minrow_di
 
 int check_params(sspp_ctx* ctx, const sspp_params* p) {
     if (!p) return set_err(ctx, SSPP_ERR_BAD_INPUT, "null params");
-    if (p->dualize != 0 && p->dualize != 1) return set_err(ctx, SSPP_ERR_BAD_INPUT, "dualize must be 0 or 1");
+    if (p->dualize < 0 || p->dualize > 2) return set_err(ctx, SSPP_ERR_BAD_INPUT, "dualize must be 0, 1 or 2");
     if (p->model < 0 || p->model > 3) return set_err(ctx, SSPP_ERR_BAD_INPUT, "model must be 0..3");
     if (p->max_iteration < 0) return set_err(ctx, SSPP_ERR_BAD_INPUT, "max_iteration must be >= 0");
     if (p->ss_block_size < 1) return set_err(ctx, SSPP_ERR_BAD_INPUT, "ss_block_size must be >= 1");
@@ -245,6 +251,7 @@ int check_params(sspp_ctx* ctx, const sspp_params* p) {
         return set_err(ctx, SSPP_ERR_BAD_INPUT, "heavy_threads must be 0, 128 or 256");
     if (p->level1_capacity < 0 || p->level2_capacity < 0)
         return set_err(ctx, SSPP_ERR_BAD_INPUT, "level capacities must be >= 0");
+    if (p->autotune < 0 || p->autotune > 2) return set_err(ctx, SSPP_ERR_BAD_INPUT, "autotune must be 0, 1 or 2");
     return SSPP_OK;
 }
 
@@ -375,7 +382,7 @@ int run_init(sspp_ctx* ctx) {
         if (rc2) return rc2;
     }
     ctx->launches += init_compress(D, dropped_of(ctx), s);
-    if (ctx->params.dualize) ctx->launches += dualize(D, s);
+    if (ctx->params.dualize == 1) ctx->launches += dualize(D, 1, s);
     ctx->launches += active_list(D, s);
     span_end(ctx, PH_INIT, ev0);
     CK(cudaGetLastError());
@@ -398,38 +405,12 @@ int run_init(sspp_ctx* ctx) {
     return SSPP_OK;
 }
 
-int run_compute(sspp_ctx* ctx) {
-    ctx->err.clear();
-    ctx->host_pairs_valid = false;
+// Runs one spectral-sequence schedule: per step a light-tier launch on the
+// main stream and a heavy-tier launch for the columns it deferred.
+int run_steps(sspp_ctx* ctx, const std::vector<Step>& steps, int cap1, int cap2, int ht) {
     Device& D = ctx->D;
     cudaStream_t s = ctx->stream;
-    auto t0 = std::chrono::steady_clock::now();
-    if (D.n == 0) {
-        std::memset(ctx->hcounters, 0, sizeof(ctx->hcounters));
-        ctx->compute_ms = 0;
-        ctx->ss_steps = 0;
-        ctx->computed = true;
-        return SSPP_OK;
-    }
     const sspp_params& P = ctx->params;
-    const int cap1 = level1_cap(P), cap2 = level2_cap(P);
-    const int ht = P.heavy_threads == 128 ? 128 : 256;
-    if (cap1 != ctx->configured_cap1 || cap2 != ctx->configured_cap2 || ht != ctx->configured_ht) {
-        CK(reduce_configure(cap1, cap2, ht, &ctx->light_blocks_per_sm, &ctx->heavy_blocks_per_sm));
-        ctx->configured_cap1 = cap1;
-        ctx->configured_cap2 = cap2;
-        ctx->configured_ht = ht;
-        if (ctx->light_blocks_per_sm < 1 || ctx->heavy_blocks_per_sm < 1)
-            return set_err(ctx, SSPP_ERR_CAPACITY, "level capacities too large for shared memory");
-    }
-    // schedule: dimensions high to low, or low to high for the dual matrix
-    // (include/specseq.h:598-600)
-    std::vector<Step> steps;
-    const DimInfo& I = ctx->hinfo;
-    for (int k = 0; k <= kMaxDim; k++) {
-        const int d = P.dualize ? k : kMaxDim - k;
-        ss_schedule(P, I.act_begin[d], I.act_end[d], I.min_row[d] == INT_MAX ? 0 : I.min_row[d], I.max_row[d], steps);
-    }
     if (4 * int64_t(steps.size()) > D.cap_steps) {
         if (D.step_ctr) cudaFree(D.step_ctr);
         D.step_ctr = nullptr;
@@ -506,15 +487,78 @@ int run_compute(sspp_ctx* ctx) {
         if (rcj) return rcj;
     }
     ctx->ss_steps = int64_t(steps.size());
+    return SSPP_OK;
+}
+
+int run_compute(sspp_ctx* ctx) {
+    ctx->err.clear();
+    ctx->host_pairs_valid = false;
+    ctx->host_ess_valid = false;
+    Device& D = ctx->D;
+    cudaStream_t s = ctx->stream;
+    auto t0 = std::chrono::steady_clock::now();
+    if (D.n == 0) {
+        std::memset(ctx->hcounters, 0, sizeof(ctx->hcounters));
+        ctx->compute_ms = 0;
+        ctx->ss_steps = 0;
+        ctx->computed = true;
+        return SSPP_OK;
+    }
+    const sspp_params& P = ctx->params;
+    const int cap1 = level1_cap(P), cap2 = level2_cap(P);
+    const int ht = P.heavy_threads == 128 ? 128 : 256;
+    if (cap1 != ctx->configured_cap1 || cap2 != ctx->configured_cap2 || ht != ctx->configured_ht) {
+        CK(reduce_configure(cap1, cap2, ht, &ctx->light_blocks_per_sm, &ctx->heavy_blocks_per_sm));
+        ctx->configured_cap1 = cap1;
+        ctx->configured_cap2 = cap2;
+        ctx->configured_ht = ht;
+        if (ctx->light_blocks_per_sm < 1 || ctx->heavy_blocks_per_sm < 1)
+            return set_err(ctx, SSPP_ERR_CAPACITY, "level capacities too large for shared memory");
+    }
+    // schedule: dimensions high to low, or low to high for the dual matrix
+    // (include/specseq.h:598-600).  dualize 2: the boundary matrix's edge
+    // columns first (0-dimensional pairs), then the coboundary matrix from
+    // dimension 1 up.
+    const DimInfo& I = ctx->hinfo;
+    auto schedule = [&](int dlo, int dhi, bool ascending) {
+        std::vector<Step> st;
+        for (int k = 0; k <= dhi - dlo; k++) {
+            const int d = ascending ? dlo + k : dhi - k;
+            ss_schedule(P, I.act_begin[d], I.act_end[d], I.min_row[d] == INT_MAX ? 0 : I.min_row[d], I.max_row[d], st);
+        }
+        return st;
+    };
+    int64_t nsteps = 0;
+    if (P.dualize == 2) {
+        int rc = run_steps(ctx, schedule(1, 1, false), cap1, cap2, ht);
+        if (rc) return rc;
+        nsteps += ctx->ss_steps;
+        ctx->launches += dualize(D, 2, s);
+        ctx->launches += active_list(D, s);
+        CK(cudaMemcpyAsync(ctx->h_info, D.diminfo, sizeof(DimInfo), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        ctx->hinfo = *ctx->h_info;
+        rc = run_steps(ctx, schedule(1, kMaxDim, true), cap1, cap2, ht);
+        if (rc) return rc;
+        nsteps += ctx->ss_steps;
+    } else {
+        int rc = P.dualize ? run_steps(ctx, schedule(0, kMaxDim, true), cap1, cap2, ht)
+                           : run_steps(ctx, schedule(0, kMaxDim, false), cap1, cap2, ht);
+        if (rc) return rc;
+        nsteps += ctx->ss_steps;
+    }
+    ctx->ss_steps = nsteps;
     cudaEvent_t ep = nullptr;
     span_begin(ctx, ep);
-    ctx->launches += extract_pairs(D, P.dualize, dropped_of(ctx), s);
+    ctx->launches += extract_pairs(D, P.dualize != 0, dropped_of(ctx), s);
     span_end(ctx, PH_PAIRS, ep);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(ctx->h_err, D.err, sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(ctx->h_counters, D.counters, sizeof(long long) * CNT_NUM, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(ctx->h_top, D.arena_top, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     std::memcpy(ctx->hcounters, ctx->h_counters, sizeof(ctx->hcounters));
+    ctx->arena_used = int64_t(*ctx->h_top);
     ctx->compute_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     span_collect(ctx);
     const int e = *ctx->h_err;
@@ -531,6 +575,7 @@ int load_common(sspp_ctx* ctx, int64_t n, int64_t nnz) {
     ctx->loaded = ctx->inited = ctx->computed = false;
     ctx->batch_start.clear();
     ctx->host_pairs_valid = false;
+    ctx->host_ess_valid = false;
     int rc = ensure_columns(ctx, std::max<int64_t>(n, 1), std::max<int64_t>(nnz, 1));
     if (rc) return rc;
     ctx->D.n = n;
@@ -585,6 +630,7 @@ sspp_ctx* sspp_create(const sspp_config* cfg) {
     auto* ctx = new (std::nothrow) sspp_ctx;
     if (!ctx) return nullptr;
     if (cfg) ctx->cfg = *cfg;
+    ctx->xfer.set_threads(ctx->cfg.host_threads);
     if (cudaSetDevice(ctx->cfg.device) != cudaSuccess) { delete ctx; return nullptr; }
     if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess) { delete ctx; return nullptr; }
     for (int q = 0; q < sspp_ctx::kSide; q++) {
@@ -713,7 +759,7 @@ int32_t sspp_load_batch(sspp_ctx* ctx, int32_t k, const int64_t* ncols, const in
     if (rc) return rc;
     rc = ensure_own(ctx, n, nnz);
     if (rc) return rc;
-    CK(grow(ctx->d_batch, ctx->cap_d_batch, int64_t(starts.size())));
+    CK(grow(ctx->d_batch, ctx->cap_d_batch, int64_t(starts.size()) + 1));  // + the bad-index flag
     cudaStream_t s = ctx->stream;
     // the complexes side by side; indices are shifted on the device
     std::vector<Piece> pcs;
@@ -725,11 +771,18 @@ int32_t sspp_load_batch(sspp_ctx* ctx, int32_t k, const int64_t* ncols, const in
     for (int32_t i = 0; i < k; i++)
         pcs.push_back({rows[i], ctx->own_rows + est[i], sizeof(int32_t) * size_t(est[i + 1] - est[i])});
     pcs.push_back({starts.data(), ctx->d_batch, sizeof(int64_t) * starts.size()});
+    int* d_bad = reinterpret_cast<int*>(ctx->d_batch + starts.size());
     CK(cudaMemsetAsync(ctx->own_colptr, 0, sizeof(int64_t), s));
+    CK(cudaMemsetAsync(d_bad, 0, sizeof(int), s));
     CK(ctx->xfer.h2d(pcs, s));
-    batch_rebase(n, nnz, k, ctx->d_batch, ctx->d_batch + k + 1, ctx->own_colptr, ctx->own_rows, s);
+    batch_rebase(n, nnz, k, ctx->d_batch, ctx->d_batch + k + 1, ctx->own_colptr, ctx->own_rows, d_bad, s);
     CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(ctx->h_err, d_bad, sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
+    if (*ctx->h_err) {
+        ctx->loaded = false;
+        return set_err(ctx, SSPP_ERR_BAD_INPUT, "a face index lies outside its own complex");
+    }
     ctx->D.in_dims = ctx->own_dims;
     ctx->D.in_colptr = ctx->own_colptr;
     ctx->D.in_rows = ctx->own_rows;
@@ -803,6 +856,43 @@ int64_t sspp_batch_pairs(sspp_ctx* ctx, int32_t i, int64_t* out, int64_t cap) {
     return n;
 }
 
+// essentials of complex i (the ascending global list is copied once)
+static int batch_ess_slice(sspp_ctx* ctx, int32_t i, int64_t& b, int64_t& e) {
+    if (!ctx->computed || ctx->batch_start.empty() || i < 0 || i + 1 >= int32_t(ctx->batch_start.size()))
+        return SSPP_ERR_STATE;
+    if (!ctx->host_ess_valid) {
+        const int64_t k = ctx->hcounters[CNT_NESS];
+        ctx->host_ess.resize(size_t(k));
+        if (k > 0 && ctx->xfer.d2h({{ctx->D.ess, ctx->host_ess.data(), sizeof(int64_t) * size_t(k)}}, ctx->stream) !=
+                         cudaSuccess)
+            return SSPP_ERR_CUDA;
+        ctx->host_ess_valid = true;
+    }
+    const auto& v = ctx->host_ess;
+    b = std::lower_bound(v.begin(), v.end(), ctx->batch_start[size_t(i)]) - v.begin();
+    e = std::lower_bound(v.begin(), v.end(), ctx->batch_start[size_t(i) + 1]) - v.begin();
+    return SSPP_OK;
+}
+
+int64_t sspp_batch_num_essential(sspp_ctx* ctx, int32_t i) {
+    if (!ctx) return -1;
+    cudaSetDevice(ctx->cfg.device);
+    int64_t b, e;
+    if (batch_ess_slice(ctx, i, b, e)) return -1;
+    return e - b;
+}
+
+int64_t sspp_batch_essentials(sspp_ctx* ctx, int32_t i, int64_t* out, int64_t cap) {
+    if (!ctx || cap < 0 || (!out && cap > 0)) return -1;
+    cudaSetDevice(ctx->cfg.device);
+    int64_t b, e;
+    if (batch_ess_slice(ctx, i, b, e)) return -1;
+    const int64_t off = ctx->batch_start[size_t(i)];
+    const int64_t n = std::min(cap, e - b);
+    for (int64_t t = 0; t < n; t++) out[t] = ctx->host_ess[size_t(b + t)] - off;
+    return n;
+}
+
 int32_t sspp_load_phat(sspp_ctx* ctx, const char* path, int32_t fmt) {
     if (!ctx) return SSPP_ERR_BAD_INPUT;
     if (!path || (fmt != SSPP_ASCII && fmt != SSPP_BINARY)) return set_err(ctx, SSPP_ERR_BAD_INPUT, "bad path or format");
@@ -819,6 +909,20 @@ int32_t sspp_init(sspp_ctx* ctx, const sspp_params* p, void* stream) {
     int rc = check_params(ctx, p);
     if (rc) return rc;
     ctx->params = *p;
+    ctx->user_params = *p;
+    ctx->tune_cand = -1;
+    if (p->autotune) {
+        Knobs k;
+        ctx->tune_cand = tune_choose(ctx->D.n, p->model, p->dualize, p->autotune == 2, &k);
+        sspp_params& q = ctx->params;
+        q.ss_block_size = k.ss_block_size;
+        q.growth = k.growth;
+        q.queue_size = k.queue_size;
+        q.level1_capacity = k.level1;
+        q.level2_capacity = k.level2;
+        q.heavy_threads = k.heavy_threads;
+        q.dualize = k.dualize;
+    }
     ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
     return run_init(ctx);
 }
@@ -830,6 +934,12 @@ int32_t sspp_compute(sspp_ctx* ctx, void* stream) {
     if (stream) ctx->stream = static_cast<cudaStream_t>(stream);
     for (int attempt = 0; attempt < 6; attempt++) {
         int rc = run_compute(ctx);
+        if (rc == SSPP_OK && ctx->tune_cand >= 0) {
+            const sspp_params& u = ctx->user_params;
+            const double base = double(ctx->D.nnz + (kHdr + 3) * ctx->D.n + 4);
+            tune_record(ctx->D.n, u.model, u.dualize, u.autotune == 2, ctx->tune_cand, ctx->init_ms + ctx->compute_ms,
+                        double(ctx->arena_used) / base);
+        }
         if (rc != SSPP_ERR_CAPACITY || !ctx->err.empty()) return rc;
         // arena or heavy pool exhausted: grow both and redo the whole reduction from the input
         ctx->arena_request = std::max<int64_t>(ctx->D.arena_cap * 2, arena_need(ctx));
@@ -889,6 +999,12 @@ int32_t sspp_write_pairs(sspp_ctx* ctx, const char* path, int32_t fmt) {
     return SSPP_OK;
 }
 
+int32_t sspp_get_params(const sspp_ctx* ctx, sspp_params* out) {
+    if (!ctx || !out) return SSPP_ERR_BAD_INPUT;
+    *out = ctx->params;
+    return SSPP_OK;
+}
+
 int32_t sspp_get_stats(const sspp_ctx* ctx, sspp_stats* o) {
     if (!ctx || !o) return SSPP_ERR_BAD_INPUT;
     std::memset(o, 0, sizeof(*o));
@@ -900,6 +1016,8 @@ int32_t sspp_get_stats(const sspp_ctx* ctx, sspp_stats* o) {
     o->cleared_init = c[CNT_CLEARED];
     o->highclear_cleared = c[CNT_HIGHCLEAR];
     o->collapse_dropped = c[CNT_DROPPED];
+    o->arena_ints_used = ctx->arena_used;
+    o->tuned_candidate = ctx->tune_cand;
     o->additions = c[CNT_ADDITIONS];
     o->add_ints = c[CNT_ADD_INTS];
     o->published_ints = c[CNT_PUBLISHED];

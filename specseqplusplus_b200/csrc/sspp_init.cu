@@ -96,20 +96,24 @@ __device__ __forceinline__ int32_t batch_member(const int64_t* start, int32_t k,
 }
 
 __global__ void k_batch_rebase(int64_t n, int64_t nnz, int32_t k, const int64_t* cstart, const int64_t* estart,
-                               int64_t* colptr, int32_t* rows) {
+                               int64_t* colptr, int32_t* rows, int* bad) {
     const int64_t stride = int64_t(gridDim.x) * blockDim.x;
-    for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < nnz; t += stride)
-        rows[t] += int32_t(cstart[batch_member(estart, k, t)]);
+    for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < nnz; t += stride) {
+        const int32_t i = batch_member(estart, k, t);
+        const int32_t r = rows[t];
+        if (r < 0 || r >= cstart[i + 1] - cstart[i]) *bad = 1;  // a face outside its own complex
+        rows[t] = r + int32_t(cstart[i]);
+    }
     for (int64_t j = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; j < n; j += stride)
         colptr[j + 1] += estart[batch_member(cstart, k, j)];
 }
 
 int batch_rebase(int64_t n, int64_t nnz, int32_t k, const int64_t* d_cstart, const int64_t* d_estart,
-                 int64_t* colptr, int32_t* rows, cudaStream_t s) {
+                 int64_t* colptr, int32_t* rows, int* d_bad, cudaStream_t s) {
     const int64_t m = n > nnz ? n : nnz;
     if (m == 0 || k <= 1) return 0;
     k_batch_rebase<<<grid_for(m, 256) > 16384 ? 16384 : grid_for(m, 256), 256, 0, s>>>(n, nnz, k, d_cstart, d_estart,
-                                                                                       colptr, rows);
+                                                                                       colptr, rows, d_bad);
     return 1;
 }
 

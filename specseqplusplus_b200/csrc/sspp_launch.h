@@ -15,9 +15,10 @@ void fill_i64(int64_t* p, int64_t v, int64_t n, cudaStream_t s);
 // Each launcher returns the number of kernels it launched.
 int validate(Device& D, cudaStream_t s);  // sets ERRB_BAD_INPUT
 // k complexes copied side by side (cstart/estart: k+1 column / entry starts on
-// the device): shifts each one's face indices and col_ptr entries
+// the device): shifts each one's face indices and col_ptr entries; *d_bad = 1
+// when a face index lies outside its own complex
 int batch_rebase(int64_t n, int64_t nnz, int32_t k, const int64_t* d_cstart, const int64_t* d_estart,
-                 int64_t* colptr, int32_t* rows, cudaStream_t s);
+                 int64_t* colptr, int32_t* rows, int* d_bad, cudaStream_t s);
 int reorder(Device& D, cudaStream_t s);
 int64_t reorder_total_slot(const Device& D);  // index into D.blk of the arena total
 
@@ -25,8 +26,10 @@ int init_passes(Device& D, cudaStream_t s);
 int init_compress(Device& D, const uint8_t* dropped, cudaStream_t s);
 int active_list(Device& D, cudaStream_t s);
 // anti-transpose of the compressed matrix behind the primal columns in the
-// arena; remaps pivots, states, dims and the per-dimension column ranges
-int dualize(Device& D, cudaStream_t s);
+// arena; remaps pivots, states, dims and the per-dimension column ranges.
+// mode 1: the whole matrix; mode 2: after the edge columns were reduced (the
+// 0-dimensional pairs are final, the vertices' dual columns are skipped)
+int dualize(Device& D, int mode, cudaStream_t s);
 int extract_pairs(Device& D, int dual, const uint8_t* dropped, cudaStream_t s);
 
 cudaError_t reduce_configure(int cap1, int cap2, int heavy_threads, int* light_blocks_per_sm,

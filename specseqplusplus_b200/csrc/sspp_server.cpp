@@ -1,0 +1,419 @@
+// Resident request loop with continuous batching (include/sspp.h, "Serving").
+//
+// No counterpart in the reference, whose command line reduces one file per
+// process (src/main.cu:269-352).  Requests are copied (or referenced) at
+// submission and queued in arrival order.  Each worker thread owns a context
+// (its own stream, device buffers and pinned staging) and loops: take the
+// queued requests, oldest first, while the batch's device-memory estimate
+// fits the worker's share of the budget; reduce them as one block-diagonal
+// batch; hand every request its own pairs and essentials.  Requests that
+// arrive meanwhile wait for the next free worker, which forms the next batch
+// from whatever is queued then, so batches are formed continuously and the
+// workers' batches overlap on the GPU.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/sspp.h"
+#include "sspp_tune.h"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Request {
+    int64_t id = 0;
+    int64_t ncols = 0, nnz = 0;
+    std::vector<int32_t> dims_copy;
+    std::vector<int64_t> colptr_copy;
+    std::vector<int32_t> rows_copy;
+    const int32_t* dims = nullptr;
+    const int64_t* colptr = nullptr;
+    const int32_t* rows = nullptr;
+    double est = 0;
+    int state = SSPP_REQ_QUEUED;
+    int32_t status = SSPP_OK;
+    std::string msg;
+    std::vector<int64_t> pairs, ess;
+    Clock::time_point t_submit, t_done;
+};
+
+double ms_between(Clock::time_point a, Clock::time_point b) {
+    return std::chrono::duration<double, std::milli>(b - a).count();
+}
+
+}  // namespace
+
+struct sspp_server {
+    sspp_server_config cfg{};
+    sspp_params params{};
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<Request*> queue;
+    std::unordered_map<int64_t, std::unique_ptr<Request>> reqs;
+    int64_t next_id = 0;
+    std::vector<std::thread> workers;
+    bool stop = false;
+    double budget = 0, share = 0;
+    std::string err;
+    std::vector<double> lat_ms;
+    int64_t submitted = 0, completed = 0, failed = 0, rejected = 0, batches = 0, columns = 0, batch_reqs = 0;
+    bool have_first = false;
+    Clock::time_point t_first, t_last;
+};
+
+namespace {
+
+// device bytes one request adds to a batch
+double estimate(const sspp_params& p, int64_t ncols, int64_t nnz) {
+    const double fill = sspp::tune_fill(ncols, p.model, p.dualize, p.autotune == 2, 3.0);
+    const double base = double(nnz) + 7.0 * double(ncols) + 4.0;
+    double b = 128.0 * double(ncols) + 4.0 * double(nnz) + 4.0 * fill * base;
+    if (p.dualize || p.autotune == 2) b += 4.0 * base;  // dual columns built behind the primal ones
+    return b;
+}
+
+void set_result(Request* r, int32_t status, const char* msg) {
+    r->status = status;
+    r->msg = msg ? msg : "";
+}
+
+// one batch through one context; SSPP_OK when every request has its results
+int32_t try_batch(sspp_ctx* ctx, const sspp_params& params, const std::vector<Request*>& b) {
+    if (!ctx) {
+        for (Request* r : b) set_result(r, SSPP_ERR_CUDA, "no usable CUDA device");
+        return SSPP_ERR_CUDA;
+    }
+    const int32_t k = int32_t(b.size());
+    std::vector<int64_t> nc(b.size());
+    std::vector<const int32_t*> d(b.size()), rw(b.size());
+    std::vector<const int64_t*> cp(b.size());
+    for (size_t i = 0; i < b.size(); i++) {
+        nc[i] = b[i]->ncols;
+        d[i] = b[i]->dims;
+        cp[i] = b[i]->colptr;
+        rw[i] = b[i]->rows;
+    }
+    int32_t rc = sspp_load_batch(ctx, k, nc.data(), d.data(), cp.data(), rw.data());
+    if (rc == SSPP_OK) rc = sspp_reduce(ctx, &params, nullptr);
+    if (rc != SSPP_OK) {
+        for (Request* r : b) set_result(r, rc, sspp_last_error(ctx));
+        return rc;
+    }
+    for (int32_t i = 0; i < k; i++) {
+        Request* r = b[size_t(i)];
+        const int64_t np = sspp_batch_num_pairs(ctx, i), ne = sspp_batch_num_essential(ctx, i);
+        if (np < 0 || ne < 0) {
+            set_result(r, SSPP_ERR_CUDA, "result copy failed");
+            continue;
+        }
+        r->pairs.resize(size_t(2 * np));
+        r->ess.resize(size_t(ne));
+        if (sspp_batch_pairs(ctx, i, r->pairs.data(), np) != np || sspp_batch_essentials(ctx, i, r->ess.data(), ne) != ne)
+            set_result(r, SSPP_ERR_CUDA, "result copy failed");
+        else
+            set_result(r, SSPP_OK, nullptr);
+    }
+    return SSPP_OK;
+}
+
+void worker_main(sspp_server* S, int host_threads) {
+    sspp_config c;
+    std::memset(&c, 0, sizeof(c));
+    c.device = S->cfg.device;
+    c.host_threads = host_threads;
+    sspp_ctx* ctx = sspp_create(&c);
+    const size_t max_req = S->cfg.max_batch_requests > 0 ? size_t(S->cfg.max_batch_requests) : SIZE_MAX;
+    const int64_t max_cols = S->cfg.max_batch_cols > 0 ? S->cfg.max_batch_cols : INT64_MAX;
+    std::vector<Request*> batch;
+    for (;;) {
+        batch.clear();
+        {
+            std::unique_lock<std::mutex> l(S->mu);
+            S->cv_work.wait(l, [&] { return S->stop || !S->queue.empty(); });
+            if (S->queue.empty()) break;  // stopping and drained
+            if (S->cfg.batch_window_ms > 0 && !S->stop && S->queue.size() < max_req) {
+                S->cv_work.wait_for(l, std::chrono::duration<double, std::milli>(S->cfg.batch_window_ms),
+                                    [&] { return S->stop || S->queue.size() >= max_req; });
+                if (S->queue.empty()) continue;  // another worker took them
+            }
+            double est = 0;
+            int64_t cols = 0;
+            while (!S->queue.empty()) {
+                Request* r = S->queue.front();
+                if (!batch.empty() &&
+                    (est + r->est > S->share || cols + r->ncols > max_cols || batch.size() >= max_req))
+                    break;
+                S->queue.pop_front();
+                r->state = SSPP_REQ_RUNNING;
+                batch.push_back(r);
+                est += r->est;
+                cols += r->ncols;
+            }
+        }
+        int32_t rc = try_batch(ctx, S->params, batch);
+        if (rc != SSPP_OK && batch.size() > 1)  // isolate the request that failed
+            for (Request* r : batch) try_batch(ctx, S->params, {r});
+        {
+            std::lock_guard<std::mutex> l(S->mu);
+            const Clock::time_point now = Clock::now();
+            for (Request* r : batch) {
+                r->t_done = now;
+                r->state = r->status == SSPP_OK ? SSPP_REQ_DONE : SSPP_REQ_FAILED;
+                if (r->status == SSPP_OK) {
+                    S->completed++;
+                    S->columns += r->ncols;
+                    S->lat_ms.push_back(ms_between(r->t_submit, now));
+                } else {
+                    S->failed++;
+                }
+                // inputs are no longer needed
+                std::vector<int32_t>().swap(r->dims_copy);
+                std::vector<int64_t>().swap(r->colptr_copy);
+                std::vector<int32_t>().swap(r->rows_copy);
+                r->dims = nullptr;
+                r->colptr = nullptr;
+                r->rows = nullptr;
+            }
+            S->batches++;
+            S->batch_reqs += int64_t(batch.size());
+            S->t_last = now;
+        }
+        S->cv_done.notify_all();
+    }
+    if (ctx) sspp_destroy(ctx);
+}
+
+Request* find(sspp_server* S, int64_t id) {
+    auto it = S->reqs.find(id);
+    return it == S->reqs.end() ? nullptr : it->second.get();
+}
+
+bool finished(const Request* r) { return r->state == SSPP_REQ_DONE || r->state == SSPP_REQ_FAILED; }
+
+double percentile(std::vector<double> v, double q) {
+    if (v.empty()) return 0;
+    std::sort(v.begin(), v.end());
+    const double pos = q * double(v.size() - 1);
+    const size_t lo = size_t(std::floor(pos)), hi = std::min(v.size() - 1, lo + 1);
+    return v[lo] + (pos - double(lo)) * (v[hi] - v[lo]);
+}
+
+}  // namespace
+
+extern "C" {
+
+sspp_server* sspp_server_create(const sspp_server_config* cfg, const sspp_params* params) {
+    auto* S = new (std::nothrow) sspp_server;
+    if (!S) return nullptr;
+    if (cfg) S->cfg = *cfg;
+    if (params) S->params = *params;
+    else sspp_default_params(&S->params);
+    if (S->cfg.workers <= 0) S->cfg.workers = 2;
+    if (cudaSetDevice(S->cfg.device) != cudaSuccess) {
+        delete S;
+        return nullptr;
+    }
+    S->budget = double(S->cfg.memory_budget);
+    if (S->budget <= 0) {
+        size_t fr = 0, tot = 0;
+        if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+            delete S;
+            return nullptr;
+        }
+        S->budget = 0.85 * double(fr);
+    }
+    S->share = S->budget / double(S->cfg.workers);
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const int per = std::max(1, int(hw) / S->cfg.workers);
+    for (int w = 0; w < S->cfg.workers; w++) S->workers.emplace_back(worker_main, S, per);
+    return S;
+}
+
+void sspp_server_destroy(sspp_server* S) {
+    if (!S) return;
+    {
+        std::lock_guard<std::mutex> l(S->mu);
+        S->stop = true;
+    }
+    S->cv_work.notify_all();
+    for (auto& t : S->workers) t.join();
+    delete S;
+}
+
+const char* sspp_server_last_error(sspp_server* S) { return S ? S->err.c_str() : "null server"; }
+
+int64_t sspp_server_submit(sspp_server* S, int64_t ncols, const int32_t* dims, const int64_t* col_ptr,
+                           const int32_t* rows, int32_t flags) {
+    if (!S) return -SSPP_ERR_BAD_INPUT;
+    if (ncols < 0 || !col_ptr || (ncols > 0 && !dims) || col_ptr[0] != 0 || col_ptr[ncols] < 0 ||
+        (col_ptr[ncols] > 0 && !rows)) {
+        std::lock_guard<std::mutex> l(S->mu);
+        S->err = "bad request arrays";
+        S->rejected++;
+        return -SSPP_ERR_BAD_INPUT;
+    }
+    auto r = std::make_unique<Request>();
+    r->ncols = ncols;
+    r->nnz = col_ptr[ncols];
+    if (flags & SSPP_SUBMIT_NOCOPY) {
+        r->dims = dims;
+        r->colptr = col_ptr;
+        r->rows = rows;
+    } else {
+        r->dims_copy.assign(dims, dims + ncols);
+        r->colptr_copy.assign(col_ptr, col_ptr + ncols + 1);
+        r->rows_copy.assign(rows, rows + r->nnz);
+        r->dims = r->dims_copy.data();
+        r->colptr = r->colptr_copy.data();
+        r->rows = r->rows_copy.data();
+    }
+    r->est = estimate(S->params, ncols, r->nnz);
+    std::lock_guard<std::mutex> l(S->mu);
+    if (r->est > S->budget) {
+        S->err = "request larger than the device-memory budget";
+        S->rejected++;
+        return -SSPP_ERR_CAPACITY;
+    }
+    const int64_t id = S->next_id++;
+    r->id = id;
+    r->t_submit = Clock::now();
+    if (!S->have_first) {
+        S->have_first = true;
+        S->t_first = r->t_submit;
+    }
+    S->submitted++;
+    S->queue.push_back(r.get());
+    S->reqs.emplace(id, std::move(r));
+    S->cv_work.notify_one();
+    return id;
+}
+
+int32_t sspp_server_wait(sspp_server* S, int64_t id, double timeout_ms) {
+    if (!S) return SSPP_ERR_BAD_INPUT;
+    std::unique_lock<std::mutex> l(S->mu);
+    Request* r = find(S, id);
+    if (!r) return SSPP_ERR_STATE;
+    auto done = [&] { return finished(r); };
+    if (timeout_ms < 0) S->cv_done.wait(l, done);
+    else if (!S->cv_done.wait_for(l, std::chrono::duration<double, std::milli>(timeout_ms), done))
+        return SSPP_ERR_TIMEOUT;
+    return SSPP_OK;
+}
+
+int32_t sspp_server_state(sspp_server* S, int64_t id) {
+    if (!S) return -SSPP_ERR_BAD_INPUT;
+    std::lock_guard<std::mutex> l(S->mu);
+    Request* r = find(S, id);
+    return r ? r->state : -SSPP_ERR_STATE;
+}
+
+int32_t sspp_server_result(sspp_server* S, int64_t id, char* msg, int32_t msg_cap) {
+    if (!S) return SSPP_ERR_BAD_INPUT;
+    std::lock_guard<std::mutex> l(S->mu);
+    Request* r = find(S, id);
+    if (!r || !finished(r)) return SSPP_ERR_STATE;
+    if (msg && msg_cap > 0) {
+        std::strncpy(msg, r->msg.c_str(), size_t(msg_cap) - 1);
+        msg[msg_cap - 1] = 0;
+    }
+    return r->status;
+}
+
+int64_t sspp_server_num_pairs(sspp_server* S, int64_t id) {
+    if (!S) return -1;
+    std::lock_guard<std::mutex> l(S->mu);
+    Request* r = find(S, id);
+    if (!r || r->state != SSPP_REQ_DONE) return -1;
+    return int64_t(r->pairs.size() / 2);
+}
+
+int64_t sspp_server_pairs(sspp_server* S, int64_t id, int64_t* out, int64_t cap) {
+    if (!S || cap < 0 || (!out && cap > 0)) return -1;
+    std::lock_guard<std::mutex> l(S->mu);
+    Request* r = find(S, id);
+    if (!r || r->state != SSPP_REQ_DONE) return -1;
+    const int64_t n = std::min<int64_t>(cap, int64_t(r->pairs.size() / 2));
+    if (n > 0) std::memcpy(out, r->pairs.data(), sizeof(int64_t) * 2 * size_t(n));
+    return n;
+}
+
+int64_t sspp_server_num_essential(sspp_server* S, int64_t id) {
+    if (!S) return -1;
+    std::lock_guard<std::mutex> l(S->mu);
+    Request* r = find(S, id);
+    if (!r || r->state != SSPP_REQ_DONE) return -1;
+    return int64_t(r->ess.size());
+}
+
+int64_t sspp_server_essentials(sspp_server* S, int64_t id, int64_t* out, int64_t cap) {
+    if (!S || cap < 0 || (!out && cap > 0)) return -1;
+    std::lock_guard<std::mutex> l(S->mu);
+    Request* r = find(S, id);
+    if (!r || r->state != SSPP_REQ_DONE) return -1;
+    const int64_t n = std::min<int64_t>(cap, int64_t(r->ess.size()));
+    if (n > 0) std::memcpy(out, r->ess.data(), sizeof(int64_t) * size_t(n));
+    return n;
+}
+
+double sspp_server_latency_ms(sspp_server* S, int64_t id) {
+    if (!S) return -1;
+    std::lock_guard<std::mutex> l(S->mu);
+    Request* r = find(S, id);
+    if (!r || !finished(r)) return -1;
+    return ms_between(r->t_submit, r->t_done);
+}
+
+int32_t sspp_server_release(sspp_server* S, int64_t id) {
+    if (!S) return SSPP_ERR_BAD_INPUT;
+    std::lock_guard<std::mutex> l(S->mu);
+    auto it = S->reqs.find(id);
+    if (it == S->reqs.end() || !finished(it->second.get())) return SSPP_ERR_STATE;
+    S->reqs.erase(it);
+    return SSPP_OK;
+}
+
+int32_t sspp_server_get_stats(sspp_server* S, sspp_server_stats* o) {
+    if (!S || !o) return SSPP_ERR_BAD_INPUT;
+    std::lock_guard<std::mutex> l(S->mu);
+    std::memset(o, 0, sizeof(*o));
+    o->submitted = S->submitted;
+    o->completed = S->completed;
+    o->failed = S->failed;
+    o->rejected = S->rejected;
+    o->batches = S->batches;
+    o->columns = S->columns;
+    o->wall_s = (S->have_first && S->batches) ? ms_between(S->t_first, S->t_last) / 1000.0 : 0.0;
+    o->cols_per_s = o->wall_s > 0 ? double(S->columns) / o->wall_s : 0.0;
+    o->p50_ms = percentile(S->lat_ms, 0.50);
+    o->p95_ms = percentile(S->lat_ms, 0.95);
+    o->p99_ms = percentile(S->lat_ms, 0.99);
+    o->max_ms = S->lat_ms.empty() ? 0.0 : *std::max_element(S->lat_ms.begin(), S->lat_ms.end());
+    double sum = 0;
+    for (double x : S->lat_ms) sum += x;
+    o->mean_ms = S->lat_ms.empty() ? 0.0 : sum / double(S->lat_ms.size());
+    o->mean_batch_requests = S->batches ? double(S->batch_reqs) / double(S->batches) : 0.0;
+    return SSPP_OK;
+}
+
+int32_t sspp_server_reset_stats(sspp_server* S) {
+    if (!S) return SSPP_ERR_BAD_INPUT;
+    std::lock_guard<std::mutex> l(S->mu);
+    S->lat_ms.clear();
+    S->submitted = S->completed = S->failed = S->rejected = S->batches = S->columns = S->batch_reqs = 0;
+    S->have_first = false;
+    return SSPP_OK;
+}
+
+}  // extern "C"

@@ -80,8 +80,8 @@ Xfer::~Xfer() {
 
 HostPool& Xfer::pool() {
     if (!pool_) {
-        unsigned hw = std::thread::hardware_concurrency();
-        pool_ = new HostPool(int(std::max(1u, std::min(hw, 16u))));
+        const unsigned hw = std::max(1u, std::min(std::thread::hardware_concurrency(), 16u));
+        pool_ = new HostPool(threads_ > 0 ? std::min(threads_, int(hw)) : int(hw));
     }
     return *pool_;
 }

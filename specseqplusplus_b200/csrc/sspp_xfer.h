@@ -55,6 +55,7 @@ public:
     // device -> host; returns when every byte has landed in host memory
     cudaError_t d2h(const std::vector<Piece>& pieces, cudaStream_t s);
     HostPool& pool();
+    void set_threads(int n) { threads_ = n; }  // before the first copy; 0 = all cores
 
 private:
     cudaError_t ensure();
@@ -68,6 +69,7 @@ private:
     cudaEvent_t ev_[2] = {nullptr, nullptr};
     bool used_[2] = {false, false};
     HostPool* pool_ = nullptr;
+    int threads_ = 0;
 };
 
 }  // namespace sspp

@@ -31,7 +31,7 @@ class SsppError(RuntimeError):
 
 class _Config(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("arena_bytes", ctypes.c_int64), ("verbose", ctypes.c_int32),
-                ("profile", ctypes.c_int32)]
+                ("profile", ctypes.c_int32), ("host_threads", ctypes.c_int32)]
 
 
 class _Params(ctypes.Structure):
@@ -47,7 +47,20 @@ class _Stats(ctypes.Structure):
         "collapse_dropped", "additions", "add_ints", "published_ints", "displaced", "ss_steps", "npairs",
         "nessential")] + [("init_ms", ctypes.c_double), ("compute_ms", ctypes.c_double), ("launches", ctypes.c_int64)] + [
         (k, ctypes.c_double) for k in ("init_gpu_ms", "light_gpu_ms", "heavy_gpu_ms", "pairs_gpu_ms")] + [
-        ("light_launches", ctypes.c_int64), ("heavy_launches", ctypes.c_int64)]
+        ("light_launches", ctypes.c_int64), ("heavy_launches", ctypes.c_int64), ("arena_ints_used", ctypes.c_int64),
+        ("tuned_candidate", ctypes.c_int64)]
+
+
+class _ServerConfig(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int32), ("workers", ctypes.c_int32), ("memory_budget", ctypes.c_int64),
+                ("max_batch_cols", ctypes.c_int64), ("max_batch_requests", ctypes.c_int32),
+                ("batch_window_ms", ctypes.c_double)]
+
+
+class _ServerStats(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_int64) for k in ("submitted", "completed", "failed", "rejected", "batches", "columns")] + [
+        (k, ctypes.c_double) for k in ("wall_s", "cols_per_s", "p50_ms", "p95_ms", "p99_ms", "max_ms", "mean_ms",
+                                       "mean_batch_requests")]
 
 
 @dataclass
@@ -103,6 +116,24 @@ def load_library():
         "sspp_load_batch_device": (i32, [vp, i32, vp, vp, vp, vp]),
         "sspp_batch_num_pairs": (i64, [vp, i32]),
         "sspp_batch_pairs": (i64, [vp, i32, vp, i64]),
+        "sspp_get_params": (i32, [vp, ctypes.POINTER(_Params)]),
+        "sspp_batch_num_essential": (i64, [vp, i32]),
+        "sspp_batch_essentials": (i64, [vp, i32, vp, i64]),
+        "sspp_server_create": (vp, [ctypes.POINTER(_ServerConfig), ctypes.POINTER(_Params)]),
+        "sspp_server_destroy": (None, [vp]),
+        "sspp_server_last_error": (ctypes.c_char_p, [vp]),
+        "sspp_server_submit": (i64, [vp, i64, vp, vp, vp, i32]),
+        "sspp_server_wait": (i32, [vp, i64, ctypes.c_double]),
+        "sspp_server_state": (i32, [vp, i64]),
+        "sspp_server_result": (i32, [vp, i64, ctypes.c_char_p, i32]),
+        "sspp_server_num_pairs": (i64, [vp, i64]),
+        "sspp_server_pairs": (i64, [vp, i64, vp, i64]),
+        "sspp_server_num_essential": (i64, [vp, i64]),
+        "sspp_server_essentials": (i64, [vp, i64, vp, i64]),
+        "sspp_server_latency_ms": (ctypes.c_double, [vp, i64]),
+        "sspp_server_release": (i32, [vp, i64]),
+        "sspp_server_get_stats": (i32, [vp, ctypes.POINTER(_ServerStats)]),
+        "sspp_server_reset_stats": (i32, [vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -116,7 +147,11 @@ EXPORTED = ("sspp_create", "sspp_destroy", "sspp_last_error", "sspp_default_para
             "sspp_load_csc", "sspp_load_csc_device", "sspp_init", "sspp_compute", "sspp_reduce", "sspp_num_pairs",
             "sspp_pairs", "sspp_num_essential", "sspp_essentials", "sspp_write_pairs", "sspp_get_stats",
             "sspp_reduce_noalloc", "sspp_load_batch", "sspp_load_batch_device", "sspp_batch_num_pairs",
-            "sspp_batch_pairs")
+            "sspp_batch_pairs", "sspp_get_params", "sspp_batch_num_essential", "sspp_batch_essentials",
+            "sspp_server_create", "sspp_server_destroy", "sspp_server_last_error", "sspp_server_submit",
+            "sspp_server_wait", "sspp_server_state", "sspp_server_result", "sspp_server_num_pairs",
+            "sspp_server_pairs", "sspp_server_num_essential", "sspp_server_essentials", "sspp_server_latency_ms",
+            "sspp_server_release", "sspp_server_get_stats", "sspp_server_reset_stats")
 
 
 class Engine:
@@ -180,6 +215,15 @@ class Engine:
             self._check(ERR_CUDA)
         return out
 
+    def batch_essentials(self, i: int) -> np.ndarray:
+        n = self._lib.sspp_batch_num_essential(self._h, i)
+        if n < 0:
+            self._check(ERR_STATE)
+        out = np.empty(n, dtype=np.int64)
+        if self._lib.sspp_batch_essentials(self._h, i, out.ctypes.data, n) != n:
+            self._check(ERR_CUDA)
+        return out
+
     def load_phat(self, path: str, fmt: int = ASCII) -> None:
         self._check(self._lib.sspp_load_phat(self._h, path.encode(), fmt))
 
@@ -230,6 +274,12 @@ class Engine:
         st = _Stats()
         self._check(self._lib.sspp_get_stats(self._h, ctypes.byref(st)))
         return {k: getattr(st, k) for k, _ in _Stats._fields_}
+
+    def params(self) -> Params:
+        """Parameters of the last init, autotuned values included."""
+        p = _Params()
+        self._check(self._lib.sspp_get_params(self._h, ctypes.byref(p)))
+        return Params(*(getattr(p, f) for f, _ in _Params._fields_))
 
 
 def reduce_noalloc(ncols: int, nnz: int, d_dims: int, d_col_ptr: int, d_rows: int, d_pairs: int, d_npairs: int,
@@ -287,3 +337,106 @@ class SpecSeqPlusPlus:
 
     def stats(self) -> dict:
         return self._e.stats()
+
+
+REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
+
+
+class Server:
+    """Resident request loop with continuous batching (sspp_server_* in include/sspp.h).
+
+    submit() queues a complex and returns its id; workers reduce queued
+    requests in batches as they free up; wait() / pairs() / essentials() read
+    one request's results in its own indices.  With copy=False the matrix's
+    arrays are referenced, not copied, and kept alive here until release().
+    """
+
+    def __init__(self, params: Params | None = None, device: int = 0, workers: int = 2, memory_budget: int = 0,
+                 max_batch_cols: int = 0, max_batch_requests: int = 0, batch_window_ms: float = 0.0):
+        self._lib = load_library()
+        cfg = _ServerConfig(device, workers, memory_budget, max_batch_cols, max_batch_requests, batch_window_ms)
+        p = (params or Params())._c()
+        self._h = self._lib.sspp_server_create(ctypes.byref(cfg), ctypes.byref(p))
+        if not self._h:
+            raise SsppError(ERR_CUDA, "sspp_server_create failed (no usable CUDA device)")
+        self._keep = {}
+
+    def close(self) -> None:
+        if self._h:
+            self._lib.sspp_server_destroy(self._h)
+            self._h = None
+            self._keep.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, m, copy: bool = True) -> int:
+        dims = np.ascontiguousarray(m.dims, dtype=np.int32)
+        col_ptr = np.ascontiguousarray(m.col_ptr, dtype=np.int64)
+        rows = np.ascontiguousarray(m.rows if m.nnz else np.zeros(1, np.int32), dtype=np.int32)
+        rid = self._lib.sspp_server_submit(self._h, dims.shape[0], dims.ctypes.data, col_ptr.ctypes.data,
+                                           rows.ctypes.data, 0 if copy else 1)
+        if rid < 0:
+            raise SsppError(-rid, self._lib.sspp_server_last_error(self._h).decode(errors="replace"))
+        if not copy:
+            self._keep[rid] = (dims, col_ptr, rows)
+        return int(rid)
+
+    def wait(self, rid: int, timeout_ms: float = -1.0) -> bool:
+        rc = self._lib.sspp_server_wait(self._h, rid, timeout_ms)
+        if rc == ERR_TIMEOUT:
+            return False
+        if rc != OK:
+            raise SsppError(rc, "unknown request id")
+        return True
+
+    def state(self, rid: int) -> int:
+        return int(self._lib.sspp_server_state(self._h, rid))
+
+    def _raise_failed(self, rid: int) -> None:
+        buf = ctypes.create_string_buffer(512)
+        rc = self._lib.sspp_server_result(self._h, rid, buf, 512)
+        if rc != OK:
+            raise SsppError(rc, buf.value.decode(errors="replace"))
+
+    def pairs(self, rid: int) -> np.ndarray:
+        self.wait(rid)
+        self._raise_failed(rid)
+        n = self._lib.sspp_server_num_pairs(self._h, rid)
+        out = np.empty((max(n, 0), 2), dtype=np.int64)
+        if n > 0:
+            self._lib.sspp_server_pairs(self._h, rid, out.ctypes.data, n)
+        return out
+
+    def essentials(self, rid: int) -> np.ndarray:
+        self.wait(rid)
+        self._raise_failed(rid)
+        n = self._lib.sspp_server_num_essential(self._h, rid)
+        out = np.empty(max(n, 0), dtype=np.int64)
+        if n > 0:
+            self._lib.sspp_server_essentials(self._h, rid, out.ctypes.data, n)
+        return out
+
+    def latency_ms(self, rid: int) -> float:
+        return float(self._lib.sspp_server_latency_ms(self._h, rid))
+
+    def release(self, rid: int) -> None:
+        self._lib.sspp_server_release(self._h, rid)
+        self._keep.pop(rid, None)
+
+    def stats(self) -> dict:
+        st = _ServerStats()
+        self._lib.sspp_server_get_stats(self._h, ctypes.byref(st))
+        return {k: getattr(st, k) for k, _ in _ServerStats._fields_}
+
+    def reset_stats(self) -> None:
+        self._lib.sspp_server_reset_stats(self._h)

@@ -34,6 +34,20 @@ def test_python_mirror_binds_every_symbol():
     assert set(declared("sspp.h")) <= set(engine.EXPORTED) | {"sspp_default_params"}
 
 
+def test_server_without_a_gpu_fails_cleanly():
+    from specseqplusplus_b200 import Server, SsppError
+
+    try:
+        import torch
+
+        if torch.cuda.is_available():
+            pytest.skip("a GPU is present")
+    except ImportError:
+        pass
+    with pytest.raises(SsppError):
+        Server()
+
+
 def test_cli_help_and_argument_errors(tmp_path):
     assert os.path.exists(CLI)
     r = subprocess.run([CLI, "-help"], capture_output=True, text=True)

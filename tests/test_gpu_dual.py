@@ -1,4 +1,4 @@
-"""GPU parity of the dualized reduction (dualize = 1) against the oracle.
+"""GPU parity of the dualized reductions (dualize = 1 and 2) against the oracle.
 
 The dual matrix is the anti-transpose of the cleared and compressed boundary
 matrix (include/kernel.h:521-580, include/specseq.h:303-363); it is reduced
@@ -123,3 +123,50 @@ def test_dual_batch_and_class_mirror():
     alg.GPU_Init()
     alg.GPU_Compute()
     assert np.array_equal(alg.GetPersistencePairs(), oracle.reduce(m).pairs)
+
+
+# dualize = 2: the 0-dimensional pairs from the boundary matrix's edge columns,
+# then the coboundary matrix from dimension 1 up; the pairs never change
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_mode2_random_small_complexes(seed):
+    rng = np.random.default_rng(4000 + seed)
+    m = random_complex(rng, nverts=6 + seed % 5, p=0.65, maxdim=3)
+    want = dense_standard_pairs(m)
+    pairs, ess, _ = run(m, Params(dualize=2, ss_block_size=1 + seed % 5, level1_capacity=32,
+                                  level2_capacity=32 + 32 * (seed % 2)))
+    assert np.array_equal(pairs, want)
+    assert np.array_equal(ess, essentials_from_pairs(m.ncols, want))
+
+
+@pytest.mark.parametrize("p", [
+    Params(dualize=2),
+    Params(dualize=2, ss_block_size=64, growth=1.2, level1_capacity=32, level2_capacity=64),
+    Params(dualize=2, model=3, max_iteration=10),
+    Params(dualize=2, model=1, max_iteration=100, level1_capacity=32, level2_capacity=8192),
+])
+def test_mode2_matches_primal(p):
+    for m in (gen.rips(2000, 3, 1, 0.08, 3), gen.rips(1500, 2, 5, 0.06, 2), gen.lowerstar(16, 2.0, 2),
+              hub_complex(1500)):
+        ref = oracle.reduce(m, model=p.model, max_iteration=p.max_iteration)
+        pairs, ess, _ = run(m, p)
+        assert np.array_equal(pairs, ref.pairs)
+        assert np.array_equal(ess, ref.essential)
+
+
+def test_mode2_dense_rips_and_batch():
+    from specseqplusplus_b200 import workloads
+
+    m = gen.rips(1500, 3, 9, gen.rips_radius_for_degree(1500, 3, 35), 3)
+    ref = oracle.reduce(m, dualize=1)
+    pairs, ess, st = run(m, Params(dualize=2, level1_capacity=32))
+    assert np.array_equal(pairs, ref.pairs)
+    assert np.array_equal(ess, ref.essential)
+    mats, _ = workloads.batch_of_rips(12, seed=13, n_min=100, n_max=900)
+    with Engine(0) as e:
+        e.load_batch(mats)
+        e.reduce(Params(dualize=2, level1_capacity=32))
+        for i, mm in enumerate(mats):
+            assert np.array_equal(e.batch_pairs(i), oracle.reduce(mm).pairs), i
+            assert np.array_equal(e.batch_essentials(i), oracle.reduce(mm).essential), i

@@ -1,0 +1,134 @@
+"""GPU tests of the autotuner and of the serving loop (continuous batching).
+
+Every autotuner candidate gives the same pairs, so a class that cycles through
+all of them must keep matching the oracle.  The server must give each request
+exactly the result the same complex gets when reduced alone, whatever batch it
+landed in and whatever arrived around it; a malformed request fails alone; a
+request above the device-memory budget is refused at submission.
+"""
+import threading
+import time
+
+import numpy as np
+import pytest
+
+import oracle
+from helpers import random_complex
+from specseqplusplus_b200 import Engine, Params, Server, SsppError, gen
+
+pytestmark = pytest.mark.gpu
+
+
+def alone(m, p):
+    with Engine(0) as e:
+        e.load_csc(m)
+        e.reduce(p)
+        return e.pairs(), e.essentials()
+
+
+@pytest.mark.parametrize("autotune", [1, 2])
+def test_autotune_cycles_candidates_with_identical_pairs(autotune):
+    cases = [gen.rips(1500, 3, 4, 0.1, 3), gen.lowerstar(14, 1.5, 3)]
+    refs = [oracle.reduce(m) for m in cases]
+    seen = set()
+    with Engine(0) as e:
+        for rep in range(10):
+            for m, ref in zip(cases, refs):
+                e.load_csc(m)
+                e.reduce(Params(autotune=autotune))
+                st = e.stats()
+                p = e.params()
+                seen.add((p.ss_block_size, p.level1_capacity, p.level2_capacity, p.heavy_threads, p.dualize))
+                assert st["tuned_candidate"] >= 0
+                assert np.array_equal(e.pairs(), ref.pairs), (rep, p)
+                assert np.array_equal(e.essentials(), ref.essential)
+    assert len(seen) >= (8 if autotune == 2 else 4)
+
+
+def _mix(seed):
+    rng = np.random.default_rng(seed)
+    mats = []
+    for i in range(36):
+        kind = i % 4
+        if kind == 0:
+            mats.append(gen.rips(int(rng.integers(100, 1500)), 2, int(rng.integers(1 << 30)), 0.08, 2))
+        elif kind == 1:
+            mats.append(gen.rips(int(rng.integers(100, 1200)), 3, int(rng.integers(1 << 30)), 0.15, 3))
+        elif kind == 2:
+            mats.append(gen.lowerstar(int(rng.integers(4, 14)), 1.5, int(rng.integers(1 << 30))))
+        else:
+            mats.append(random_complex(rng, nverts=8, p=0.6, maxdim=3))
+    mats.append(gen.BoundaryMatrix.from_columns([0, 0, 0], [[], [], []]))
+    mats.append(gen.BoundaryMatrix.from_columns([], []))
+    return mats
+
+
+@pytest.mark.parametrize("p,workers", [(Params(), 2), (Params(model=3, max_iteration=10, dualize=1), 3),
+                                       (Params(autotune=2), 2)])
+def test_server_results_same_alone_and_in_mix(p, workers):
+    mats = _mix(7)
+    want = [alone(m, p) for m in mats]
+    ids = [None] * len(mats)
+    with Server(p, workers=workers, batch_window_ms=2.0) as srv:
+        def submitter():
+            rng = np.random.default_rng(1)
+            for i, m in enumerate(mats):
+                ids[i] = srv.submit(m, copy=(i % 2 == 0))
+                time.sleep(float(rng.exponential(0.002)))
+
+        th = threading.Thread(target=submitter)
+        th.start()
+        th.join()
+        for i, m in enumerate(mats):
+            assert np.array_equal(srv.pairs(ids[i]), want[i][0]), i
+            assert np.array_equal(srv.essentials(ids[i]), want[i][1]), i
+            assert srv.latency_ms(ids[i]) > 0
+        st = srv.stats()
+        assert st["completed"] == len(mats) and st["failed"] == 0
+        assert st["batches"] < len(mats)  # some requests shared a batch
+        assert 0 < st["p50_ms"] <= st["p95_ms"] <= st["p99_ms"] <= st["max_ms"]
+    for i in range(0, len(mats), 7):
+        assert np.array_equal(want[i][0], oracle.reduce(mats[i], dualize=p.dualize, model=p.model,
+                                                        max_iteration=p.max_iteration).pairs)
+
+
+def test_server_failure_is_isolated():
+    good = [gen.rips(300, 2, s, 0.12, 2) for s in range(6)]
+    bad = gen.BoundaryMatrix(np.array([0, 0, 1], np.int32), np.array([0, 0, 0, 2], np.int64),
+                             np.array([0, 7], np.int32))  # face index out of range
+    with Server(Params(), workers=1, batch_window_ms=20.0) as srv:
+        ids = [srv.submit(m) for m in good[:3]] + [srv.submit(bad)] + [srv.submit(m) for m in good[3:]]
+        for rid in ids:
+            srv.wait(rid)
+        with pytest.raises(SsppError) as ei:
+            srv.pairs(ids[3])
+        assert ei.value.code == 1
+        for rid, m in zip(ids[:3] + ids[4:], good):
+            assert np.array_equal(srv.pairs(rid), oracle.reduce(m).pairs)
+        st = srv.stats()
+        assert st["failed"] == 1 and st["completed"] == 6
+
+
+def test_server_refuses_requests_above_budget():
+    with Server(Params(), workers=1, memory_budget=1 << 20) as srv:
+        with pytest.raises(SsppError) as ei:
+            srv.submit(gen.lowerstar(12, 1.0, 1))
+        assert ei.value.code == 2
+        rid = srv.submit(gen.BoundaryMatrix.from_columns([0, 0], [[], []]))
+        assert len(srv.essentials(rid)) == 2
+        srv.release(rid)
+        assert srv.state(rid) < 0
+
+
+def test_batch_rejects_face_outside_its_complex():
+    # a face index that would be valid in the concatenation but not in its own complex
+    good = gen.rips(200, 2, 1, 0.15, 2)
+    bad = gen.BoundaryMatrix(np.array([0, 0, 1], np.int32), np.array([0, 0, 0, 2], np.int64),
+                             np.array([0, 7], np.int32))
+    with Engine(0) as e:
+        with pytest.raises(SsppError) as ei:
+            e.load_batch([good, bad])
+        assert ei.value.code == 1
+        e.load_batch([good, good])
+        e.reduce(Params())
+        assert np.array_equal(e.batch_pairs(1), oracle.reduce(good).pairs)
