@@ -23,6 +23,17 @@ seeded data stands in for the reference's input files.
 Multi-GPU: one process per GPU (torchrun); a single reduction does not shard,
 so every rank reduces its own replica of the workload (request-level weak
 scaling, no collective on the data path); value = total columns / max time.
+
+Extra keys (rank 0, after the timed legs; --no-extra skips them):
+  rips2000  2,000-point Rips, model 0, reference default parameters (e2e)
+  vr100k    100,000-point Rips, model 3, max_iteration 100 (collapse +
+            guided clearing), with the reduction's roofline
+  batched   512 uneven Rips complexes reduced as one batch (autotuned) vs the
+            same 512 one at a time with the reference's default parameters
+  served    a seeded Poisson request stream through the serving loop vs a
+            serial one-at-a-time loop: columns/s and p50/p95/p99 latency
+Every leg checks its pairs (against the oracle, or against the plain path
+whose pairs are checked against the oracle on a sample).
 """
 from __future__ import annotations
 
@@ -34,6 +45,8 @@ import subprocess
 import sys
 import tempfile
 import time
+
+import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
@@ -115,8 +128,7 @@ def load_traffic():
 
 
 def oracle_run(m):
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle
+    oracle = oracle_module()
 
     t = time.perf_counter()
     r = oracle.reduce(m, model=MODEL, max_iteration=MAX_ITER)
@@ -149,6 +161,213 @@ def reference_arm(args):
     return 0
 
 
+# ------------------------------------------------------------------ extra legs
+# Each returns a dict added to the JSON line under its own key.  Host timers
+# (time.perf_counter) bracket whole calls that end with the results in host
+# memory, so these are end-to-end numbers through the public API.
+
+def _timed(fn):
+    t = time.perf_counter()
+    out = fn()
+    return time.perf_counter() - t, out
+
+
+def leg_rips2000(steps):
+    """2,000 points in [0,1]^3, radius 0.08, dim <= 3, model 0 (reference defaults)."""
+    from specseqplusplus_b200 import Engine, Params, gen
+
+    m = gen.rips(2000, 3, 1, 0.08, 3)
+    p = Params()
+    with Engine(0) as e:
+        for _ in range(3):
+            e.load_csc(m)
+            e.reduce(p)
+        ts = []
+        for _ in range(max(steps, 5)):
+            dt, _ = _timed(lambda: (e.load_csc(m), e.reduce(p), e.pairs(), e.essentials()))
+            ts.append(dt)
+        pr = e.pairs()
+    ref = oracle_module().reduce(m)
+    return {"workload": "Rips 2000 pts [0,1]^3 r 0.08 dim<=3, model 0, reference default parameters",
+            "ncols": m.ncols, "cols_per_s_e2e": m.ncols / statistics.median(ts), "ms_e2e": 1000 * statistics.median(ts),
+            "pairs_exact": bool(np.array_equal(pr, ref.pairs))}
+
+
+def leg_vr100k(steps, peak):
+    """100,000 points, radius 0.016, dim <= 3, model 3 (collapse + guided clearing, max_iteration 100)."""
+    import torch
+
+    from specseqplusplus_b200 import Engine, Params, gen
+
+    m = gen.rips(100000, 3, 7, 0.016, 3)
+    p = Params(model=3, max_iteration=100, queue_size=65536, level1_capacity=100, level2_capacity=250)
+    dev = torch.device("cuda", 0)
+    d = [torch.from_numpy(x).to(dev) for x in (m.dims, m.col_ptr, m.rows)]
+    stream = torch.cuda.current_stream(dev)
+    with Engine(0, profile=1) as e:
+        e.load_csc_device(m.ncols, d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr())
+        for _ in range(3):
+            e.reduce(p, stream=stream.cuda_stream)
+        dev_ms, host_ms, red_ms = [], [], []
+        for _ in range(max(steps, 5)):
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            a.record(stream)
+            e.reduce(p, stream=stream.cuda_stream)
+            b.record(stream)
+            torch.cuda.synchronize()
+            host_ms.append(1000 * (time.perf_counter() - t0))
+            dev_ms.append(a.elapsed_time(b))
+            st = e.stats()
+            red_ms.append(st["light_gpu_ms"] + st["heavy_gpu_ms"])
+        pr, es = e.pairs(), e.essentials()
+        st = e.stats()
+    ref = oracle_module().reduce(m, model=3, max_iteration=100)
+    exact = bool(np.array_equal(pr, ref.pairs) and np.array_equal(es, ref.essential))
+    rms = statistics.median(red_ms)
+    ach = ref.stats["add_bytes"] / (rms / 1000) / 1e9 if rms > 0 else None
+    return {"workload": "Rips 100k pts [0,1]^3 r 0.016 dim<=3, model 3, max_iteration 100, queue 65536, L1/L2 100/250",
+            "ncols": m.ncols, "nnz": m.nnz, "cols_per_s": m.ncols / (statistics.median(host_ms) / 1000),
+            "device_ms": statistics.median(dev_ms), "host_ms": statistics.median(host_ms),
+            "collapse_dropped": st["collapse_dropped"], "highclear_cleared": st["highclear_cleared"],
+            "reduction_gpu_ms": rms, "additions": st["additions"],
+            "roofline": {"bound": "hbm", "kernel": "reduction", "achieved": ach, "peak": peak, "unit": "GB/s",
+                         "frac": (ach / peak) if ach else None, "algorithmic_bytes": ref.stats["add_bytes"],
+                         "note": "about 1 MB of input: latency-bound, not bandwidth-bound"},
+            "pairs_exact": exact}
+
+
+def leg_batched(steps):
+    """512 Rips complexes (200-5,000 points log-uniform, half 2-D dim<=2, half 3-D dim<=3, mean degree 8-40),
+    reduced together (one block-diagonal reduction, autotuned) vs one at a time."""
+    from specseqplusplus_b200 import Engine, Params, workloads
+
+    mats, _ = workloads.batch_of_rips(512)
+    N = sum(m.ncols for m in mats)
+    p_auto, p_ref = Params(autotune=1), Params()
+    with Engine(0) as e:
+        for _ in range(6):  # the autotuner tries its candidates on this size class first
+            e.load_batch(mats)
+            e.reduce(p_auto)
+            e.batch_results()
+        ts = []
+        for _ in range(max(steps, 3)):
+            dt, res = _timed(lambda: (e.load_batch(mats), e.reduce(p_auto), e.batch_results())[2])
+            ts.append(dt)
+        chosen = e.params()
+
+    def one_at_a_time(p, reps):
+        with Engine(0) as e1:
+            for m in mats:  # warm-up (and, with autotune, the per-class trials)
+                for _ in range(reps):
+                    e1.load_csc(m)
+                    e1.reduce(p)
+            out = []
+            t = time.perf_counter()
+            for m in mats:
+                e1.load_csc(m)
+                e1.reduce(p)
+                out.append((e1.pairs(), e1.essentials()))
+            return time.perf_counter() - t, out
+
+    t_ref, plain = one_at_a_time(p_ref, 1)
+    t_auto, _ = one_at_a_time(p_auto, 5)
+    same = all(np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]) for a, b in zip(res, plain))
+    orc = oracle_module()
+    sample = list(range(0, len(mats), 32))
+    exact = all(np.array_equal(res[i][0], orc.reduce(mats[i]).pairs) for i in sample)
+    tb = statistics.median(ts)
+    return {"workload": "512 Rips complexes, 200-5000 pts log-uniform, half 2-D (dim<=2) half 3-D (dim<=3), "
+                        "mean degree U[8,40], per-instance seeds",
+            "ncols": N, "batched_cols_per_s": N / tb, "batched_ms": 1000 * tb,
+            "plain_cols_per_s": N / t_ref, "plain_ms": 1000 * t_ref,
+            "plain_autotuned_cols_per_s": N / t_auto,
+            "speedup_vs_plain": t_ref / tb, "speedup_vs_plain_autotuned": t_auto / tb,
+            "batched_params": {"level1_capacity": chosen.level1_capacity, "level2_capacity": chosen.level2_capacity,
+                               "ss_block_size": chosen.ss_block_size, "growth": chosen.growth,
+                               "heavy_threads": chosen.heavy_threads},
+            "plain_params": "reference defaults (level capacities 1000/8000, ss_block_size 102400, growth 1.05, "
+                            "queue_size 65536)",
+            "pairs_equal_plain_all": bool(same), "pairs_exact_oracle_sample": bool(exact),
+            "oracle_sample": f"{len(sample)} of {len(mats)} instances (every 32nd)"}
+
+
+def leg_served(count=48, rates=(100.0, None)):
+    """Poisson request stream (Rips 300-20,000 pts 2-D/3-D degree 8-40; lower-star 16^3-96^3 sigma 1-3):
+    the serving loop (2 workers, autotuned, continuous batching) vs a serial one-at-a-time loop."""
+    from specseqplusplus_b200 import Engine, Params, Server, workloads
+
+    stream = workloads.serving_stream(count, 1.0, seed=5)
+    mats = [m for _, _, m, _ in stream]
+    gaps = np.diff([0.0] + [a for a, _, _, _ in stream])
+    N = sum(m.ncols for m in mats)
+    warm = [m for _, _, m, _ in workloads.serving_stream(16, 1.0, seed=99)]
+    out = {"workload": f"{count} requests, Poisson arrivals (seeded); 75% Rips 300-20000 pts (2-D/3-D, degree "
+                       f"8-40, dim<=3), 25% lower-star 16^3-96^3 sigma 1-3",
+           "ncols": N, "max_request_cols": max(m.ncols for m in mats), "rates": []}
+    plain_results = None
+    for rate in rates:
+        arrivals = np.cumsum(gaps / rate) if rate else np.zeros(count)
+
+        def plain(p):
+            with Engine(0) as e:
+                for _ in range(2):
+                    for m in warm:
+                        e.load_csc(m)
+                        e.reduce(p)
+                lat, res = [], []
+                t0 = time.perf_counter()
+                for a, m in zip(arrivals, mats):
+                    now = time.perf_counter() - t0
+                    if now < a:
+                        time.sleep(a - now)
+                    e.load_csc(m)
+                    e.reduce(p)
+                    res.append((e.pairs(), e.essentials()))
+                    lat.append(1000 * (time.perf_counter() - t0 - a))
+                return N / (time.perf_counter() - t0 - arrivals[0]), np.percentile(lat, [50, 95, 99]), res
+
+        cp, lp, pres = plain(Params())
+        if plain_results is None:
+            plain_results = pres
+        with Server(Params(autotune=1), workers=2) as srv:
+            for _ in range(2):
+                ids = [srv.submit(m, copy=False) for m in warm]
+                for i in ids:
+                    srv.wait(i)
+                    srv.release(i)
+            srv.reset_stats()
+            ids = []
+            t0 = time.perf_counter()
+            for a, m in zip(arrivals, mats):
+                now = time.perf_counter() - t0
+                if now < a:
+                    time.sleep(a - now)
+                ids.append(srv.submit(m, copy=False))
+            for i in ids:
+                srv.wait(i)
+            st = srv.stats()
+            same = all(np.array_equal(srv.pairs(i), r[0]) and np.array_equal(srv.essentials(i), r[1])
+                       for i, r in zip(ids, plain_results))
+        out["rates"].append({"rate_per_s": rate if rate else "all at once",
+                             "served_cols_per_s": st["cols_per_s"], "served_p50_ms": st["p50_ms"],
+                             "served_p95_ms": st["p95_ms"], "served_p99_ms": st["p99_ms"],
+                             "served_mean_batch": st["mean_batch_requests"],
+                             "plain_cols_per_s": cp, "plain_p50_ms": float(lp[0]), "plain_p95_ms": float(lp[1]),
+                             "plain_p99_ms": float(lp[2]), "speedup_vs_plain": st["cols_per_s"] / cp,
+                             "results_equal_plain": bool(same)})
+    return out
+
+
+def oracle_module():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    return oracle
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -158,6 +377,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grid", type=int, default=GRID, help="smaller grid for profiling runs (default 64)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the batched, served, 2000-point Rips and 100k-point VR legs")
     args = ap.parse_args()
     if args.grid != GRID:
         globals()["GRID"] = args.grid
@@ -291,7 +512,11 @@ def main():
                "sample": f"full workload ({n} columns), one run, single-threaded C++ restatement"}
     ph = {k: v / args.steps for k, v in phases.items()}
     init_bytes = 16 * nnz + 8 * n           # CSC read three times and written once, pivot + low tables
-    red_ms = ph["light_gpu_ms"] + ph["heavy_gpu_ms"]
+    # the heavy-tier launches overlap each other on side streams, so the
+    # reduction's device time is the step's event time less the phases that
+    # run alone on the main stream (init passes, pair extraction)
+    red_ms = min(ph["light_gpu_ms"] + ph["heavy_gpu_ms"],
+                 total_ms / args.steps - ph["init_gpu_ms"] - ph["pairs_gpu_ms"])
     candidates = {"init_passes": (ph["init_gpu_ms"], init_bytes),
                   "reduction": (red_ms, alg_add_bytes if alg_add_bytes is not None else None)}
     dom = max(candidates, key=lambda k: candidates[k][0])
@@ -303,6 +528,11 @@ def main():
         roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "kernel": dom, "peak_kind": peak_kind,
                 "algorithmic_bytes_per_step": dom_bytes, "device_ms_per_step": dom_ms}
+    init_roof = None
+    if ph["init_gpu_ms"] > 0:
+        ia = init_bytes / (ph["init_gpu_ms"] / 1000) / 1e9
+        init_roof = {"bound": "hbm", "achieved": ia, "peak": peak, "unit": "GB/s", "frac": ia / peak,
+                     "algorithmic_bytes_per_step": init_bytes, "device_ms_per_step": ph["init_gpu_ms"]}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
@@ -313,9 +543,14 @@ def main():
             "phases_ms_per_step": ph,
             "launches_per_step": {"total": launches // args.steps, "light": light_launches // args.steps,
                                   "heavy": heavy_launches // args.steps},
-            "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
+            "roofline": roof, "roofline_init": init_roof, "cpu_baseline": cpu, "clocks": clk,
             "stats": {k: st[k] for k in ("active_after_init", "apparent_pairs", "cleared_init", "highclear_cleared",
                                          "additions", "displaced", "ss_steps", "npairs", "nessential")}}
+    if not args.no_extra:
+        line["rips2000"] = leg_rips2000(args.steps)
+        line["vr100k"] = leg_vr100k(args.steps, peak)
+        line["batched"] = leg_batched(args.steps)
+        line["served"] = leg_served()
     print(json.dumps(line), flush=True)
     return 0
 

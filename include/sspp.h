@@ -159,6 +159,12 @@ int64_t sspp_batch_num_pairs(sspp_ctx* ctx, int32_t i);
 int64_t sspp_batch_pairs(sspp_ctx* ctx, int32_t i, int64_t* out_birth_death, int64_t cap);
 int64_t sspp_batch_num_essential(sspp_ctx* ctx, int32_t i);
 int64_t sspp_batch_essentials(sspp_ctx* ctx, int32_t i, int64_t* out, int64_t cap);
+/* Bulk form for large batches: sspp_batch_counts writes every complex's pair
+ * and essential counts (arrays of k, either may be NULL); sspp_batch_copy then
+ * fills pairs_out[i] (2 * npairs[i] int64) and ess_out[i] (ness[i] int64) in
+ * the complexes' own indices in one staged copy (NULL entries are skipped). */
+int32_t sspp_batch_counts(sspp_ctx* ctx, int64_t* npairs, int64_t* ness);
+int32_t sspp_batch_copy(sspp_ctx* ctx, int64_t* const* pairs_out, int64_t* const* ess_out);
 
 /* Replaces: writeVectorToFile (src/main.cu:191-229). */
 int32_t sspp_write_pairs(sspp_ctx* ctx, const char* path, int32_t fmt);
@@ -198,6 +204,8 @@ typedef struct sspp_server_stats {
     double cols_per_s;           /* columns of completed requests / wall_s         */
     double p50_ms, p95_ms, p99_ms, max_ms, mean_ms;
     double mean_batch_requests;
+    double load_s, reduce_s, results_s;  /* host time in each batch phase, summed
+                                            over workers                        */
 } sspp_server_stats;
 
 /* request states */

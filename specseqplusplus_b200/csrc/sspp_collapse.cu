@@ -389,11 +389,12 @@ __global__ void k_empty_dropped(int64_t n, int32_t* arena, uint64_t* desc, const
     if ((threadIdx.x & 31) == 0 && cnt) cnt_add(&counters[CNT_DROPPED], cnt);
 }
 
+// stream-ordered, like the engine's other buffers
 template <typename T>
-cudaError_t grow_buf(T*& p, int64_t want) {
-    if (p) cudaFree(p);
+cudaError_t grow_buf(T*& p, int64_t want, cudaStream_t s) {
+    if (p) cudaFreeAsync(p, s);
     p = nullptr;
-    return cudaMalloc(&p, size_t(want > 0 ? want : 1) * sizeof(T));
+    return cudaMallocAsync(reinterpret_cast<void**>(&p), size_t(want > 0 ? want : 1) * sizeof(T), s);
 }
 
 }  // namespace
@@ -416,17 +417,17 @@ int collapse(Device& D, const DimInfo& info, uint8_t* dropped, CollapseScratch& 
     if (ne == 0 || nv == 0) return 0;
     *err_msg = "edge collapse: device allocation failed";
     if (ne > S.cap_e) {
-        if (grow_buf(S.eu, ne) || grow_buf(S.ev, ne) || grow_buf(S.ecol, ne) || grow_buf(S.adj, 2 * ne) ||
-            grow_buf(S.arr, ne) || grow_buf(S.crit, ne) || grow_buf(S.ins, ne) || grow_buf(S.heap, ne) ||
-            grow_buf(S.cas, ne))
+        if (grow_buf(S.eu, ne, s) || grow_buf(S.ev, ne, s) || grow_buf(S.ecol, ne, s) || grow_buf(S.adj, 2 * ne, s) ||
+            grow_buf(S.arr, ne, s) || grow_buf(S.crit, ne, s) || grow_buf(S.ins, ne, s) || grow_buf(S.heap, ne, s) ||
+            grow_buf(S.cas, ne, s))
             return -1;
         S.cap_e = ne;
     }
     if (nv + 1 > S.cap_v) {
-        if (grow_buf(S.deg, nv + 1) || grow_buf(S.adj_off, nv + 1)) return -1;
+        if (grow_buf(S.deg, nv + 1, s) || grow_buf(S.adj_off, nv + 1, s)) return -1;
         S.cap_v = nv + 1;
     }
-    if (!S.misc && grow_buf(S.misc, 8)) return -1;
+    if (!S.misc && grow_buf(S.misc, 8, s)) return -1;
     cudaMemsetAsync(S.misc, 0, 8 * sizeof(int32_t), s);
     // edge list: the 2-row columns of dimension 1, in filtration order
     {
@@ -483,7 +484,7 @@ int collapse(Device& D, const DimInfo& info, uint8_t* dropped, CollapseScratch& 
     const int64_t gcap = maxdeg > kCapB ? maxdeg : 0;
     const int64_t want = std::max<int64_t>(warps_a * per_warp, 3 * gcap) + 1;
     if (want > S.cap_cbuf) {
-        if (grow_buf(S.cbuf, want)) return -1;
+        if (grow_buf(S.cbuf, want, s)) return -1;
         S.cap_cbuf = want;
     }
     k_arrival<<<unsigned(warps_a / kWarpsA), kWarpsA * 32, 0, s>>>(

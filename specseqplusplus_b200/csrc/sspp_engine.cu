@@ -103,6 +103,7 @@ struct sspp_ctx {
     std::vector<int64_t> host_pairs;
     bool host_pairs_valid = false;
     std::vector<int64_t> host_ess;     // essentials, copied back once for slicing
+    std::vector<int64_t> batch_bounds; // per-complex pair and essential slice starts
     bool host_ess_valid = false;
     int64_t launches = 0, light_launches = 0, heavy_launches = 0;
 };
@@ -122,13 +123,17 @@ int set_err(sspp_ctx* c, int code, const std::string& msg) {
             return set_err(ctx, SSPP_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));    \
     } while (0)
 
+// Device buffers are stream-ordered allocations: growing one neither
+// synchronises the device nor waits for other contexts' work, as cudaFree
+// would (the server runs several contexts side by side).  Freed memory stays
+// in the device's pool for reuse.
 template <typename T>
-cudaError_t grow(T*& p, int64_t& cap, int64_t want) {
+cudaError_t grow(T*& p, int64_t& cap, int64_t want, cudaStream_t s) {
     if (want <= cap && p) return cudaSuccess;
-    if (p) cudaFree(p);
+    if (p) cudaFreeAsync(p, s);
     p = nullptr;
     cap = 0;
-    cudaError_t e = cudaMalloc(&p, size_t(std::max<int64_t>(want, 1)) * sizeof(T));
+    cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&p), size_t(std::max<int64_t>(want, 1)) * sizeof(T), s);
     if (e == cudaSuccess) cap = want;
     return e;
 }
@@ -151,8 +156,8 @@ int ensure_columns(sspp_ctx* ctx, int64_t n, int64_t nnz) {
         auto g = [&](auto*& p, int64_t mult) {
             using T = std::remove_reference_t<decltype(*p)>;
             int64_t cap = 0;
-            if (p) { cudaFree(p); p = nullptr; }
-            return grow<T>(p, cap, c * mult + 1);
+            if (p) { cudaFreeAsync(p, ctx->stream); p = nullptr; }
+            return grow<T>(p, cap, c * mult + 1, ctx->stream);
         };
         CK(g(D.dim, 1));
         CK(g(D.perm, 1));
@@ -171,9 +176,9 @@ int ensure_columns(sspp_ctx* ctx, int64_t n, int64_t nnz) {
         CK(g(D.ess, 1));
         D.cap_n = c;
         int64_t nb = (c + 4095) / 4096 + 2;
-        CK(grow(D.blk, D.cap_blk, nb));
+        CK(grow(D.blk, D.cap_blk, nb, ctx->stream));
         int64_t nbp = (c + 255) / 256 + 1;
-        CK(grow(D.dimcnt, D.cap_dimcnt, nbp * kNumDims));
+        CK(grow(D.dimcnt, D.cap_dimcnt, nbp * kNumDims, ctx->stream));
     }
     if (!D.diminfo) {
         CK(cudaMalloc(&D.diminfo, sizeof(DimInfo)));
@@ -193,10 +198,10 @@ constexpr int64_t kArenaGuard = 8192;
 int ensure_arena(sspp_ctx* ctx, int64_t ints) {
     Device& D = ctx->D;
     if (ints <= D.arena_cap) return SSPP_OK;
-    if (D.arena) cudaFree(D.arena);
+    if (D.arena) cudaFreeAsync(D.arena, ctx->stream);
     D.arena = nullptr;
     D.arena_cap = 0;
-    CK(cudaMalloc(&D.arena, size_t(ints + kArenaGuard) * sizeof(int32_t)));
+    CK(cudaMallocAsync(reinterpret_cast<void**>(&D.arena), size_t(ints + kArenaGuard) * sizeof(int32_t), ctx->stream));
     D.arena_cap = ints;
     return SSPP_OK;
 }
@@ -299,10 +304,10 @@ int run_collapse(sspp_ctx* ctx) {
     Device& D = ctx->D;
     cudaStream_t s = ctx->stream;
     if (D.n > ctx->cap_dropped) {
-        if (ctx->dropped) cudaFree(ctx->dropped);
+        if (ctx->dropped) cudaFreeAsync(ctx->dropped, s);
         ctx->dropped = nullptr;
         ctx->cap_dropped = 0;
-        CK(grow(ctx->dropped, ctx->cap_dropped, D.n));
+        CK(grow(ctx->dropped, ctx->cap_dropped, D.n, s));
     }
     CK(cudaMemcpyAsync(ctx->h_info, D.diminfo, sizeof(DimInfo), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
@@ -329,16 +334,16 @@ int run_highclear(sspp_ctx* ctx) {
         if (info.col_end[d] > info.col_begin[d]) { top = d; break; }
     if (top < 1) return SSPP_OK;
     for (int d = 1; d <= top; d++)
-        CK(grow(S.tup[d], S.cap_tup[d], int64_t(d + 1) * (info.col_end[d] - info.col_begin[d]) + 1));
+        CK(grow(S.tup[d], S.cap_tup[d], int64_t(d + 1) * (info.col_end[d] - info.col_begin[d]) + 1, s));
     const int64_t nv = info.col_end[0] - info.col_begin[0];
     const int64_t ne = info.col_end[1] - info.col_begin[1];
-    CK(grow(S.deg, S.cap_deg, nv + 2));
-    CK(grow(S.adj_off, S.cap_adj_off, nv + 2));
-    CK(grow(S.adj, S.cap_adj, 2 * ne + 1));
+    CK(grow(S.deg, S.cap_deg, nv + 2, s));
+    CK(grow(S.adj_off, S.cap_adj_off, nv + 2, s));
+    CK(grow(S.adj, S.cap_adj, 2 * ne + 1, s));
     const int64_t ntop = info.col_end[top] - info.col_begin[top];
     int64_t slots = 1024;
     while (slots < 2 * ntop) slots *= 2;
-    CK(grow(S.table, S.cap_table, slots));
+    CK(grow(S.table, S.cap_table, slots, s));
     S.mask = uint32_t(slots - 1);
     ctx->launches += highclear(D, info, ctx->params.max_iteration, dropped_of(ctx), S, s);
     return SSPP_OK;
@@ -412,20 +417,20 @@ int run_steps(sspp_ctx* ctx, const std::vector<Step>& steps, int cap1, int cap2,
     cudaStream_t s = ctx->stream;
     const sspp_params& P = ctx->params;
     if (4 * int64_t(steps.size()) > D.cap_steps) {
-        if (D.step_ctr) cudaFree(D.step_ctr);
+        if (D.step_ctr) cudaFreeAsync(D.step_ctr, s);
         D.step_ctr = nullptr;
         D.cap_steps = 0;
-        CK(grow(D.step_ctr, D.cap_steps, 4 * int64_t(steps.size()) + 64));
+        CK(grow(D.step_ctr, D.cap_steps, 4 * int64_t(steps.size()) + 64, s));
     }
     if (!steps.empty()) CK(cudaMemsetAsync(D.step_ctr, 0, sizeof(int) * 4 * steps.size(), s));
     // heavy pool: deferrals are rare (heavy columns and displaced owners); a
     // full pool sets the capacity bit and the run is repeated with a larger one
     const int64_t want_pool = std::max<int64_t>(ctx->pool_request, std::max<int64_t>(D.n / 4, 1 << 16));
     if (want_pool > D.pool_cap) {
-        if (D.heavy) cudaFree(D.heavy);
+        if (D.heavy) cudaFreeAsync(D.heavy, s);
         D.heavy = nullptr;
         D.pool_cap = 0;
-        CK(grow(D.heavy, D.pool_cap, want_pool));
+        CK(grow(D.heavy, D.pool_cap, want_pool, s));
     }
     CK(cudaMemsetAsync(D.pool_tail, 0, sizeof(int), s));
     const int light_max = std::max(1, ctx->num_sms * ctx->light_blocks_per_sm);
@@ -587,22 +592,22 @@ int load_common(sspp_ctx* ctx, int64_t n, int64_t nnz) {
 // Device buffers for inputs copied from the host (grown, never shrunk).
 int ensure_own(sspp_ctx* ctx, int64_t n, int64_t nnz) {
     if (n + 1 > ctx->cap_own_n) {
-        if (ctx->own_dims) cudaFree(ctx->own_dims);
-        if (ctx->own_colptr) cudaFree(ctx->own_colptr);
+        if (ctx->own_dims) cudaFreeAsync(ctx->own_dims, ctx->stream);
+        if (ctx->own_colptr) cudaFreeAsync(ctx->own_colptr, ctx->stream);
         ctx->own_dims = nullptr;
         ctx->own_colptr = nullptr;
         ctx->cap_own_n = 0;
         int64_t c1 = 0, c2 = 0;
-        CK(grow(ctx->own_dims, c1, n + 1));
-        CK(grow(ctx->own_colptr, c2, n + 1));
+        CK(grow(ctx->own_dims, c1, n + 1, ctx->stream));
+        CK(grow(ctx->own_colptr, c2, n + 1, ctx->stream));
         ctx->cap_own_n = n + 1;
     }
     if (nnz > ctx->cap_own_nnz || !ctx->own_rows) {
-        if (ctx->own_rows) cudaFree(ctx->own_rows);
+        if (ctx->own_rows) cudaFreeAsync(ctx->own_rows, ctx->stream);
         ctx->own_rows = nullptr;
         ctx->cap_own_nnz = 0;
         int64_t c3 = 0;
-        CK(grow(ctx->own_rows, c3, std::max<int64_t>(nnz, 1)));
+        CK(grow(ctx->own_rows, c3, std::max<int64_t>(nnz, 1), ctx->stream));
         ctx->cap_own_nnz = std::max<int64_t>(nnz, 1);
     }
     return SSPP_OK;
@@ -642,6 +647,13 @@ sspp_ctx* sspp_create(const sspp_config* cfg) {
     }
     ctx->stream = ctx->own_stream;
     cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->cfg.device);
+    {  // keep freed stream-ordered allocations in the pool (no release at synchronisations)
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, ctx->cfg.device) == cudaSuccess) {
+            uint64_t keep = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+    }
     if (cudaMallocHost(&ctx->h_err, sizeof(int)) != cudaSuccess ||
         cudaMallocHost(&ctx->h_counters, sizeof(long long) * CNT_NUM) != cudaSuccess ||
         cudaMallocHost(&ctx->h_info, sizeof(DimInfo)) != cudaSuccess ||
@@ -759,18 +771,19 @@ int32_t sspp_load_batch(sspp_ctx* ctx, int32_t k, const int64_t* ncols, const in
     if (rc) return rc;
     rc = ensure_own(ctx, n, nnz);
     if (rc) return rc;
-    CK(grow(ctx->d_batch, ctx->cap_d_batch, int64_t(starts.size()) + 1));  // + the bad-index flag
+    // starts (2 (k+1)), the bad-index flag, then the result slice starts (2 (k+1))
+    CK(grow(ctx->d_batch, ctx->cap_d_batch, 2 * int64_t(starts.size()) + 1, ctx->stream));
     cudaStream_t s = ctx->stream;
     // the complexes side by side; indices are shifted on the device
     std::vector<Piece> pcs;
     pcs.reserve(size_t(3) * size_t(k) + 1);
     for (int32_t i = 0; i < k; i++)
-        pcs.push_back({dims[i], ctx->own_dims + cst[i], sizeof(int32_t) * size_t(ncols[i])});
+        pcs.push_back({dims[i], ctx->own_dims + cst[i], sizeof(int32_t) * size_t(ncols[i]), 0});
     for (int32_t i = 0; i < k; i++)
-        pcs.push_back({col_ptr[i] + 1, ctx->own_colptr + cst[i] + 1, sizeof(int64_t) * size_t(ncols[i])});
+        pcs.push_back({col_ptr[i] + 1, ctx->own_colptr + cst[i] + 1, sizeof(int64_t) * size_t(ncols[i]), 1});
     for (int32_t i = 0; i < k; i++)
-        pcs.push_back({rows[i], ctx->own_rows + est[i], sizeof(int32_t) * size_t(est[i + 1] - est[i])});
-    pcs.push_back({starts.data(), ctx->d_batch, sizeof(int64_t) * starts.size()});
+        pcs.push_back({rows[i], ctx->own_rows + est[i], sizeof(int32_t) * size_t(est[i + 1] - est[i]), 2});
+    pcs.push_back({starts.data(), ctx->d_batch, sizeof(int64_t) * starts.size(), 3});
     int* d_bad = reinterpret_cast<int*>(ctx->d_batch + starts.size());
     CK(cudaMemsetAsync(ctx->own_colptr, 0, sizeof(int64_t), s));
     CK(cudaMemsetAsync(d_bad, 0, sizeof(int), s));
@@ -802,6 +815,10 @@ int32_t sspp_load_batch_device(sspp_ctx* ctx, int32_t k, const int64_t* ncols, c
     }
     int rc = sspp_load_csc_device(ctx, starts[size_t(k)], d_dims, d_col_ptr, d_rows);
     if (rc) return rc;
+    CK(grow(ctx->d_batch, ctx->cap_d_batch, 4 * (int64_t(k) + 1) + 1, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->d_batch, starts.data(), sizeof(int64_t) * starts.size(), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
     ctx->batch_start = starts;
     return SSPP_OK;
 }
@@ -891,6 +908,64 @@ int64_t sspp_batch_essentials(sspp_ctx* ctx, int32_t i, int64_t* out, int64_t ca
     const int64_t n = std::min(cap, e - b);
     for (int64_t t = 0; t < n; t++) out[t] = ctx->host_ess[size_t(b + t)] - off;
     return n;
+}
+
+// Bulk results of a batch: per-complex counts, then one staged copy of every
+// complex's pairs and essentials (indices made local on the device).
+int32_t sspp_batch_counts(sspp_ctx* ctx, int64_t* npairs, int64_t* ness) {
+    if (!ctx) return SSPP_ERR_BAD_INPUT;
+    cudaSetDevice(ctx->cfg.device);
+    if (!ctx->computed || ctx->batch_start.empty()) return set_err(ctx, SSPP_ERR_STATE, "no reduced batch");
+    const int32_t k = int32_t(ctx->batch_start.size()) - 1;
+    const int64_t np = ctx->hcounters[CNT_NPAIRS], ne = ctx->hcounters[CNT_NESS];
+    int64_t* d_cstart = ctx->d_batch;
+    int64_t* d_ps = ctx->d_batch + 2 * (int64_t(k) + 1) + 1;
+    int64_t* d_es = d_ps + k + 1;
+    cudaStream_t s = ctx->stream;
+    batch_bounds(k, d_cstart, np, ctx->D.pairs, ne, ctx->D.ess, d_ps, d_es, s);
+    ctx->batch_bounds.resize(2 * (size_t(k) + 1));
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(ctx->batch_bounds.data(), d_ps, sizeof(int64_t) * 2 * (size_t(k) + 1), cudaMemcpyDeviceToHost,
+                       s));
+    CK(cudaStreamSynchronize(s));
+    const int64_t* ps = ctx->batch_bounds.data();
+    const int64_t* es = ps + k + 1;
+    for (int32_t i = 0; i < k; i++) {
+        if (npairs) npairs[i] = (i + 1 < k ? ps[i + 1] : np) - ps[i];
+        if (ness) ness[i] = (i + 1 < k ? es[i + 1] : ne) - es[i];
+    }
+    return SSPP_OK;
+}
+
+int32_t sspp_batch_copy(sspp_ctx* ctx, int64_t* const* pairs_out, int64_t* const* ess_out) {
+    if (!ctx) return SSPP_ERR_BAD_INPUT;
+    cudaSetDevice(ctx->cfg.device);
+    const int32_t k = int32_t(ctx->batch_start.size()) - 1;
+    if (!ctx->computed || k < 0 || ctx->batch_bounds.size() != 2 * (size_t(k) + 1))
+        return set_err(ctx, SSPP_ERR_STATE, "call sspp_batch_counts first");
+    const int64_t np = ctx->hcounters[CNT_NPAIRS], ne = ctx->hcounters[CNT_NESS];
+    Device& D = ctx->D;
+    cudaStream_t s = ctx->stream;
+    // local copies live in buffers the reduction no longer needs: 2 np <= n, ne <= n
+    int64_t* lp = D.death_of;
+    int64_t* le = D.scratch64;
+    batch_localize(np, ne, k, ctx->d_batch, D.pairs, D.ess, lp, le, s);
+    CK(cudaGetLastError());
+    const int64_t* ps = ctx->batch_bounds.data();
+    const int64_t* es = ps + k + 1;
+    std::vector<Piece> pcs;
+    pcs.reserve(2 * size_t(k));
+    for (int32_t i = 0; i < k; i++) {
+        const int64_t a = ps[i], b = i + 1 < k ? ps[i + 1] : np;
+        if (b > a && pairs_out && pairs_out[i])
+            pcs.push_back({lp + 2 * a, pairs_out[i], sizeof(int64_t) * 2 * size_t(b - a), -1});
+    }
+    for (int32_t i = 0; i < k; i++) {
+        const int64_t a = es[i], b = i + 1 < k ? es[i + 1] : ne;
+        if (b > a && ess_out && ess_out[i]) pcs.push_back({le + a, ess_out[i], sizeof(int64_t) * size_t(b - a), -1});
+    }
+    CK(ctx->xfer.d2h(pcs, s));
+    return SSPP_OK;
 }
 
 int32_t sspp_load_phat(sspp_ctx* ctx, const char* path, int32_t fmt) {

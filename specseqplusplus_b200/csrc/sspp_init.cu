@@ -117,6 +117,59 @@ int batch_rebase(int64_t n, int64_t nnz, int32_t k, const int64_t* d_cstart, con
     return 1;
 }
 
+// Per-complex result slices of a batch: the sorted pairs (by birth) and the
+// ascending essentials of complex i start at the first entry >= cstart[i].
+__global__ void k_batch_bounds(int32_t k, const int64_t* cstart, int64_t npairs, const int64_t* pairs, int64_t ness,
+                               const int64_t* ess, int64_t* pstart, int64_t* estart) {
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i <= k; i += gridDim.x * blockDim.x) {
+        const int64_t x = cstart[i];
+        int64_t lo = 0, hi = npairs;
+        while (lo < hi) {
+            const int64_t m = (lo + hi) >> 1;
+            if (pairs[2 * m] < x) lo = m + 1;
+            else hi = m;
+        }
+        pstart[i] = lo;
+        lo = 0;
+        hi = ness;
+        while (lo < hi) {
+            const int64_t m = (lo + hi) >> 1;
+            if (ess[m] < x) lo = m + 1;
+            else hi = m;
+        }
+        estart[i] = lo;
+    }
+}
+
+// pairs and essentials in their own complex's indices
+__global__ void k_batch_localize(int64_t npairs, int64_t ness, int32_t k, const int64_t* cstart, const int64_t* pairs,
+                                 const int64_t* ess, int64_t* lpairs, int64_t* less) {
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < npairs; t += stride) {
+        const int64_t b = pairs[2 * t], o = cstart[batch_member(cstart, k, b)];
+        lpairs[2 * t] = b - o;
+        lpairs[2 * t + 1] = pairs[2 * t + 1] - o;
+    }
+    for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < ness; t += stride)
+        less[t] = ess[t] - cstart[batch_member(cstart, k, ess[t])];
+}
+
+int batch_bounds(int32_t k, const int64_t* d_cstart, int64_t npairs, const int64_t* pairs, int64_t ness,
+                 const int64_t* ess, int64_t* d_pstart, int64_t* d_estart, cudaStream_t s) {
+    k_batch_bounds<<<grid_for(int64_t(k) + 1, 128), 128, 0, s>>>(k, d_cstart, npairs, pairs, ness, ess, d_pstart,
+                                                                 d_estart);
+    return 1;
+}
+
+int batch_localize(int64_t npairs, int64_t ness, int32_t k, const int64_t* d_cstart, const int64_t* pairs,
+                   const int64_t* ess, int64_t* lpairs, int64_t* less, cudaStream_t s) {
+    const int64_t m = npairs > ness ? npairs : ness;
+    if (m == 0) return 0;
+    k_batch_localize<<<grid_for(m, 256) > 16384 ? 16384 : grid_for(m, 256), 256, 0, s>>>(npairs, ness, k, d_cstart,
+                                                                                         pairs, ess, lpairs, less);
+    return 1;
+}
+
 // ------------------------------------------------------------------ reorder
 constexpr int kPartThreads = 256;
 

@@ -22,6 +22,13 @@ int batch_rebase(int64_t n, int64_t nnz, int32_t k, const int64_t* d_cstart, con
 int reorder(Device& D, cudaStream_t s);
 int64_t reorder_total_slot(const Device& D);  // index into D.blk of the arena total
 
+// per-complex slice starts (k+1 each) of the sorted pairs and essentials
+int batch_bounds(int32_t k, const int64_t* d_cstart, int64_t npairs, const int64_t* pairs, int64_t ness,
+                 const int64_t* ess, int64_t* d_pstart, int64_t* d_estart, cudaStream_t s);
+// pairs / essentials with each complex's first column subtracted
+int batch_localize(int64_t npairs, int64_t ness, int32_t k, const int64_t* d_cstart, const int64_t* pairs,
+                   const int64_t* ess, int64_t* lpairs, int64_t* less, cudaStream_t s);
+
 int init_passes(Device& D, cudaStream_t s);
 int init_compress(Device& D, const uint8_t* dropped, cudaStream_t s);
 int active_list(Device& D, cudaStream_t s);

@@ -38,6 +38,7 @@
 // cancelled pairs before it (one ballot/prefix per round for both lists): no
 // atomics, no scratch in global memory.
 #include <climits>
+#include <mutex>
 
 #include "sspp_kernels.cuh"
 #include "sspp_launch.h"
@@ -856,21 +857,37 @@ void reduce_heavy_launch(const Device& D, int cap, int threads, int* ctr, int gr
     else k_reduce_heavy<128><<<grid, 128, heavy_smem_bytes(cap), s>>>(A);
 }
 
+// The dynamic shared-memory limit is a property of the kernel (per device),
+// shared by every context of the process: contexts with different capacities
+// (the server's workers, each autotuned) only ever raise it, under a lock, so
+// that no launch finds it lowered below its own request.
+static cudaError_t raise_smem_limit(const void* fn, int slot, int bytes) {
+    static std::mutex mu;
+    static int limit[64][3] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> l(mu);
+    int& cur = limit[dev & 63][slot];
+    if (bytes <= cur) return cudaSuccess;
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) cur = bytes;
+    return e;
+}
+
 cudaError_t reduce_configure(int cap1, int cap2, int heavy_threads, int* light_blocks_per_sm,
                              int* heavy_blocks_per_sm) {
-    cudaError_t e = cudaFuncSetAttribute(k_reduce_light, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         light_smem_bytes(cap1));
+    cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(k_reduce_light), 0, light_smem_bytes(cap1));
     if (e != cudaSuccess) return e;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(light_blocks_per_sm, k_reduce_light, 128, light_smem_bytes(cap1));
     if (e != cudaSuccess) return e;
     if (heavy_threads == 256) {
-        e = cudaFuncSetAttribute(k_reduce_heavy<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 heavy_smem_bytes(cap2));
+        e = raise_smem_limit(reinterpret_cast<const void*>(k_reduce_heavy<256>), 1, heavy_smem_bytes(cap2));
         if (e != cudaSuccess) return e;
         return cudaOccupancyMaxActiveBlocksPerMultiprocessor(heavy_blocks_per_sm, k_reduce_heavy<256>, 256,
                                                              heavy_smem_bytes(cap2));
     }
-    e = cudaFuncSetAttribute(k_reduce_heavy<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, heavy_smem_bytes(cap2));
+    e = raise_smem_limit(reinterpret_cast<const void*>(k_reduce_heavy<128>), 2, heavy_smem_bytes(cap2));
     if (e != cudaSuccess) return e;
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(heavy_blocks_per_sm, k_reduce_heavy<128>, 128,
                                                          heavy_smem_bytes(cap2));

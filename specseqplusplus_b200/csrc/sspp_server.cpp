@@ -45,8 +45,14 @@ struct Request {
     int state = SSPP_REQ_QUEUED;
     int32_t status = SSPP_OK;
     std::string msg;
-    std::vector<int64_t> pairs, ess;
+    // results (uninitialised storage: filled by the staged copy's threads)
+    std::unique_ptr<int64_t[]> pairs, ess;
+    int64_t npairs = 0, ness = 0;
     Clock::time_point t_submit, t_done;
+};
+
+struct Phases {
+    double load = 0, reduce = 0, results = 0;  // seconds
 };
 
 double ms_between(Clock::time_point a, Clock::time_point b) {
@@ -71,6 +77,8 @@ struct sspp_server {
     int64_t submitted = 0, completed = 0, failed = 0, rejected = 0, batches = 0, columns = 0, batch_reqs = 0;
     bool have_first = false;
     Clock::time_point t_first, t_last;
+    Phases phases;
+    int64_t queued_cols = 0;  // columns of the queued requests
 };
 
 namespace {
@@ -90,7 +98,7 @@ void set_result(Request* r, int32_t status, const char* msg) {
 }
 
 // one batch through one context; SSPP_OK when every request has its results
-int32_t try_batch(sspp_ctx* ctx, const sspp_params& params, const std::vector<Request*>& b) {
+int32_t try_batch(sspp_ctx* ctx, const sspp_params& params, const std::vector<Request*>& b, Phases& ph) {
     if (!ctx) {
         for (Request* r : b) set_result(r, SSPP_ERR_CUDA, "no usable CUDA device");
         return SSPP_ERR_CUDA;
@@ -105,27 +113,34 @@ int32_t try_batch(sspp_ctx* ctx, const sspp_params& params, const std::vector<Re
         cp[i] = b[i]->colptr;
         rw[i] = b[i]->rows;
     }
+    const Clock::time_point t0 = Clock::now();
     int32_t rc = sspp_load_batch(ctx, k, nc.data(), d.data(), cp.data(), rw.data());
+    const Clock::time_point t1 = Clock::now();
     if (rc == SSPP_OK) rc = sspp_reduce(ctx, &params, nullptr);
+    const Clock::time_point t2 = Clock::now();
+    ph.load += ms_between(t0, t1) / 1000.0;
+    ph.reduce += ms_between(t1, t2) / 1000.0;
     if (rc != SSPP_OK) {
         for (Request* r : b) set_result(r, rc, sspp_last_error(ctx));
         return rc;
     }
-    for (int32_t i = 0; i < k; i++) {
-        Request* r = b[size_t(i)];
-        const int64_t np = sspp_batch_num_pairs(ctx, i), ne = sspp_batch_num_essential(ctx, i);
-        if (np < 0 || ne < 0) {
-            set_result(r, SSPP_ERR_CUDA, "result copy failed");
-            continue;
+    std::vector<int64_t> np(b.size()), ne(b.size());
+    rc = sspp_batch_counts(ctx, np.data(), ne.data());
+    std::vector<int64_t*> po(b.size()), eo(b.size());
+    if (rc == SSPP_OK) {
+        for (size_t i = 0; i < b.size(); i++) {
+            b[i]->npairs = np[i];
+            b[i]->ness = ne[i];
+            b[i]->pairs.reset(new int64_t[size_t(std::max<int64_t>(2 * np[i], 1))]);
+            b[i]->ess.reset(new int64_t[size_t(std::max<int64_t>(ne[i], 1))]);
+            po[i] = b[i]->pairs.get();
+            eo[i] = b[i]->ess.get();
         }
-        r->pairs.resize(size_t(2 * np));
-        r->ess.resize(size_t(ne));
-        if (sspp_batch_pairs(ctx, i, r->pairs.data(), np) != np || sspp_batch_essentials(ctx, i, r->ess.data(), ne) != ne)
-            set_result(r, SSPP_ERR_CUDA, "result copy failed");
-        else
-            set_result(r, SSPP_OK, nullptr);
+        rc = sspp_batch_copy(ctx, po.data(), eo.data());
     }
-    return SSPP_OK;
+    ph.results += ms_between(t2, Clock::now()) / 1000.0;
+    for (Request* r : b) set_result(r, rc, rc == SSPP_OK ? nullptr : sspp_last_error(ctx));
+    return rc;
 }
 
 void worker_main(sspp_server* S, int host_threads) {
@@ -148,25 +163,33 @@ void worker_main(sspp_server* S, int host_threads) {
                                     [&] { return S->stop || S->queue.size() >= max_req; });
                 if (S->queue.empty()) continue;  // another worker took them
             }
+            // a fair share of the queued columns, so that the other workers'
+            // batches (and their copies) overlap with this one
+            const int64_t fair = (S->queued_cols + S->cfg.workers - 1) / S->cfg.workers;
             double est = 0;
             int64_t cols = 0;
             while (!S->queue.empty()) {
                 Request* r = S->queue.front();
-                if (!batch.empty() &&
-                    (est + r->est > S->share || cols + r->ncols > max_cols || batch.size() >= max_req))
+                if (!batch.empty() && (est + r->est > S->share || cols + r->ncols > max_cols ||
+                                       batch.size() >= max_req || cols >= fair))
                     break;
                 S->queue.pop_front();
+                S->queued_cols -= r->ncols;
                 r->state = SSPP_REQ_RUNNING;
                 batch.push_back(r);
                 est += r->est;
                 cols += r->ncols;
             }
         }
-        int32_t rc = try_batch(ctx, S->params, batch);
+        Phases ph;
+        int32_t rc = try_batch(ctx, S->params, batch, ph);
         if (rc != SSPP_OK && batch.size() > 1)  // isolate the request that failed
-            for (Request* r : batch) try_batch(ctx, S->params, {r});
+            for (Request* r : batch) try_batch(ctx, S->params, {r}, ph);
         {
             std::lock_guard<std::mutex> l(S->mu);
+            S->phases.load += ph.load;
+            S->phases.reduce += ph.reduce;
+            S->phases.results += ph.results;
             const Clock::time_point now = Clock::now();
             for (Request* r : batch) {
                 r->t_done = now;
@@ -294,6 +317,7 @@ int64_t sspp_server_submit(sspp_server* S, int64_t ncols, const int32_t* dims, c
         S->t_first = r->t_submit;
     }
     S->submitted++;
+    S->queued_cols += r->ncols;
     S->queue.push_back(r.get());
     S->reqs.emplace(id, std::move(r));
     S->cv_work.notify_one();
@@ -336,7 +360,7 @@ int64_t sspp_server_num_pairs(sspp_server* S, int64_t id) {
     std::lock_guard<std::mutex> l(S->mu);
     Request* r = find(S, id);
     if (!r || r->state != SSPP_REQ_DONE) return -1;
-    return int64_t(r->pairs.size() / 2);
+    return r->npairs;
 }
 
 int64_t sspp_server_pairs(sspp_server* S, int64_t id, int64_t* out, int64_t cap) {
@@ -344,8 +368,8 @@ int64_t sspp_server_pairs(sspp_server* S, int64_t id, int64_t* out, int64_t cap)
     std::lock_guard<std::mutex> l(S->mu);
     Request* r = find(S, id);
     if (!r || r->state != SSPP_REQ_DONE) return -1;
-    const int64_t n = std::min<int64_t>(cap, int64_t(r->pairs.size() / 2));
-    if (n > 0) std::memcpy(out, r->pairs.data(), sizeof(int64_t) * 2 * size_t(n));
+    const int64_t n = std::min<int64_t>(cap, r->npairs);
+    if (n > 0) std::memcpy(out, r->pairs.get(), sizeof(int64_t) * 2 * size_t(n));
     return n;
 }
 
@@ -354,7 +378,7 @@ int64_t sspp_server_num_essential(sspp_server* S, int64_t id) {
     std::lock_guard<std::mutex> l(S->mu);
     Request* r = find(S, id);
     if (!r || r->state != SSPP_REQ_DONE) return -1;
-    return int64_t(r->ess.size());
+    return r->ness;
 }
 
 int64_t sspp_server_essentials(sspp_server* S, int64_t id, int64_t* out, int64_t cap) {
@@ -362,8 +386,8 @@ int64_t sspp_server_essentials(sspp_server* S, int64_t id, int64_t* out, int64_t
     std::lock_guard<std::mutex> l(S->mu);
     Request* r = find(S, id);
     if (!r || r->state != SSPP_REQ_DONE) return -1;
-    const int64_t n = std::min<int64_t>(cap, int64_t(r->ess.size()));
-    if (n > 0) std::memcpy(out, r->ess.data(), sizeof(int64_t) * size_t(n));
+    const int64_t n = std::min<int64_t>(cap, r->ness);
+    if (n > 0) std::memcpy(out, r->ess.get(), sizeof(int64_t) * size_t(n));
     return n;
 }
 
@@ -404,6 +428,9 @@ int32_t sspp_server_get_stats(sspp_server* S, sspp_server_stats* o) {
     for (double x : S->lat_ms) sum += x;
     o->mean_ms = S->lat_ms.empty() ? 0.0 : sum / double(S->lat_ms.size());
     o->mean_batch_requests = S->batches ? double(S->batch_reqs) / double(S->batches) : 0.0;
+    o->load_s = S->phases.load;
+    o->reduce_s = S->phases.reduce;
+    o->results_s = S->phases.results;
     return SSPP_OK;
 }
 
@@ -413,6 +440,7 @@ int32_t sspp_server_reset_stats(sspp_server* S) {
     S->lat_ms.clear();
     S->submitted = S->completed = S->failed = S->rejected = S->batches = S->columns = S->batch_reqs = 0;
     S->have_first = false;
+    S->phases = Phases();
     return SSPP_OK;
 }
 

@@ -168,7 +168,9 @@ cudaError_t Xfer::h2d(const std::vector<Piece>& pieces, cudaStream_t s) {
         for (size_t k = 0; k < segs.size();) {  // one DMA per run contiguous on the device
             uint8_t* d0 = static_cast<uint8_t*>(pieces[segs[k].piece].dst) + segs[k].off;
             size_t len = segs[k].len, k2 = k + 1;
-            while (k2 < segs.size() && static_cast<uint8_t*>(pieces[segs[k2].piece].dst) + segs[k2].off == d0 + len)
+            const int grp = pieces[segs[k].piece].group;
+            while (k2 < segs.size() && grp >= 0 && pieces[segs[k2].piece].group == grp &&
+                   static_cast<uint8_t*>(pieces[segs[k2].piece].dst) + segs[k2].off == d0 + len)
                 len += segs[k2++].len;
             if ((e = cudaMemcpyAsync(d0, st + segs[k].so, len, cudaMemcpyHostToDevice, s)) != cudaSuccess) return e;
             k = k2;
@@ -209,7 +211,8 @@ cudaError_t Xfer::d2h(const std::vector<Piece>& pieces, cudaStream_t s) {
             for (size_t k = 0; k < cur.size();) {  // one DMA per run contiguous on the device
                 const uint8_t* s0 = static_cast<const uint8_t*>(pieces[cur[k].piece].src) + cur[k].off;
                 size_t len = cur[k].len, k2 = k + 1;
-                while (k2 < cur.size() &&
+                const int grp = pieces[cur[k].piece].group;
+                while (k2 < cur.size() && grp >= 0 && pieces[cur[k2].piece].group == grp &&
                        static_cast<const uint8_t*>(pieces[cur[k2].piece].src) + cur[k2].off == s0 + len)
                     len += cur[k2++].len;
                 if ((e = cudaMemcpyAsync(st + cur[k].so, s0, len, cudaMemcpyDeviceToHost, s)) != cudaSuccess)

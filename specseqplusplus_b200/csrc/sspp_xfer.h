@@ -37,10 +37,14 @@ private:
     bool stop_ = false;
 };
 
+// One copy.  Consecutive pieces of the same group (>= 0) that are adjacent on
+// the device are moved by one DMA; a group must lie inside one allocation (a
+// copy may not span two stream-ordered allocations, adjacent or not).
 struct Piece {
     const void* src;
     void* dst;
     size_t bytes;
+    int group = -1;
 };
 
 class Xfer {

@@ -60,7 +60,7 @@ class _ServerConfig(ctypes.Structure):
 class _ServerStats(ctypes.Structure):
     _fields_ = [(k, ctypes.c_int64) for k in ("submitted", "completed", "failed", "rejected", "batches", "columns")] + [
         (k, ctypes.c_double) for k in ("wall_s", "cols_per_s", "p50_ms", "p95_ms", "p99_ms", "max_ms", "mean_ms",
-                                       "mean_batch_requests")]
+                                       "mean_batch_requests", "load_s", "reduce_s", "results_s")]
 
 
 @dataclass
@@ -119,6 +119,8 @@ def load_library():
         "sspp_get_params": (i32, [vp, ctypes.POINTER(_Params)]),
         "sspp_batch_num_essential": (i64, [vp, i32]),
         "sspp_batch_essentials": (i64, [vp, i32, vp, i64]),
+        "sspp_batch_counts": (i32, [vp, vp, vp]),
+        "sspp_batch_copy": (i32, [vp, vp, vp]),
         "sspp_server_create": (vp, [ctypes.POINTER(_ServerConfig), ctypes.POINTER(_Params)]),
         "sspp_server_destroy": (None, [vp]),
         "sspp_server_last_error": (ctypes.c_char_p, [vp]),
@@ -148,6 +150,7 @@ EXPORTED = ("sspp_create", "sspp_destroy", "sspp_last_error", "sspp_default_para
             "sspp_pairs", "sspp_num_essential", "sspp_essentials", "sspp_write_pairs", "sspp_get_stats",
             "sspp_reduce_noalloc", "sspp_load_batch", "sspp_load_batch_device", "sspp_batch_num_pairs",
             "sspp_batch_pairs", "sspp_get_params", "sspp_batch_num_essential", "sspp_batch_essentials",
+            "sspp_batch_counts", "sspp_batch_copy",
             "sspp_server_create", "sspp_server_destroy", "sspp_server_last_error", "sspp_server_submit",
             "sspp_server_wait", "sspp_server_state", "sspp_server_result", "sspp_server_num_pairs",
             "sspp_server_pairs", "sspp_server_num_essential", "sspp_server_essentials", "sspp_server_latency_ms",
@@ -188,6 +191,7 @@ class Engine:
         rows = np.ascontiguousarray(m.rows, dtype=np.int32)
         self._check(self._lib.sspp_load_csc(self._h, dims.shape[0], dims.ctypes.data, col_ptr.ctypes.data,
                                             rows.ctypes.data))
+        self._batch_k = 0
 
     def load_csc_device(self, ncols: int, d_dims: int, d_col_ptr: int, d_rows: int) -> None:
         self._check(self._lib.sspp_load_csc_device(self._h, ncols, d_dims, d_col_ptr, d_rows))
@@ -201,10 +205,12 @@ class Engine:
         ncols = np.array([m.ncols for m in ms], dtype=np.int64)
         arr = lambda i: (ctypes.c_void_p * max(k, 1))(*[t[i].ctypes.data for t in keep])
         self._check(self._lib.sspp_load_batch(self._h, k, ncols.ctypes.data, arr(0), arr(1), arr(2)))
+        self._batch_k = k
 
     def load_batch_device(self, ncols, d_dims: int, d_col_ptr: int, d_rows: int) -> None:
         nc = np.ascontiguousarray(ncols, dtype=np.int64)
         self._check(self._lib.sspp_load_batch_device(self._h, nc.shape[0], nc.ctypes.data, d_dims, d_col_ptr, d_rows))
+        self._batch_k = int(nc.shape[0])
 
     def batch_pairs(self, i: int) -> np.ndarray:
         n = self._lib.sspp_batch_num_pairs(self._h, i)
@@ -214,6 +220,18 @@ class Engine:
         if self._lib.sspp_batch_pairs(self._h, i, out.ctypes.data, n) != n:
             self._check(ERR_CUDA)
         return out
+
+    def batch_results(self) -> list:
+        """[(pairs, essentials)] of every complex of the batch, in one staged copy."""
+        k = getattr(self, "_batch_k", 0)
+        np_ = np.zeros(max(k, 1), dtype=np.int64)
+        ne_ = np.zeros(max(k, 1), dtype=np.int64)
+        self._check(self._lib.sspp_batch_counts(self._h, np_.ctypes.data, ne_.ctypes.data))
+        outs = [(np.empty((int(np_[i]), 2), dtype=np.int64), np.empty(int(ne_[i]), dtype=np.int64)) for i in range(k)]
+        po = (ctypes.c_void_p * max(k, 1))(*[o[0].ctypes.data for o in outs])
+        eo = (ctypes.c_void_p * max(k, 1))(*[o[1].ctypes.data for o in outs])
+        self._check(self._lib.sspp_batch_copy(self._h, po, eo))
+        return outs
 
     def batch_essentials(self, i: int) -> np.ndarray:
         n = self._lib.sspp_batch_num_essential(self._h, i)

@@ -132,3 +132,22 @@ def test_batch_rejects_face_outside_its_complex():
         e.load_batch([good, good])
         e.reduce(Params())
         assert np.array_equal(e.batch_pairs(1), oracle.reduce(good).pairs)
+
+
+def test_bulk_batch_results_match_per_complex_slices():
+    from specseqplusplus_b200 import workloads
+
+    mats, _ = workloads.batch_of_rips(40, seed=17, n_min=50, n_max=3000)
+    mats.insert(5, gen.BoundaryMatrix.from_columns([0, 0], [[], []]))
+    mats.insert(9, gen.BoundaryMatrix.from_columns([], []))
+    with Engine(0) as e:
+        e.load_batch(mats)
+        e.reduce(Params(autotune=1))
+        bulk = e.batch_results()
+        assert len(bulk) == len(mats)
+        for i, m in enumerate(mats):
+            assert np.array_equal(bulk[i][0], e.batch_pairs(i)), i
+            assert np.array_equal(bulk[i][1], e.batch_essentials(i)), i
+        for i in range(0, len(mats), 9):
+            ref = oracle.reduce(mats[i])
+            assert np.array_equal(bulk[i][0], ref.pairs) and np.array_equal(bulk[i][1], ref.essential)
