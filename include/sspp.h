@@ -88,6 +88,7 @@ typedef struct sspp_stats {
     int64_t light_launches, heavy_launches;
     int64_t arena_ints_used;     /* column arena in use after the reduction (ints)  */
     int64_t tuned_candidate;     /* autotuner candidate of the last run, or -1     */
+    int64_t heavy_additions;     /* additions done by the CTA tier                 */
 } sspp_stats;
 
 /* Replaces: the SpecSeqPlusPlus constructor's allocation (include/specseq.h:486-512). */

@@ -1093,6 +1093,7 @@ int32_t sspp_get_stats(const sspp_ctx* ctx, sspp_stats* o) {
     o->collapse_dropped = c[CNT_DROPPED];
     o->arena_ints_used = ctx->arena_used;
     o->tuned_candidate = ctx->tune_cand;
+    o->heavy_additions = c[CNT_HEAVY_ADDS];
     o->additions = c[CNT_ADDITIONS];
     o->add_ints = c[CNT_ADD_INTS];
     o->published_ints = c[CNT_PUBLISHED];

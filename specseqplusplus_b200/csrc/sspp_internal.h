@@ -80,6 +80,7 @@ enum CounterIdx {
     CNT_ACTIVE,
     CNT_NPAIRS,
     CNT_NESS,
+    CNT_HEAVY_ADDS,  // additions done by the CTA tier
     CNT_NUM
 };
 

@@ -710,6 +710,7 @@ __device__ Outcome reduce_column(const G& g, const ReduceArgs& A, int col, int32
     if (g.leader() && adds) {
         cnt_add(&A.counters[CNT_ADDITIONS], adds);
         cnt_add(&A.counters[CNT_ADD_INTS], add_ints);
+        if (!defer) cnt_add(&A.counters[CNT_HEAVY_ADDS], adds);
     }
     return res;
 }
