@@ -505,6 +505,136 @@ __device__ bool publish(const G& g, const ReduceArgs& A, int col, Work& w) {
 
 enum Outcome { OUT_OWNER, OUT_ZERO, OUT_PARKED, OUT_DEFERRED, OUT_FAIL };
 
+// Short addends in the CTA tier.  Along the long chains the CTA tier runs, the
+// working column holds hundreds of entries while the addends (owners'
+// versions) hold a handful: the two tops cancel, and the addend's other
+// entries change the column only from the lowest position where one of them
+// lands.  Warp 0 alone finds those positions by binary search in shared
+// memory, rewrites just that suffix (its xor with the addend, through the
+// spare buffer) and goes on to the next lowest row, whose pivot entry it has
+// requested before the rewrite; the rest of the CTA waits at one barrier.
+// The warp stops, leaving the step to the general path, when the row must be
+// claimed (no owner, or a larger one), the column is empty or below the band,
+// or the addend is longer than kShortAddend entries or would not fit.
+// Returns the additions done, or -1 after a failed self-check.
+constexpr int kShortAddend = 28;  // header + entries in one 32-lane load
+
+struct FastState {
+    unsigned long long e;
+    long long add_ints;
+    int len, L, adds, bad;
+};
+
+template <int T>
+__device__ int fast_adds(const BlockG<T>& g, const ReduceArgs& A, int col, Work& w, int& L, uint64_t& e,
+                         int32_t* tmp, int32_t* sb, long long& adds, long long& add_ints, int iters_left) {
+    __shared__ FastState fs;
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        int32_t* a = w.buf;
+        int n = w.len, Lc = L, done = 0, bad = 0;
+        uint64_t ec = e;
+        long long ai = 0;
+        while (done < iters_left && n > 0 && Lc >= A.minrow && pv_col(ec) < col) {
+            if (pv_slot(ec) + kHdr > uint64_t(A.arena_cap)) break;  // the general path reports it
+            const int v = __ldcg(A.arena + pv_slot(ec) + lane);      // header and the first 28 entries
+            const int plen = __shfl_sync(kFull, v, 0), hcol = __shfl_sync(kFull, v, 1);
+            if (plen < 1 || plen > kShortAddend || hcol != pv_col(ec) || n + plen > A.cap) break;
+            if (__shfl_sync(kFull, v, (kHdr + plen - 1) & 31) != Lc) break;  // the general path reports it
+            const int m = plen - 1;  // addend entries below the common top
+            const int bj = __shfl_sync(kFull, v, (lane + kHdr) & 31);
+            if (lane < m) sb[lane] = bj;
+            if (lane == 0) sb[m] = Lc;
+            __syncwarp();
+            // the next lowest row is known now: request its pivot entry
+            uint64_t pref = kNoOwner;
+            int L2 = -1;
+            if (lane == 31) {
+                L2 = next_low(a, n, false, sb, plen, false);
+                if (L2 >= 0 && L2 < A.ncols && L2 >= A.minrow) pref = ld_acquire_u64(A.pivot + L2);
+            }
+            // lane j < m: where addend entry j lands below the top, and whether it cancels
+            int pos = n - 1;
+            bool fnd = false;
+            if (lane < m) {
+                pos = lower_bound_t<false>(a, n - 1, bj);
+                fnd = pos < n - 1 && lds(a + pos) == bj;
+            }
+            const int pmin = warp_min(pos);
+            const int sl = n - 1 - pmin;  // suffix below the top that the addend touches
+            const unsigned fmask = __ballot_sync(kFull, fnd);
+            const unsigned imask = __ballot_sync(kFull, lane < m && !fnd);
+            // suffix entries: shifted right by the insertions before them, left by the cancellations
+            for (int base = pmin; base < n - 1; base += 32) {
+                const int i = base + lane;
+                const bool in = i < n - 1;
+                const int x = in ? lds(a + i) : 0;
+                int shift = 0;
+                bool drop = false;
+                for (int j = 0; j < m; j++) {
+                    const int pj = __shfl_sync(kFull, pos, j);
+                    if ((fmask >> j) & 1) {
+                        if (pj < i) shift--;
+                        else if (pj == i) drop = true;
+                    } else if (pj <= i) {
+                        shift++;
+                    }
+                }
+                if (in && !drop) {
+                    const int t = i - pmin + shift;
+                    if (t >= 0 && t < A.cap) tmp[t] = x;
+                    else atomicOr(A.err, ERRB_BAD_INPUT);  // addend not strictly increasing
+                }
+            }
+            if (lane < m && !fnd) {  // inserted addend entries
+                const unsigned lt = lanemask_lt();
+                const int t = pos - pmin + __popc(imask & lt) - __popc(fmask & lt);
+                if (t >= 0 && t < A.cap) tmp[t] = bj;
+                else atomicOr(A.err, ERRB_BAD_INPUT);
+            }
+            __syncwarp();
+            const int outl = sl + __popc(imask) - __popc(fmask);
+            for (int i = lane; i < outl; i += 32) a[pmin + i] = tmp[i];
+            const int nn = pmin + outl;
+            if (lane < int(pad4(nn) - nn)) a[nn + lane] = INT_MAX;
+            __syncwarp();
+            ai += n + plen + nn;
+            n = nn;
+            done++;
+            Lc = n ? lds(a + n - 1) : -1;
+            L2 = __shfl_sync(kFull, L2, 31);
+            ec = __shfl_sync(kFull, (unsigned long long)pref, 31);
+            if (Lc >= A.ncols || Lc != L2) {  // self-check: row index, next-low prediction
+                bad = 1;
+                break;
+            }
+            if (Lc < A.minrow) ec = kNoOwner;
+        }
+        if (lane == 0) {
+            fs.len = n;
+            fs.L = Lc;
+            fs.e = ec;
+            fs.adds = done;
+            fs.add_ints = ai;
+            fs.bad = bad;
+            if (bad) atomicOr(A.err, ERRB_CHECK);
+        }
+    }
+    __syncthreads();
+    const int done = fs.adds;
+    if (fs.bad) return -1;
+    if (done > 0) {
+        w.len = fs.len;
+        w.dirty = true;
+        L = fs.L;
+        e = fs.e;
+        adds += done;
+        add_ints += fs.add_ints;
+    }
+    __syncthreads();  // fs is rewritten by the next call
+    return done;
+}
+
 // Reduces column `col` until it owns its lowest row, becomes zero, or its
 // lowest row drops below the band.  With `defer`, a column whose entries (or
 // whose next addend or sum) exceed the shared capacity is published and
@@ -600,6 +730,17 @@ __device__ Outcome reduce_column(const G& g, const ReduceArgs& A, int col, int32
             }
             e = old;  // someone else changed the owner; look again
             continue;
+        }
+        if constexpr (G::kSize > 32) {  // CTA tier: short addends by one warp
+            if (!w.global) {
+                const int done = fast_adds(g, A, col, w, L, e, w.buf == sw0 ? sw1 : sw0, sp, adds, add_ints,
+                                           kMaxMergesPerColumn - iter);
+                if (done < 0) break;
+                if (done > 0) {
+                    iter += done;
+                    continue;
+                }
+            }
         }
         // add the owner's version (p < col, same lowest row): stage header + entries
         if (pv_slot(e) + kHdr > uint64_t(A.arena_cap)) {  // self-check: entry inside the arena
