@@ -66,6 +66,7 @@ struct ReduceArgs {
     int64_t pool_cap;
     int* err;
     long long* counters;
+    int32_t light_chain;  // warp tier: additions per column before handing it to the CTA tier (0 = no limit)
 };
 
 constexpr int kMaxMergesPerColumn = 1 << 24;
@@ -731,6 +732,18 @@ __device__ Outcome reduce_column(const G& g, const ReduceArgs& A, int col, int32
             e = old;  // someone else changed the owner; look again
             continue;
         }
+        if (defer && A.light_chain > 0 && iter >= A.light_chain && (iter & 7) == 0) {
+            // once the step's window is handed out, a long chain in the warp tier
+            // only holds up the step's tail: the CTA tier continues it on a side
+            // stream while the next step runs
+            int drained = 0;
+            if (g.leader()) drained = __ldcg(A.ctr) >= A.end - A.beg;
+            if (g.bcast(drained)) {
+                if (w.dirty && !publish(g, A, col, w)) break;
+                res = OUT_DEFERRED;
+                break;
+            }
+        }
         if constexpr (G::kSize > 32) {  // CTA tier: short addends by one warp
             if (!w.global) {
                 const int done = fast_adds(g, A, col, w, L, e, w.buf == sw0 ? sw1 : sw0, sp, adds, add_ints,
@@ -950,6 +963,13 @@ __global__ void __launch_bounds__(T, 1) k_reduce_heavy(ReduceArgs A) {
 int light_smem_bytes(int cap) { return 4 * (3 * cap + kHdr) * 4; }
 int heavy_smem_bytes(int cap) { return (3 * cap + kHdr) * 4; }
 
+// Warp-tier additions per column after which, once its step's window is
+// fully handed out, the column moves to the CTA tier: a step's light launch
+// lasts as long as its longest chain, while CTA-tier launches overlap later
+// steps on side streams.  Handing chains over while the window still has work
+// would only move parallel work onto the (fewer) CTAs.
+constexpr int32_t kLightChain = 16;
+
 static ReduceArgs make_args(const Device& D, const int32_t* active, int32_t beg, int32_t end, int32_t minrow, int cap,
                             int chunk, int* ctr) {
     ReduceArgs A;
@@ -974,6 +994,7 @@ static ReduceArgs make_args(const Device& D, const int32_t* active, int32_t beg,
     A.pool_cap = D.pool_cap;
     A.err = D.err;
     A.counters = D.counters;
+    A.light_chain = kLightChain;
     return A;
 }
 
