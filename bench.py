@@ -246,9 +246,11 @@ def leg_batched(steps):
 
     mats, _ = workloads.batch_of_rips(512)
     N = sum(m.ncols for m in mats)
-    p_auto, p_ref = Params(autotune=1), Params()
+    # autotune 2: launch parameters and the choice between the boundary matrix
+    # and dualization mode 2 (the pairs are the same either way)
+    p_auto, p_ref = Params(autotune=2), Params()
     with Engine(0) as e:
-        for _ in range(6):  # the autotuner tries its candidates on this size class first
+        for _ in range(10):  # the autotuner tries its candidates on this size class first
             e.load_batch(mats)
             e.reduce(p_auto)
             e.batch_results()
@@ -273,7 +275,7 @@ def leg_batched(steps):
             return time.perf_counter() - t, out
 
     t_ref, plain = one_at_a_time(p_ref, 1)
-    t_auto, _ = one_at_a_time(p_auto, 5)
+    t_auto, _ = one_at_a_time(p_auto, 9)
     same = all(np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]) for a, b in zip(res, plain))
     orc = oracle_module()
     sample = list(range(0, len(mats), 32))
@@ -287,7 +289,7 @@ def leg_batched(steps):
             "speedup_vs_plain": t_ref / tb, "speedup_vs_plain_autotuned": t_auto / tb,
             "batched_params": {"level1_capacity": chosen.level1_capacity, "level2_capacity": chosen.level2_capacity,
                                "ss_block_size": chosen.ss_block_size, "growth": chosen.growth,
-                               "heavy_threads": chosen.heavy_threads},
+                               "heavy_threads": chosen.heavy_threads, "dualize": chosen.dualize, "autotune": 2},
             "plain_params": "reference defaults (level capacities 1000/8000, ss_block_size 102400, growth 1.05, "
                             "queue_size 65536)",
             "pairs_equal_plain_all": bool(same), "pairs_exact_oracle_sample": bool(exact),
@@ -296,7 +298,8 @@ def leg_batched(steps):
 
 def leg_served(count=48, rates=(100.0, None)):
     """Poisson request stream (Rips 300-20,000 pts 2-D/3-D degree 8-40; lower-star 16^3-96^3 sigma 1-3):
-    the serving loop (2 workers, autotuned, continuous batching) vs a serial one-at-a-time loop."""
+    the serving loop (2 workers, autotune 2, continuous batching) vs a serial one-at-a-time loop with the
+    reference's default parameters."""
     from specseqplusplus_b200 import Engine, Params, Server, workloads
 
     stream = workloads.serving_stream(count, 1.0, seed=5)
@@ -332,8 +335,8 @@ def leg_served(count=48, rates=(100.0, None)):
         cp, lp, pres = plain(Params())
         if plain_results is None:
             plain_results = pres
-        with Server(Params(autotune=1), workers=2) as srv:
-            for _ in range(2):
+        with Server(Params(autotune=2), workers=2) as srv:
+            for _ in range(3):
                 ids = [srv.submit(m, copy=False) for m in warm]
                 for i in ids:
                     srv.wait(i)
