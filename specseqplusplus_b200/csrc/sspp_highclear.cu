@@ -13,7 +13,8 @@
 // youngest facet of t, so the column of s is a sum of earlier columns and s is
 // positive: its column is cleared.  Facets are found through an open-
 // addressing hash of the top-dimension vertex tuples (the reference sorts
-// combinatorial-number keys and binary-searches them).  One warp handles one
+// combinatorial-number keys and binary-searches them).  A group of lanes
+// (max_iteration rounded up to a power of two, at most a warp) handles one
 // simplex, one lane one candidate.
 //
 // The reference walks the neighbour lists with a comparison in the wrong
@@ -181,26 +182,34 @@ __device__ __forceinline__ bool adj_has(const int32_t* adj, const int64_t* adj_o
     return lo < adj_off[u + 1] && adj[lo] == w;
 }
 
-// one warp per top-dimension simplex, one lane per candidate
+// G lanes per top-dimension simplex (G = max_iteration rounded up to a power
+// of two, at most 32), one lane per candidate; a warp takes 32 / G simplices
+// at a time, so a small max_iteration does not leave most lanes idle.
+template <int G>
 __global__ void k_highclear(int32_t cb, int32_t ce, int D, int max_iter, const int32_t* tup, const int32_t* adj,
                             const int64_t* adj_off, const int32_t* table, uint32_t mask, const uint8_t* dropped,
                             uint8_t* cleared, long long* counters) {
-    const int lane = threadIdx.x & 31;
+    constexpr int kPer = 32 / G;  // simplices per warp
+    constexpr unsigned kGroupMask = G == 32 ? 0xffffffffu : ((1u << G) - 1);
+    const int lane = threadIdx.x & 31, grp = lane / G, gl = lane % G;
     const int64_t warp = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5;
     const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
     const int k = D + 1;
     long long found_total = 0;
-    for (int64_t i = cb + warp; i < ce; i += nwarps) {
+    for (int64_t wb = cb + warp * kPer; wb < ce; wb += nwarps * kPer) {
+        const int64_t i = wb + grp;
         const int32_t* s = tup + (i - cb) * k;
-        if (s[0] < 0 || (dropped && dropped[i])) continue;
-        const int32_t v0 = s[0];
-        const int64_t nb = adj_off[v0 + 1] - adj_off[v0];
+        const bool valid = i < ce && s[0] >= 0 && !(dropped && dropped[i]);
+        const int32_t v0 = valid ? s[0] : 0;
+        const int64_t nb = valid ? adj_off[v0 + 1] - adj_off[v0] : 0;
         const int64_t limit = nb < max_iter ? nb : max_iter;
         bool found = false;
-        for (int64_t base = 0; base < limit && !found; base += 32) {
+        for (int64_t base = 0;; base += G) {
+            const bool act = valid && !found && base < limit;
+            if (!__any_sync(kFull, act)) break;
             bool ok = false;
-            int64_t q = base + lane;
-            if (q < limit) {
+            const int64_t q = base + gl;
+            if (act && q < limit) {
                 const int32_t w = adj[adj_off[v0] + q];
                 ok = true;
                 for (int j = 1; j < k && ok; j++) ok = adj_has(adj, adj_off, s[j], w);
@@ -225,13 +234,15 @@ __global__ void k_highclear(int32_t cb, int32_t ce, int D, int max_iter, const i
                     }
                 }
             }
-            found = __any_sync(kFull, ok);
+            const unsigned bl = __ballot_sync(kFull, ok);
+            found = found || ((bl >> (grp * G)) & kGroupMask) != 0;
         }
-        if (found && lane == 0) {
+        if (valid && found && gl == 0) {
             cleared[i] = 1;
             found_total++;
         }
     }
+    found_total = warp_sum(found_total);
     if (lane == 0 && found_total) cnt_add(&counters[CNT_HIGHCLEAR], found_total);
 }
 
@@ -270,8 +281,16 @@ int highclear(Device& D, const DimInfo& info, int max_iteration, const uint8_t* 
     cudaMemsetAsync(S.table, 0xff, sizeof(int32_t) * (size_t(S.mask) + 1), s);
     const int32_t cb = info.col_begin[top], ce = info.col_end[top];
     k_hash_insert<<<gridn(ce - cb, 256), 256, 0, s>>>(cb, ce, top + 1, S.tup[top], dropped, S.table, S.mask);
-    k_highclear<<<gridn(int64_t(ce - cb) * 32, 256, 148 * 64), 256, 0, s>>>(
-        cb, ce, top, max_iteration, S.tup[top], S.adj, S.adj_off, S.table, S.mask, dropped, D.cleared, D.counters);
+    const int g = max_iteration <= 4 ? 4 : max_iteration <= 8 ? 8 : max_iteration <= 16 ? 16 : 32;
+    const unsigned grid = gridn(int64_t(ce - cb) * g, 256, 148 * 64);
+#define SSPP_HC(G_)                                                                                               \
+    k_highclear<G_><<<grid, 256, 0, s>>>(cb, ce, top, max_iteration, S.tup[top], S.adj, S.adj_off, S.table, S.mask, \
+                                         dropped, D.cleared, D.counters)
+    if (g == 4) SSPP_HC(4);
+    else if (g == 8) SSPP_HC(8);
+    else if (g == 16) SSPP_HC(16);
+    else SSPP_HC(32);
+#undef SSPP_HC
     launches += 2;
     return launches;
 }

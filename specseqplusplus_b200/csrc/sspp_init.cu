@@ -188,42 +188,44 @@ __global__ void __launch_bounds__(kPartThreads) k_dim_count(const int32_t* dims,
     if (threadIdx.x < kNumDims) dimcnt[int64_t(blockIdx.x) * kNumDims + threadIdx.x] = cnt[threadIdx.x];
 }
 
-// one block: per-dimension exclusive scan over blocks, then global dim starts
+// one block per dimension: exclusive scan of that dimension's per-block
+// counts; the dimension's total goes to col_end[d] until k_dim_starts
 __global__ void __launch_bounds__(1024) k_dim_offsets(int32_t* dimcnt, int64_t nb, DimInfo* info) {
-    __shared__ int64_t tot[kNumDims];
     __shared__ int64_t wt[32];
     __shared__ int64_t carry;
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    for (int d = 0; d < kNumDims; d++) {
-        if (tid == 0) carry = 0;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, d = blockIdx.x;
+    if (tid == 0) carry = 0;
+    __syncthreads();
+    for (int64_t base = 0; base < nb; base += 1024) {
+        int64_t i = base + tid;
+        int64_t v = i < nb ? dimcnt[i * kNumDims + d] : 0;
+        int64_t inc = warp_inclusive_scan(v);
+        if (lane == 31) wt[wid] = inc;
         __syncthreads();
-        for (int64_t base = 0; base < nb; base += 1024) {
-            int64_t i = base + tid;
-            int64_t v = i < nb ? dimcnt[i * kNumDims + d] : 0;
-            int64_t inc = warp_inclusive_scan(v);
-            if (lane == 31) wt[wid] = inc;
-            __syncthreads();
-            if (wid == 0) {
-                int64_t t = wt[lane];
-                int64_t ti = warp_inclusive_scan(t);
-                wt[lane] = ti - t;
-            }
-            __syncthreads();
-            int64_t ex = carry + wt[wid] + inc - v;
-            if (i < nb) dimcnt[i * kNumDims + d] = int32_t(ex);
-            __syncthreads();
-            if (tid == 1023) carry = ex + v;
-            __syncthreads();
+        if (wid == 0) {
+            int64_t t = wt[lane];
+            int64_t ti = warp_inclusive_scan(t);
+            wt[lane] = ti - t;
         }
-        if (tid == 0) tot[d] = carry;
+        __syncthreads();
+        int64_t ex = carry + wt[wid] + inc - v;
+        if (i < nb) dimcnt[i * kNumDims + d] = int32_t(ex);
+        __syncthreads();
+        if (tid == 1023) carry = ex + v;
         __syncthreads();
     }
-    if (tid == 0) {
-        int64_t s = 0;
+    if (tid == 0) info->col_end[d] = int32_t(carry);
+}
+
+// per-dimension totals -> dimension ranges of the reordered columns
+__global__ void k_dim_starts(DimInfo* info) {
+    if (threadIdx.x == 0) {
+        int32_t s = 0;
         for (int d = 0; d < kNumDims; d++) {
-            info->col_begin[d] = int32_t(s);
-            s += tot[d];
-            info->col_end[d] = int32_t(s);
+            const int32_t c = info->col_end[d];
+            info->col_begin[d] = s;
+            s += c;
+            info->col_end[d] = s;
         }
     }
 }
@@ -294,7 +296,8 @@ int reorder(Device& D, cudaStream_t s) {
     const int64_t n = D.n;
     const int64_t nb = (n + kPartThreads - 1) / kPartThreads;
     k_dim_count<<<unsigned(nb), kPartThreads, 0, s>>>(D.in_dims, n, D.dimcnt, D.err);
-    k_dim_offsets<<<1, 1024, 0, s>>>(D.dimcnt, nb, D.diminfo);
+    k_dim_offsets<<<kNumDims, 1024, 0, s>>>(D.dimcnt, nb, D.diminfo);
+    k_dim_starts<<<1, 32, 0, s>>>(D.diminfo);
     k_dim_assign<<<unsigned(nb), kPartThreads, 0, s>>>(D.in_dims, n, D.dimcnt, D.diminfo, D.newidx, D.perm, D.dim);
     // padded column offsets in reordered order
     const int64_t* colptr = D.in_colptr;
@@ -304,7 +307,7 @@ int reorder(Device& D, cudaStream_t s) {
          [=] __device__(int64_t i, int64_t pre, int64_t) { off[i] = pre; }, n, D.blk, s);
     k_scatter_cols<<<grid_for(n, 256) > 65536 ? 65536 : grid_for(n, 256), 256, 0, s>>>(
         n, D.in_colptr, D.in_rows, D.in_dims, D.perm, D.newidx, off, D.arena, D.desc, D.leftmost, D.err);
-    return 7;
+    return 8;
 }
 
 // ------------------------------------------------------------- init passes
