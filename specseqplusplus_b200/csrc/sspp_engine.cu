@@ -142,7 +142,7 @@ cudaError_t grow(T*& p, int64_t& cap, int64_t want, cudaStream_t s) {
 void free_device(Device& D) {
     void* ptrs[] = {D.dim, D.perm, D.newidx, D.scratch64, D.arena, D.arena_top,
                     D.desc, D.low, D.pivot, D.state, D.cleared, D.negative, D.leftmost, D.active, D.blk, D.dimcnt,
-                    D.diminfo, D.err, D.counters, D.step_ctr, D.heavy, D.pool_tail, D.death_of, D.pairs, D.ess, D.misc};
+                    D.diminfo, D.err, D.counters, D.step_ctr, D.heavy, D.pool_tail, D.death_of, D.pairs, D.ess, D.misc, D.app};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     D = Device();
@@ -175,6 +175,7 @@ int ensure_columns(sspp_ctx* ctx, int64_t n, int64_t nnz) {
         CK(g(D.death_of, 1));
         CK(g(D.pairs, 2));
         CK(g(D.ess, 1));
+        CK(g(D.app, 1));
         D.cap_n = c;
         int64_t nb = (c + 4095) / 4096 + 2;
         CK(grow(D.blk, D.cap_blk, nb, ctx->stream));
@@ -389,6 +390,7 @@ int run_init(sspp_ctx* ctx) {
     }
     ctx->launches += init_compress(D, dropped_of(ctx), s);
     if (ctx->params.dualize == 1) ctx->launches += dualize(D, 1, s);
+    ctx->launches += build_apparent(D, s);
     ctx->launches += active_list(D, s);
     span_end(ctx, PH_INIT, ev0);
     CK(cudaGetLastError());
@@ -540,6 +542,7 @@ int run_compute(sspp_ctx* ctx) {
         if (rc) return rc;
         nsteps += ctx->ss_steps;
         ctx->launches += dualize(D, 2, s);
+        ctx->launches += build_apparent(D, s);
         ctx->launches += active_list(D, s);
         CK(cudaMemcpyAsync(ctx->h_info, D.diminfo, sizeof(DimInfo), cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));

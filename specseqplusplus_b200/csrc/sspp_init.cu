@@ -439,6 +439,32 @@ int init_compress(Device& D, const uint8_t* dropped, cudaStream_t s) {
     return 1;
 }
 
+// Inline copies of the short apparent columns, by row (see Device::app).
+__global__ void k_build_apparent(int64_t n, const uint64_t* pivot, const int32_t* arena, int4* app) {
+    for (int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; r < n; r += int64_t(gridDim.x) * blockDim.x) {
+        int4 v = make_int4(-1, INT_MAX, INT_MAX, INT_MAX);
+        const uint64_t e = pivot[r];
+        if (e != kNoOwner) {
+            const int32_t* h = arena + pv_slot(e);
+            const int len = h[0];
+            if (len >= 1 && len <= 4 && h[kHdr + len - 1] == int32_t(r)) {
+                v.x = len - 1;
+                if (len > 1) v.y = h[kHdr];
+                if (len > 2) v.z = h[kHdr + 1];
+                if (len > 3) v.w = h[kHdr + 2];
+            }
+        }
+        app[r] = v;
+    }
+}
+
+int build_apparent(Device& D, cudaStream_t s) {
+    const int64_t n = D.n;
+    if (n == 0) return 0;
+    k_build_apparent<<<grid_for(n, 256) > 65536 ? 65536 : grid_for(n, 256), 256, 0, s>>>(n, D.pivot, D.arena, D.app);
+    return 1;
+}
+
 // Active list in reordered order (dimension segments are contiguous) and the
 // per-dimension bounds.
 __global__ void k_act_segments(const int64_t* actpos, int64_t n, DimInfo* info) {

@@ -128,6 +128,11 @@ struct Device {
     int64_t* pairs = nullptr;      // [2n]
     int64_t* ess = nullptr;        // [n]
     int64_t* misc = nullptr;       // [8] small device scalars of the dualization
+    // [n] per row owned by an apparent pair whose column holds at most 4
+    // entries: {entries below the top, then up to 3 of them}; x = -1 otherwise.
+    // Apparent owners never change, so the reduction reads an addend here with
+    // one load that does not wait for the pivot entry.
+    int4* app = nullptr;
 };
 
 }  // namespace sspp

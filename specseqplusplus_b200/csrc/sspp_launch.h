@@ -32,6 +32,8 @@ int batch_localize(int64_t npairs, int64_t ness, int32_t k, const int64_t* d_cst
 int init_passes(Device& D, cudaStream_t s);
 int init_compress(Device& D, const uint8_t* dropped, cudaStream_t s);
 int active_list(Device& D, cudaStream_t s);
+// D.app from the pivot table as it stands (apparent pairs only)
+int build_apparent(Device& D, cudaStream_t s);
 // anti-transpose of the compressed matrix behind the primal columns in the
 // arena; remaps pivots, states, dims and the per-dimension column ranges.
 // mode 1: the whole matrix; mode 2: after the edge columns were reduced (the

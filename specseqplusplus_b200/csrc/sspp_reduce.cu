@@ -67,6 +67,7 @@ struct ReduceArgs {
     int* err;
     long long* counters;
     int32_t light_chain;  // warp tier: additions per column before handing it to the CTA tier (0 = no limit)
+    const int4* app;      // inline short apparent columns by row (Device::app)
 };
 
 constexpr int kMaxMergesPerColumn = 1 << 24;
@@ -536,23 +537,46 @@ __device__ int fast_adds(const BlockG<T>& g, const ReduceArgs& A, int col, Work&
         int n = w.len, Lc = L, done = 0, bad = 0;
         uint64_t ec = e;
         long long ai = 0;
-        while (done < iters_left && n > 0 && Lc >= A.minrow && pv_col(ec) < col) {
-            if (pv_slot(ec) + kHdr > uint64_t(A.arena_cap)) break;  // the general path reports it
-            const int v = __ldcg(A.arena + pv_slot(ec) + lane);      // header and the first 28 entries
-            const int plen = __shfl_sync(kFull, v, 0), hcol = __shfl_sync(kFull, v, 1);
-            if (plen < 1 || plen > kShortAddend || hcol != pv_col(ec) || n + plen > A.cap) break;
-            if (__shfl_sync(kFull, v, (kHdr + plen - 1) & 31) != Lc) break;  // the general path reports it
+        // inline copy of the current row's apparent column, if it has one
+        int4 ap = make_int4(-1, 0, 0, 0);
+        if (lane == 31 && Lc >= 0 && Lc < A.ncols) ap = __ldg(A.app + Lc);
+        ap.x = __shfl_sync(kFull, ap.x, 31);
+        ap.y = __shfl_sync(kFull, ap.y, 31);
+        ap.z = __shfl_sync(kFull, ap.z, 31);
+        ap.w = __shfl_sync(kFull, ap.w, 31);
+        bool have_e = true;  // ec is the pivot entry of Lc
+        while (done < iters_left && n > 0 && Lc >= A.minrow) {
+            int plen, bj;
+            if (ap.x >= 0) {  // apparent owner: permanent, its entries are at hand
+                plen = ap.x + 1;
+                bj = lane == 0 ? ap.y : (lane == 1 ? ap.z : ap.w);
+                if (n + plen > A.cap) break;
+            } else {
+                if (!have_e) {
+                    uint64_t t = 0;
+                    if (lane == 0) t = ld_acquire_u64(A.pivot + Lc);
+                    ec = __shfl_sync(kFull, (unsigned long long)t, 0);
+                    have_e = true;
+                }
+                if (pv_col(ec) >= col) break;                         // claim: the general path
+                if (pv_slot(ec) + kHdr > uint64_t(A.arena_cap)) break;  // the general path reports it
+                const int v = __ldcg(A.arena + pv_slot(ec) + lane);      // header and the first 28 entries
+                plen = __shfl_sync(kFull, v, 0);
+                const int hcol = __shfl_sync(kFull, v, 1);
+                if (plen < 1 || plen > kShortAddend || hcol != pv_col(ec) || n + plen > A.cap) break;
+                if (__shfl_sync(kFull, v, (kHdr + plen - 1) & 31) != Lc) break;  // the general path reports it
+                bj = __shfl_sync(kFull, v, (lane + kHdr) & 31);
+            }
             const int m = plen - 1;  // addend entries below the common top
-            const int bj = __shfl_sync(kFull, v, (lane + kHdr) & 31);
             if (lane < m) sb[lane] = bj;
             if (lane == 0) sb[m] = Lc;
             __syncwarp();
-            // the next lowest row is known now: request its pivot entry
-            uint64_t pref = kNoOwner;
+            // the next lowest row is known now: request its inline apparent column
+            int4 apn = make_int4(-1, 0, 0, 0);
             int L2 = -1;
             if (lane == 31) {
                 L2 = next_low(a, n, false, sb, plen, false);
-                if (L2 >= 0 && L2 < A.ncols && L2 >= A.minrow) pref = ld_acquire_u64(A.pivot + L2);
+                if (L2 >= 0 && L2 < A.ncols && L2 >= A.minrow) apn = __ldg(A.app + L2);
             }
             // lane j < m: where addend entry j lands below the top, and whether it cancels
             int pos = n - 1;
@@ -604,12 +628,16 @@ __device__ int fast_adds(const BlockG<T>& g, const ReduceArgs& A, int col, Work&
             done++;
             Lc = n ? lds(a + n - 1) : -1;
             L2 = __shfl_sync(kFull, L2, 31);
-            ec = __shfl_sync(kFull, (unsigned long long)pref, 31);
             if (Lc >= A.ncols || Lc != L2) {  // self-check: row index, next-low prediction
                 bad = 1;
                 break;
             }
-            if (Lc < A.minrow) ec = kNoOwner;
+            ap.x = __shfl_sync(kFull, apn.x, 31);
+            ap.y = __shfl_sync(kFull, apn.y, 31);
+            ap.z = __shfl_sync(kFull, apn.z, 31);
+            ap.w = __shfl_sync(kFull, apn.w, 31);
+            have_e = false;
+            ec = kNoOwner;  // unknown; the general path's claim retries with the real entry
         }
         if (lane == 0) {
             fs.len = n;
@@ -995,6 +1023,7 @@ static ReduceArgs make_args(const Device& D, const int32_t* active, int32_t beg,
     A.err = D.err;
     A.counters = D.counters;
     A.light_chain = kLightChain;
+    A.app = D.app;
     return A;
 }
 
