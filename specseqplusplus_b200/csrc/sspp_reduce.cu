@@ -712,6 +712,9 @@ __device__ Outcome reduce_column(const G& g, const ReduceArgs& A, int col, int32
         if (g.leader()) atomicOr(A.err, ERRB_CHECK);
         return OUT_FAIL;
     }
+    // inline apparent column of row r (every thread loads it: one transaction per warp)
+    auto app_of = [&](int r) { return (r >= 0 && r >= A.minrow) ? __ldg(A.app + r) : make_int4(-1, 0, 0, 0); };
+    int4 apc = app_of(L);
     if (L >= A.minrow) {
         if (g.leader()) e = ld_acquire_u64(A.pivot + L);
         e = g.bcast64(e);
@@ -779,6 +782,7 @@ __device__ Outcome reduce_column(const G& g, const ReduceArgs& A, int col, int32
                 if (done < 0) break;
                 if (done > 0) {
                     iter += done;
+                    apc = app_of(L);
                     continue;
                 }
             }
@@ -789,17 +793,33 @@ __device__ Outcome reduce_column(const G& g, const ReduceArgs& A, int col, int32
             break;
         }
         const int32_t* src = A.arena + pv_slot(e);
-        copy4(g, sp, src, 0, first4);
-        g.sync();
-        const int plen = sp[0];
-        if (plen < 1 || plen > int(kMaxColLen) || sp[1] != p ||
-            int64_t(pv_slot(e)) + slot_ints(plen) > A.arena_cap) {  // self-check: header of the owner's version
-            if (g.leader()) atomicOr(A.err, ERRB_CHECK);
-            break;
+        int plen;
+        if (apc.x >= 0) {  // apparent owner: its entries are inline, no arena read
+            plen = apc.x + 1;
+            if (g.leader()) {
+                sp[kHdr] = apc.y;
+                sp[kHdr + 1] = apc.z;
+                sp[kHdr + 2] = apc.w;
+                sp[kHdr + 3] = INT_MAX;
+                sp[kHdr + apc.x] = L;
+            }
+            g.sync();
+        } else {
+            copy4(g, sp, src, 0, first4);
+            g.sync();
+            plen = sp[0];
+            if (plen < 1 || plen > int(kMaxColLen) || sp[1] != p ||
+                int64_t(pv_slot(e)) + slot_ints(plen) > A.arena_cap) {  // self-check: header of the owner's version
+                if (g.leader()) atomicOr(A.err, ERRB_CHECK);
+                break;
+            }
         }
         const int32_t* pb;
         bool pg;
-        if (plen <= A.cap) {
+        if (apc.x >= 0) {
+            pb = sp + kHdr;
+            pg = false;
+        } else if (plen <= A.cap) {
             const int n4 = (kHdr + int(pad4(plen))) >> 2;
             if (n4 > first4) {
                 copy4(g, sp, src, first4, n4);
@@ -826,6 +846,7 @@ __device__ Outcome reduce_column(const G& g, const ReduceArgs& A, int col, int32
         // element, so its acquire load completes while the others merge
         uint64_t pref = kNoOwner;
         if (g.rank() == G::kSize - 1 && L2 >= A.minrow && L2 >= 0) pref = ld_acquire_u64(A.pivot + L2);
+        const int4 apn = app_of(L2);
         int out_len;
         const int bound = w.len + plen - 2;
         if (bound <= A.cap) {
@@ -888,6 +909,7 @@ __device__ Outcome reduce_column(const G& g, const ReduceArgs& A, int col, int32
         w.dirty = true;
         L = L2;
         e = g.bcast64_last(pref);
+        apc = apn;
     }
     if (g.leader() && adds) {
         cnt_add(&A.counters[CNT_ADDITIONS], adds);
