@@ -167,6 +167,32 @@ int64_t sspp_batch_essentials(sspp_ctx* ctx, int32_t i, int64_t* out, int64_t ca
 int32_t sspp_batch_counts(sspp_ctx* ctx, int64_t* npairs, int64_t* ness);
 int32_t sspp_batch_copy(sspp_ctx* ctx, int64_t* const* pairs_out, int64_t* const* ess_out);
 
+/* Host-side PHAT files, no device needed.  sspp_phat_read parses a boundary
+ * matrix as processFiles does (src/main.cu:90-167; 0-based indices, every
+ * column sorted and de-duplicated) on several host threads for large files;
+ * the handle hands out its size and a copy of the arrays.  sspp_phat_write
+ * writes a matrix in either format (the layout sspp_phat_read accepts). */
+typedef struct sspp_phat sspp_phat;
+sspp_phat* sspp_phat_read(const char* path, int32_t fmt, char* err_msg, int32_t err_cap);
+int64_t sspp_phat_ncols(const sspp_phat* h);
+int64_t sspp_phat_nnz(const sspp_phat* h);
+int32_t sspp_phat_copy(const sspp_phat* h, int32_t* dims, int64_t* col_ptr, int32_t* rows);
+void sspp_phat_free(sspp_phat* h);
+int32_t sspp_phat_write(const char* path, int32_t fmt, int64_t ncols, const int32_t* dims, const int64_t* col_ptr,
+                        const int32_t* rows, char* err_msg, int32_t err_cap);
+
+/* Replaces: the HIGHOUT build's out_maxdimclear (include/specseq.h:1108-1129,
+ * Makefile:33-34).  Writes the loaded matrix, in input order and indices, with
+ * the columns that guided clearing (model bit 1) clears and that the edge
+ * collapse (model bit 2) drops written as dimension-only lines; every other
+ * column as loaded.  Reducing the written file gives the same pairs.  The
+ * guided clearing here walks the neighbour lists in the intended direction,
+ * while the reference's walk only ever accepts the smallest common neighbour
+ * (include/kernel.h:217), so more columns can be cleared than in the
+ * reference's files.  Leaves the context loaded but not initialised (call
+ * sspp_init again). */
+int32_t sspp_export_preprocessed(sspp_ctx* ctx, const sspp_params* p, const char* path, int32_t fmt);
+
 /* Replaces: writeVectorToFile (src/main.cu:191-229). */
 int32_t sspp_write_pairs(sspp_ctx* ctx, const char* path, int32_t fmt);
 

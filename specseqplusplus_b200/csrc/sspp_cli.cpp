@@ -3,11 +3,16 @@
 //   specseq++ <input_file> <output_file> <ascii|binary> <ascii|binary> <dualize>
 //             <model> <max_iteration> <ss_block_size> <block_size_growth_rate>
 //             <queue_size> <level1_capacity> <level2_capacity> [--auto] [--device N]
+//             [--export-preprocessed]
 //
 // Same 12 positional arguments, same pair file bytes (count line, then
 // "birth death" lines, or int64 count + int64 pairs), same exit codes (0, or 1
 // with the help text on bad arguments).  `--auto` lets the engine pick the
 // block sizes, queue size and capacities for the input's size class.
+// `--export-preprocessed` does what the reference's HIGHOUT build does
+// (include/specseq.h:545-549, 1108-1129): it writes the input with the guided
+// clearing / edge collapse of <model> applied to <output_file> (in the output
+// format) instead of the pairs, and stops.
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -19,7 +24,7 @@ static void print_help() {
     std::printf(
         "Usage: specseq++ <input_file> <output_file> <input_format> <output_format> <dualize> <model> "
         "<max_iteration> <ss_block_size> <block_size_growth_rate> <queue_size> <level1_capacity> "
-        "<level2_capacity> [--auto] [--device N]\n"
+        "<level2_capacity> [--auto] [--device N] [--export-preprocessed]\n"
         "input_format: ascii or binary\n"
         "output_format: ascii or binary\n"
         "dualize: \n"
@@ -38,6 +43,8 @@ static void print_help() {
         "level1_capacity: on-chip capacity (ints) of a column worker\n"
         "level2_capacity: on-chip capacity (ints) of a block worker\n"
         "--auto: choose ss_block_size, growth, queue_size and capacities automatically\n"
+        "--export-preprocessed: write the input with the model's clearing / collapse applied (cleared columns "
+        "as dimension-only lines) to output_file instead of the pairs\n"
         "Example: ./specseq++ input.txt output.txt ascii ascii 0 1 10 1024000 1.05 65536 1000 2000\n");
 }
 
@@ -93,8 +100,10 @@ int main(int argc, char** argv) {
     }
     sspp_config cfg;
     std::memset(&cfg, 0, sizeof(cfg));
+    bool export_only = false;
     for (int i = 13; i < argc; i++) {
         if (!std::strcmp(argv[i], "--auto")) p.autotune = 1;
+        else if (!std::strcmp(argv[i], "--export-preprocessed")) export_only = true;
         else if (!std::strcmp(argv[i], "--device") && i + 1 < argc) cfg.device = std::atoi(argv[++i]);
     }
     sspp_ctx* ctx = sspp_create(&cfg);
@@ -104,6 +113,12 @@ int main(int argc, char** argv) {
     }
     int rc = sspp_load_phat(ctx, in, in_fmt);
     if (rc == SSPP_OK) std::printf("-----------------------------------------------Reading  completed-----------------------------------------------\n");
+    if (rc == SSPP_OK && export_only) {
+        rc = sspp_export_preprocessed(ctx, &p, out, out_fmt);
+        if (rc != SSPP_OK) std::fprintf(stderr, "Error: %s\n", sspp_last_error(ctx));
+        sspp_destroy(ctx);
+        return rc == SSPP_OK ? 0 : 1;
+    }
     if (rc == SSPP_OK) rc = sspp_init(ctx, &p, nullptr);
     if (rc == SSPP_OK) rc = sspp_compute(ctx, nullptr);
     if (rc != SSPP_OK) {

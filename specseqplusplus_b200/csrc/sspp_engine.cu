@@ -1067,6 +1067,77 @@ int64_t sspp_essentials(sspp_ctx* ctx, int64_t* out, int64_t cap) {
     return n;
 }
 
+int32_t sspp_export_preprocessed(sspp_ctx* ctx, const sspp_params* p, const char* path, int32_t fmt) {
+    if (!ctx) return SSPP_ERR_BAD_INPUT;
+    cudaSetDevice(ctx->cfg.device);
+    if (!ctx->loaded) return set_err(ctx, SSPP_ERR_STATE, "no matrix loaded");
+    if (!path || (fmt != SSPP_ASCII && fmt != SSPP_BINARY)) return set_err(ctx, SSPP_ERR_BAD_INPUT, "bad path or format");
+    int rc = check_params(ctx, p);
+    if (rc) return rc;
+    ctx->params = *p;
+    ctx->inited = ctx->computed = false;
+    Device& D = ctx->D;
+    cudaStream_t s = ctx->stream;
+    const int64_t n = D.n, nnz = D.nnz;
+    std::vector<int32_t> dims(size_t(std::max<int64_t>(n, 1)));
+    std::vector<int64_t> cp(size_t(n) + 1, 0);
+    std::vector<int32_t> rows(size_t(std::max<int64_t>(nnz, 1)));
+    if (n > 0) {
+        CK(cudaMemcpyAsync(dims.data(), D.in_dims, 4 * size_t(n), cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(cp.data(), D.in_colptr, 8 * (size_t(n) + 1), cudaMemcpyDeviceToHost, s));
+    }
+    if (nnz > 0) CK(cudaMemcpyAsync(rows.data(), D.in_rows, 4 * size_t(nnz), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemsetAsync(D.err, 0, sizeof(int), s));
+    CK(cudaMemsetAsync(D.counters, 0, sizeof(long long) * CNT_NUM, s));
+    CK(cudaStreamSynchronize(s));
+    std::vector<uint8_t> drop(size_t(std::max<int64_t>(n, 1)), 0);
+    if (n > 0 && (p->model & 3)) {
+        rc = ensure_arena(ctx, arena_need(ctx));
+        if (rc) return rc;
+        validate(D, s);
+        CK(cudaMemcpyAsync(ctx->h_err, D.err, sizeof(int), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        if (*ctx->h_err) return set_err(ctx, SSPP_ERR_BAD_INPUT, "dimension out of range 0..7 or malformed col_ptr");
+        reorder(D, s);
+        CK(cudaMemcpyAsync(D.arena_top, D.blk + reorder_total_slot(D), sizeof(unsigned long long),
+                           cudaMemcpyDeviceToDevice, s));
+        CK(cudaMemcpyAsync(ctx->h_err, D.err, sizeof(int), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        if (*ctx->h_err) return set_err(ctx, SSPP_ERR_BAD_INPUT, "malformed boundary matrix");
+        if (p->model & 2) {
+            rc = run_collapse(ctx);
+            if (rc) return rc;
+        }
+        CK(cudaMemsetAsync(D.cleared, 0, size_t(n), s));
+        if ((p->model & 1) && p->max_iteration > 0) {
+            rc = run_highclear(ctx);
+            if (rc) return rc;
+        }
+        std::vector<int32_t> perm(static_cast<size_t>(n));
+        std::vector<uint8_t> cl(static_cast<size_t>(n)), dr(static_cast<size_t>(n), 0);
+        CK(cudaMemcpyAsync(perm.data(), D.perm, 4 * size_t(n), cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(cl.data(), D.cleared, size_t(n), cudaMemcpyDeviceToHost, s));
+        if (p->model & 2) CK(cudaMemcpyAsync(dr.data(), ctx->dropped, size_t(n), cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(ctx->h_counters, D.counters, sizeof(long long) * CNT_NUM, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        CK(cudaGetLastError());
+        std::memcpy(ctx->hcounters, ctx->h_counters, sizeof(ctx->hcounters));
+        for (int64_t i = 0; i < n; i++)
+            if (cl[size_t(i)] || dr[size_t(i)]) drop[size_t(perm[size_t(i)])] = 1;
+    }
+    // cleared and dropped columns become dimension-only lines (include/specseq.h:1115-1123)
+    std::vector<int64_t> ocp(size_t(n) + 1, 0);
+    std::vector<int32_t> orows;
+    orows.reserve(size_t(std::max<int64_t>(nnz, 1)));
+    for (int64_t j = 0; j < n; j++) {
+        if (!drop[size_t(j)]) orows.insert(orows.end(), rows.begin() + cp[size_t(j)], rows.begin() + cp[size_t(j) + 1]);
+        ocp[size_t(j) + 1] = int64_t(orows.size());
+    }
+    std::string e;
+    if (!write_phat(path, fmt, n, dims.data(), ocp.data(), orows.data(), e)) return set_err(ctx, SSPP_ERR_IO, e);
+    return SSPP_OK;
+}
+
 int32_t sspp_write_pairs(sspp_ctx* ctx, const char* path, int32_t fmt) {
     if (!ctx) return SSPP_ERR_BAD_INPUT;
     if (!ctx->computed) return set_err(ctx, SSPP_ERR_STATE, "no pairs computed");

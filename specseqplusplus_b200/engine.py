@@ -136,6 +136,13 @@ def load_library():
         "sspp_server_release": (i32, [vp, i64]),
         "sspp_server_get_stats": (i32, [vp, ctypes.POINTER(_ServerStats)]),
         "sspp_server_reset_stats": (i32, [vp]),
+        "sspp_export_preprocessed": (i32, [vp, ctypes.POINTER(_Params), ctypes.c_char_p, i32]),
+        "sspp_phat_read": (vp, [ctypes.c_char_p, i32, ctypes.c_char_p, i32]),
+        "sspp_phat_ncols": (i64, [vp]),
+        "sspp_phat_nnz": (i64, [vp]),
+        "sspp_phat_copy": (i32, [vp, vp, vp, vp]),
+        "sspp_phat_free": (None, [vp]),
+        "sspp_phat_write": (i32, [ctypes.c_char_p, i32, i64, vp, vp, vp, ctypes.c_char_p, i32]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -154,7 +161,9 @@ EXPORTED = ("sspp_create", "sspp_destroy", "sspp_last_error", "sspp_default_para
             "sspp_server_create", "sspp_server_destroy", "sspp_server_last_error", "sspp_server_submit",
             "sspp_server_wait", "sspp_server_state", "sspp_server_result", "sspp_server_num_pairs",
             "sspp_server_pairs", "sspp_server_num_essential", "sspp_server_essentials", "sspp_server_latency_ms",
-            "sspp_server_release", "sspp_server_get_stats", "sspp_server_reset_stats")
+            "sspp_server_release", "sspp_server_get_stats", "sspp_server_reset_stats", "sspp_phat_read",
+            "sspp_phat_ncols", "sspp_phat_nnz", "sspp_phat_copy", "sspp_phat_free", "sspp_phat_write",
+            "sspp_export_preprocessed")
 
 
 class Engine:
@@ -241,6 +250,12 @@ class Engine:
         if self._lib.sspp_batch_essentials(self._h, i, out.ctypes.data, n) != n:
             self._check(ERR_CUDA)
         return out
+
+    def export_preprocessed(self, path: str, params: Params | None = None, fmt: int = ASCII) -> None:
+        """Writes the loaded matrix with guided clearing / edge collapse applied (cleared and dropped
+        columns as dimension-only lines), as the reference's HIGHOUT build does."""
+        p = (params or Params())._c()
+        self._check(self._lib.sspp_export_preprocessed(self._h, ctypes.byref(p), str(path).encode(), fmt))
 
     def load_phat(self, path: str, fmt: int = ASCII) -> None:
         self._check(self._lib.sspp_load_phat(self._h, path.encode(), fmt))
@@ -458,3 +473,37 @@ class Server:
 
     def reset_stats(self) -> None:
         self._lib.sspp_server_reset_stats(self._h)
+
+
+def read_phat(path: str, fmt: int = ASCII):
+    """PHAT boundary matrix from a file, read on the host by the library's reader
+    (processFiles semantics: 0-based faces, columns sorted and de-duplicated)."""
+    from .gen import BoundaryMatrix
+
+    lib = load_library()
+    err = ctypes.create_string_buffer(256)
+    h = lib.sspp_phat_read(str(path).encode(), fmt, err, 256)
+    if not h:
+        raise SsppError(ERR_IO, err.value.decode(errors="replace"))
+    try:
+        n, nnz = lib.sspp_phat_ncols(h), lib.sspp_phat_nnz(h)
+        dims = np.empty(n, dtype=np.int32)
+        col_ptr = np.empty(n + 1, dtype=np.int64)
+        rows = np.empty(max(nnz, 1), dtype=np.int32)
+        lib.sspp_phat_copy(h, dims.ctypes.data, col_ptr.ctypes.data, rows.ctypes.data)
+    finally:
+        lib.sspp_phat_free(h)
+    return BoundaryMatrix(dims, col_ptr, rows[:nnz])
+
+
+def write_phat(path: str, m, fmt: int = ASCII) -> None:
+    """Writes a boundary matrix in PHAT ascii or binary format."""
+    lib = load_library()
+    dims = np.ascontiguousarray(m.dims, dtype=np.int32)
+    col_ptr = np.ascontiguousarray(m.col_ptr, dtype=np.int64)
+    rows = np.ascontiguousarray(m.rows if m.nnz else np.zeros(1, np.int32), dtype=np.int32)
+    err = ctypes.create_string_buffer(256)
+    rc = lib.sspp_phat_write(str(path).encode(), fmt, dims.shape[0], dims.ctypes.data, col_ptr.ctypes.data,
+                             rows.ctypes.data, err, 256)
+    if rc != OK:
+        raise SsppError(rc, err.value.decode(errors="replace"))

@@ -65,12 +65,13 @@ class BoundaryMatrix:
     @staticmethod
     def from_columns(dims, columns) -> "BoundaryMatrix":
         dims = np.asarray(dims, dtype=np.int32)
-        col_ptr = np.zeros(len(columns) + 1, dtype=np.int64)
-        for j, c in enumerate(columns):
+        cols = [sorted(set(int(x) for x in c)) for c in columns]
+        col_ptr = np.zeros(len(cols) + 1, dtype=np.int64)
+        for j, c in enumerate(cols):
             col_ptr[j + 1] = col_ptr[j] + len(c)
         rows = np.zeros(int(col_ptr[-1]), dtype=np.int32)
-        for j, c in enumerate(columns):
-            rows[col_ptr[j]:col_ptr[j + 1]] = sorted(set(int(x) for x in c))
+        for j, c in enumerate(cols):
+            rows[col_ptr[j]:col_ptr[j + 1]] = c
         return BoundaryMatrix(dims, col_ptr, rows)
 
 

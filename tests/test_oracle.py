@@ -141,3 +141,28 @@ def test_collapse_keeps_homology_of_flag_complex():
     b0 = np.bincount(m.dims[r0.essential], minlength=3)
     b2 = np.bincount(m.dims[r2.essential], minlength=3)
     assert b0[0] == b2[0]
+
+
+REF_ALPHA = "/root/reference/data/Alpha"
+
+
+@pytest.mark.skipif(not os.path.isdir(REF_ALPHA), reason="reference tree absent")
+def test_reference_highclear_artefacts_keep_the_pairs():
+    # The reference's HIGHOUT build wrote each Alpha input again with its guided
+    # clearing applied (cleared columns as dimension-only lines,
+    # include/specseq.h:1108-1129); both files must give the same pairs.
+    names = sorted(f for f in os.listdir(REF_ALPHA) if f.endswith(".txt") and not f.endswith("_maxclear.txt"))
+    checked = 0
+    for f in names:
+        cleared = os.path.join(REF_ALPHA, f[:-4] + "_maxclear.txt")
+        if not os.path.exists(cleared):
+            continue
+        mats = []
+        for path in (os.path.join(REF_ALPHA, f), cleared):
+            d, c, r = oracle.read_phat(path, False)
+            mats.append(gen.BoundaryMatrix(d, c, r))
+        assert mats[0].ncols == mats[1].ncols
+        a, b = oracle.reduce(mats[0]), oracle.reduce(mats[1])
+        assert np.array_equal(a.pairs, b.pairs), f
+        checked += 1
+    assert checked >= 3
