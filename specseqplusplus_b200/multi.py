@@ -1,0 +1,64 @@
+"""Batches over several GPUs: one process per GPU, complexes sharded by size.
+
+A single reduction does not shard (one pivot table, arbitrary column
+dependencies), but independent complexes do.  Every rank takes a share of the
+complexes - assigned largest first to the rank with the fewest columns so far,
+the same assignment on every rank, with no communication - reduces its share
+as one batch on its own GPU, and the results are gathered on the host of one
+rank.  Nothing crosses between GPUs on the data path; the only collective is
+the final gather of host arrays over torch.distributed (gloo or nccl object
+collectives).
+"""
+from __future__ import annotations
+
+import heapq
+
+import numpy as np
+
+
+def shard(ncols, world: int) -> list:
+    """Complex indices of each rank (largest complexes first, to the least loaded rank)."""
+    order = sorted(range(len(ncols)), key=lambda i: (-int(ncols[i]), i))
+    heap = [(0, r) for r in range(world)]
+    parts = [[] for _ in range(world)]
+    for i in order:
+        load, r = heapq.heappop(heap)
+        parts[r].append(i)
+        heapq.heappush(heap, (load + int(ncols[i]), r))
+    return [sorted(p) for p in parts]
+
+
+def _reduce_local(mats, params, device):
+    from .engine import Engine
+
+    if not mats:
+        return []
+    with Engine(device) as e:
+        e.load_batch(mats)
+        e.reduce(params)
+        return e.batch_results()
+
+
+def reduce_batch(mats, params, group=None, device: int = 0, dst: int = 0, reduce_fn=None):
+    """Reduces `mats` (the same list on every rank) across the ranks of `group`.
+
+    Returns [(pairs, essentials)] in input order on rank `dst`, None elsewhere.
+    reduce_fn(local_mats, params, device) replaces the single-GPU batch reduction
+    (the default runs the engine on `device`).
+    """
+    import torch.distributed as dist
+
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    parts = shard([m.ncols for m in mats], world)
+    mine = parts[rank]
+    res = (reduce_fn or _reduce_local)([mats[i] for i in mine], params, device)
+    payload = [(i, np.asarray(p), np.asarray(e)) for i, (p, e) in zip(mine, res)]
+    gathered = [None] * world if rank == dst else None
+    dist.gather_object(payload, gathered, dst=dst, group=group)
+    if rank != dst:
+        return None
+    out = [None] * len(mats)
+    for part in gathered:
+        for i, p, e in part:
+            out[i] = (p, e)
+    return out

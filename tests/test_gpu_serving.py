@@ -151,3 +151,27 @@ def test_bulk_batch_results_match_per_complex_slices():
         for i in range(0, len(mats), 9):
             ref = oracle.reduce(mats[i])
             assert np.array_equal(bulk[i][0], ref.pairs) and np.array_equal(bulk[i][1], ref.essential)
+
+
+def test_multi_gpu_dispatcher_single_rank_runs_the_engine():
+    import datetime
+    import socket
+
+    import torch.distributed as dist
+
+    from specseqplusplus_b200 import workloads
+    from specseqplusplus_b200.multi import reduce_batch
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        mats, _ = workloads.batch_of_rips(7, seed=41, n_min=80, n_max=600)
+        res = reduce_batch(mats, Params(autotune=1))
+        for (p, e), m in zip(res, mats):
+            ref = oracle.reduce(m)
+            assert np.array_equal(p, ref.pairs) and np.array_equal(e, ref.essential)
+    finally:
+        dist.destroy_process_group()
