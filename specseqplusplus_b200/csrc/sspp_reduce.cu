@@ -745,10 +745,15 @@ __device__ Outcome reduce_column(const G& g, const ReduceArgs& A, int col, int32
             if (w.dirty && !publish(g, A, col, w)) break;
             uint64_t old = 0;
             if (g.leader()) {
+                // the column's final state goes out before the claim: a group
+                // that later displaces it writes its own state after this one
+                const uint8_t was = A.state[col];
                 A.low[col] = L;
+                A.state[col] = ST_OWNER;
                 __threadfence();
                 old = atomicCAS(reinterpret_cast<unsigned long long*>(A.pivot + L), (unsigned long long)e,
                                 (unsigned long long)pv_pack(col, uint64_t(w.slot)));
+                if (old != e) A.state[col] = was;  // not claimed: still in progress here
             }
             old = g.bcast64(old);
             if (old == e) {
@@ -924,7 +929,7 @@ template <class G>
 __device__ __forceinline__ bool settle(const G& g, const ReduceArgs& A, int col, Outcome o) {
     if (g.leader()) {
         switch (o) {
-            case OUT_OWNER: A.state[col] = ST_OWNER; break;
+            case OUT_OWNER: break;  // written before the claim
             case OUT_ZERO: A.state[col] = ST_ZERO; break;
             case OUT_DEFERRED: {
                 A.state[col] = ST_HEAVY;
