@@ -140,12 +140,28 @@ static size_t next_chunk(const std::vector<Piece>& pieces, size_t& pi, size_t& p
     return fill;
 }
 
+// host memory the copy engines can read directly (cudaMallocHost / registered)
+static bool pinned(const void* p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();  // unregistered pageable memory on some drivers
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+static bool all_pinned(const std::vector<Piece>& pieces, bool src) {
+    for (const Piece& p : pieces)
+        if (p.bytes && !pinned(src ? p.src : p.dst)) return false;
+    return true;
+}
+
 cudaError_t Xfer::h2d(const std::vector<Piece>& pieces, cudaStream_t s) {
     size_t total = 0;
     for (const Piece& p : pieces) total += p.bytes;
     if (total == 0) return cudaSuccess;
     cudaError_t e;
-    if (total <= kDirectBytes) {
+    if (total <= kDirectBytes || all_pinned(pieces, true)) {  // pinned sources: straight to the copy engine
         for (const Piece& p : pieces)
             if (p.bytes && (e = cudaMemcpyAsync(p.dst, p.src, p.bytes, cudaMemcpyHostToDevice, s)) != cudaSuccess)
                 return e;
@@ -187,7 +203,7 @@ cudaError_t Xfer::d2h(const std::vector<Piece>& pieces, cudaStream_t s) {
     for (const Piece& p : pieces) total += p.bytes;
     if (total == 0) return cudaSuccess;
     cudaError_t e;
-    if (total <= kDirectBytes) {
+    if (total <= kDirectBytes || all_pinned(pieces, false)) {
         for (const Piece& p : pieces)
             if (p.bytes && (e = cudaMemcpyAsync(p.dst, p.src, p.bytes, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
                 return e;
