@@ -68,6 +68,8 @@ struct sspp_ctx {
     sspp_params params{};          // effective parameters (after autotuning)
     sspp_params user_params{};     // as passed to sspp_init
     int tune_cand = -1;            // autotuner candidate of this run, -1 without autotune
+    int tune_shape = 0;            // shape class of the loaded complex (autotuner key)
+    bool tune_locked = false;      // a capacity repeat keeps the candidate
     int64_t arena_used = 0;        // arena ints in use after the last reduction
     bool loaded = false, inited = false, computed = false;
     DimInfo hinfo{};
@@ -211,7 +213,7 @@ int ensure_arena(sspp_ctx* ctx, int64_t ints) {
 int64_t arena_need(const sspp_ctx* ctx) {
     const int64_t base = ctx->D.nnz + (kHdr + 3) * ctx->D.n + 4;
     int64_t want = base + std::max<int64_t>(2 * base, int64_t(16) << 20);
-    if (ctx->params.dualize) want += base;  // the dual columns are built behind the primal ones
+    if (ctx->params.dualize || ctx->user_params.autotune == 2) want += base;  // dual columns behind the primal ones
     if (ctx->cfg.arena_bytes > 0) want = std::max<int64_t>(want, ctx->cfg.arena_bytes / 4);
     return std::max(want, ctx->arena_request);
 }
@@ -351,6 +353,33 @@ int run_highclear(sspp_ctx* ctx) {
     return SSPP_OK;
 }
 
+// Autotuned parameters for the loaded complex, chosen once its dimension
+// ranges are known (one host read): the shape key is the top dimension and
+// the quarter of the columns that lie in it.
+int autotune_choose(sspp_ctx* ctx) {
+    Device& D = ctx->D;
+    CK(cudaMemcpyAsync(ctx->h_info, D.diminfo, sizeof(DimInfo), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    const DimInfo& I = *ctx->h_info;
+    int top = 0;
+    for (int d = kMaxDim; d >= 0; d--)
+        if (I.col_end[d] > I.col_begin[d]) { top = d; break; }
+    const double frac = D.n ? double(I.col_end[top] - I.col_begin[top]) / double(D.n) : 0.0;
+    ctx->tune_shape = top * 4 + std::min(3, int(frac * 4.0));
+    const sspp_params& u = ctx->user_params;
+    Knobs k;
+    ctx->tune_cand = tune_choose(D.n, ctx->tune_shape, u.model, u.dualize, u.autotune == 2, &k);
+    sspp_params& q = ctx->params;
+    q.ss_block_size = k.ss_block_size;
+    q.growth = k.growth;
+    q.queue_size = k.queue_size;
+    q.level1_capacity = k.level1;
+    q.level2_capacity = k.level2;
+    q.heavy_threads = k.heavy_threads;
+    q.dualize = k.dualize;
+    return SSPP_OK;
+}
+
 int run_init(sspp_ctx* ctx) {
     Device& D = ctx->D;
     cudaStream_t s = ctx->stream;
@@ -379,6 +408,10 @@ int run_init(sspp_ctx* ctx) {
     ctx->launches += reorder(D, s);
     CK(cudaMemcpyAsync(D.arena_top, D.blk + reorder_total_slot(D), sizeof(unsigned long long),
                        cudaMemcpyDeviceToDevice, s));
+    if (ctx->user_params.autotune && !ctx->tune_locked) {
+        int rc2 = autotune_choose(ctx);
+        if (rc2) return rc2;
+    }
     if (ctx->params.model & 2) {  // collapse before everything else: dropped columns are emptied
         int rc2 = run_collapse(ctx);
         if (rc2) return rc2;
@@ -990,18 +1023,7 @@ int32_t sspp_init(sspp_ctx* ctx, const sspp_params* p, void* stream) {
     ctx->params = *p;
     ctx->user_params = *p;
     ctx->tune_cand = -1;
-    if (p->autotune) {
-        Knobs k;
-        ctx->tune_cand = tune_choose(ctx->D.n, p->model, p->dualize, p->autotune == 2, &k);
-        sspp_params& q = ctx->params;
-        q.ss_block_size = k.ss_block_size;
-        q.growth = k.growth;
-        q.queue_size = k.queue_size;
-        q.level1_capacity = k.level1;
-        q.level2_capacity = k.level2;
-        q.heavy_threads = k.heavy_threads;
-        q.dualize = k.dualize;
-    }
+    ctx->tune_locked = false;
     ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
     return run_init(ctx);
 }
@@ -1016,10 +1038,11 @@ int32_t sspp_compute(sspp_ctx* ctx, void* stream) {
         if (rc == SSPP_OK && ctx->tune_cand >= 0) {
             const sspp_params& u = ctx->user_params;
             const double base = double(ctx->D.nnz + (kHdr + 3) * ctx->D.n + 4);
-            tune_record(ctx->D.n, u.model, u.dualize, u.autotune == 2, ctx->tune_cand, ctx->init_ms + ctx->compute_ms,
-                        double(ctx->arena_used) / base);
+            tune_record(ctx->D.n, ctx->tune_shape, u.model, u.dualize, u.autotune == 2, ctx->tune_cand,
+                        ctx->init_ms + ctx->compute_ms, double(ctx->arena_used) / base);
         }
         if (rc != SSPP_ERR_CAPACITY || !ctx->err.empty()) return rc;
+        ctx->tune_locked = true;  // the repeat keeps this run's choice
         // arena or heavy pool exhausted: grow both and redo the whole reduction from the input
         ctx->arena_request = std::max<int64_t>(ctx->D.arena_cap * 2, arena_need(ctx));
         ctx->pool_request = std::max<int64_t>(ctx->D.pool_cap * 2, 1 << 16);

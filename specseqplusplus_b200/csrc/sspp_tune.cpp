@@ -33,7 +33,8 @@ struct Entry {
     double fill = 0;
 };
 
-using Key = std::tuple<int, int, int, int>;
+// size class (log2 columns), shape, model, dualize as asked, allow_dual
+using Key = std::tuple<int, int, int, int, int>;
 
 std::mutex g_mu;
 std::map<Key, Entry>& table() {
@@ -41,10 +42,15 @@ std::map<Key, Entry>& table() {
     return t;
 }
 
-Key key_of(int64_t ncols, int32_t model, int32_t dualize, int32_t allow_dual) {
+Key key_of(int64_t ncols, int32_t shape, int32_t model, int32_t dualize, int32_t allow_dual) {
     int lg = 0;
     while ((int64_t(1) << (lg + 1)) <= std::max<int64_t>(ncols, 1)) lg++;
-    return Key{lg, model, allow_dual ? 2 : dualize, allow_dual};
+    return Key{lg, shape, model, allow_dual ? 2 : dualize, allow_dual};
+}
+
+bool similar(const Key& a, const Key& b) {  // every field but the size
+    return std::get<1>(a) == std::get<1>(b) && std::get<2>(a) == std::get<2>(b) && std::get<3>(a) == std::get<3>(b) &&
+           std::get<4>(a) == std::get<4>(b);
 }
 
 int num_candidates(int32_t allow_dual) { return allow_dual ? 2 * kNumBase : kNumBase; }
@@ -60,34 +66,61 @@ Entry& entry_of(const Key& k, int32_t allow_dual) {
     return e;
 }
 
+// running mean per candidate over the measured classes similar to k (their
+// own means weighted by runs); infinity where none measured it
+std::vector<double> prior_of(const Key& k, int n) {
+    std::vector<double> sum(size_t(n), 0.0), w(size_t(n), 0.0), out(size_t(n), HUGE_VAL);
+    for (const auto& kv : table()) {
+        if (kv.first == k || !similar(kv.first, k)) continue;
+        for (int c = 0; c < n && c < int(kv.second.mean.size()); c++)
+            if (kv.second.runs[size_t(c)] > 0) {
+                sum[size_t(c)] += kv.second.mean[size_t(c)];
+                w[size_t(c)] += 1.0;
+            }
+    }
+    for (int c = 0; c < n; c++)
+        if (w[size_t(c)] > 0) out[size_t(c)] = sum[size_t(c)] / w[size_t(c)];
+    return out;
+}
+
 }  // namespace
 
-int tune_choose(int64_t ncols, int32_t model, int32_t dualize, int32_t allow_dual, Knobs* out) {
+int tune_choose(int64_t ncols, int32_t shape, int32_t model, int32_t dualize, int32_t allow_dual, Knobs* out) {
     std::lock_guard<std::mutex> l(g_mu);
-    Entry& e = entry_of(key_of(ncols, model, dualize, allow_dual), allow_dual);
+    const Key k = key_of(ncols, shape, model, dualize, allow_dual);
+    Entry& e = entry_of(k, allow_dual);
     const int n = int(e.mean.size());
     int pick = -1;
-    for (int c = 0; c < n && pick < 0; c++)
-        if (e.runs[size_t(c)] == 0) pick = c;
+    // untried candidates, best first by what similar classes measured; those
+    // over twice as slow there as the best are left out of the first round
+    const std::vector<double> prior = prior_of(k, n);
+    double best_prior = HUGE_VAL;
+    for (double v : prior) best_prior = std::min(best_prior, v);
+    for (int c = 0; c < n; c++) {
+        if (e.runs[size_t(c)] > 0) continue;
+        if (std::isfinite(prior[size_t(c)]) && prior[size_t(c)] > 2.0 * best_prior) continue;  // measured slow
+        if (pick < 0 || prior[size_t(c)] < prior[size_t(pick)]) pick = c;
+    }
     if (pick < 0 && e.total % kRetryEvery == kRetryEvery - 1) {
         pick = 0;  // least recently measured
         for (int c = 1; c < n; c++)
             if (e.last[size_t(c)] < e.last[size_t(pick)]) pick = c;
     }
     if (pick < 0) {
-        pick = 0;
-        for (int c = 1; c < n; c++)
-            if (e.mean[size_t(c)] < e.mean[size_t(pick)]) pick = c;
+        pick = -1;
+        for (int c = 0; c < n; c++)
+            if (e.runs[size_t(c)] > 0 && (pick < 0 || e.mean[size_t(c)] < e.mean[size_t(pick)])) pick = c;
+        if (pick < 0) pick = 0;
     }
     *out = kCandidates[pick % kNumBase];
     out->dualize = allow_dual ? (pick >= kNumBase ? 2 : 0) : dualize;
     return pick;
 }
 
-void tune_record(int64_t ncols, int32_t model, int32_t dualize, int32_t allow_dual, int cand, double ms,
-                 double arena_fill) {
+void tune_record(int64_t ncols, int32_t shape, int32_t model, int32_t dualize, int32_t allow_dual, int cand,
+                 double ms, double arena_fill) {
     std::lock_guard<std::mutex> l(g_mu);
-    Entry& e = entry_of(key_of(ncols, model, dualize, allow_dual), allow_dual);
+    Entry& e = entry_of(key_of(ncols, shape, model, dualize, allow_dual), allow_dual);
     if (cand < 0 || cand >= int(e.mean.size()) || !(ms >= 0)) return;
     const double v = ms * 1e6 / double(std::max<int64_t>(ncols, 1));
     const size_t c = size_t(cand);
@@ -99,16 +132,17 @@ void tune_record(int64_t ncols, int32_t model, int32_t dualize, int32_t allow_du
 
 double tune_fill(int64_t ncols, int32_t model, int32_t dualize, int32_t allow_dual, double fallback) {
     std::lock_guard<std::mutex> l(g_mu);
-    const Key k = key_of(ncols, model, dualize, allow_dual);
-    auto it = table().find(k);
-    if (it != table().end() && it->second.fill > 0) return it->second.fill;
-    // no run of this size class yet: the largest fill of any size with the same settings
-    double f = 0;
-    for (const auto& kv : table())
-        if (std::get<1>(kv.first) == std::get<1>(k) && std::get<2>(kv.first) == std::get<2>(k) &&
-            std::get<3>(kv.first) == std::get<3>(k))
-            f = std::max(f, kv.second.fill);
-    return f > 0 ? f : fallback;
+    // the largest fill seen for this size with these settings, any shape; else any size
+    double same = 0, any = 0;
+    const Key k = key_of(ncols, 0, model, dualize, allow_dual);
+    for (const auto& kv : table()) {
+        if (std::get<2>(kv.first) != std::get<2>(k) || std::get<3>(kv.first) != std::get<3>(k) ||
+            std::get<4>(kv.first) != std::get<4>(k))
+            continue;
+        any = std::max(any, kv.second.fill);
+        if (std::get<0>(kv.first) == std::get<0>(k)) same = std::max(same, kv.second.fill);
+    }
+    return same > 0 ? same : (any > 0 ? any : fallback);
 }
 
 }  // namespace sspp

@@ -3,14 +3,16 @@
 // The reference takes ss_block_size, block_size_growth_rate, queue_size and
 // the level capacities from its command line (src/main.cu:281-294), set by
 // hand per dataset.  Here a process-wide history, keyed by size class (log2 of
-// the column count), model, dualization and whether the tuner may choose
-// dualization itself, records the measured time of each candidate setting.  A
-// class tries every candidate once, in a fixed order, then runs the fastest
-// (by running mean of ms per column), re-trying the least recently measured
-// one every 32nd run so that the choice follows drift.  Every candidate gives
-// the same pairs; only the time differs.  The history also keeps the largest
-// arena fill seen per class (arena ints used / base ints), which admission
-// control turns into a device-memory estimate.
+// the column count), shape (top dimension and the share of columns in it),
+// model, dualization and whether the tuner may choose dualization itself,
+// records the measured time of each candidate setting.  A new class first
+// tries the candidates in the order of their means over similar classes
+// (same key but size), leaving out those over twice as slow there as the best,
+// then runs the fastest (by running mean of ms per column), re-trying the least
+// recently measured one every 32nd run so that the choice follows drift.  Every
+// candidate gives the same pairs; only the time differs.  The history also
+// keeps the largest arena fill seen per class (arena ints used / base ints),
+// which admission control turns into a device-memory estimate.
 #pragma once
 #include <stdint.h>
 
@@ -29,9 +31,12 @@ struct Knobs {
 // allow_dual: the tuner may also choose dualization mode 2 (autotune = 2);
 // it never picks the full dual (mode 1), whose vertex columns can carry very
 // long addition chains on grid-like complexes
-int tune_choose(int64_t ncols, int32_t model, int32_t dualize, int32_t allow_dual, Knobs* out);
-void tune_record(int64_t ncols, int32_t model, int32_t dualize, int32_t allow_dual, int cand, double ms,
-                 double arena_fill);
+// shape: a coarse description of the complex (top dimension and the share of
+// its columns there), so that, e.g., grids and Rips complexes of one size
+// class are tuned apart
+int tune_choose(int64_t ncols, int32_t shape, int32_t model, int32_t dualize, int32_t allow_dual, Knobs* out);
+void tune_record(int64_t ncols, int32_t shape, int32_t model, int32_t dualize, int32_t allow_dual, int cand,
+                 double ms, double arena_fill);
 // largest arena fill (used / base) recorded for this class (or, before any
 // run of it, for any size with the same settings), or `fallback`
 double tune_fill(int64_t ncols, int32_t model, int32_t dualize, int32_t allow_dual, double fallback);
