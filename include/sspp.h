@@ -89,6 +89,8 @@ typedef struct sspp_stats {
     int64_t arena_ints_used;     /* column arena in use after the reduction (ints)  */
     int64_t tuned_candidate;     /* autotuner candidate of the last run, or -1     */
     int64_t heavy_additions;     /* additions done by the CTA tier                 */
+    double build_ms;             /* last sspp_load_rips / sspp_load_lowerstar (host
+                                    clock, input staging included), else 0          */
 } sspp_stats;
 
 /* Replaces: the SpecSeqPlusPlus constructor's allocation (include/specseq.h:486-512). */
@@ -117,6 +119,35 @@ int32_t sspp_load_csc(sspp_ctx* ctx, int64_t ncols, const int32_t* dims, const i
  * the next load or sspp_destroy.  Validated on the device. */
 int32_t sspp_load_csc_device(sspp_ctx* ctx, int64_t ncols, const int32_t* d_dims, const int64_t* d_col_ptr,
                              const int32_t* d_rows);
+
+/* Builds on the device, and loads as the input matrix, the Vietoris-Rips
+ * complex of npts points (npts x space_dim float32, row-major, space_dim 1..3,
+ * in host memory or in device memory of the context's device): an edge joins
+ * two points whose float32 Euclidean distance (coordinate differences squared
+ * and summed in order, then the square root, each step rounded to nearest) is
+ * <= radius; every clique of up to maxdim + 1 (<= 4) points is a simplex whose
+ * value is its longest edge; vertices have value 0.  Columns are in (value,
+ * dimension, lexicographic vertex tuple) order, faces ascending, as in the
+ * reference's input files, which external tools write
+ * (phat-highclear/addons/rips.cpp; read by src/main.cu:90-167).
+ * Non-finite coordinates are BAD_INPUT. */
+int32_t sspp_load_rips(sspp_ctx* ctx, int64_t npts, int32_t space_dim, const float* points, float radius,
+                       int32_t maxdim);
+
+/* Same, for the lower-star filtration of the Freudenthal (Kuhn) triangulation
+ * of a gx x gy x gz grid: values[gx * gy * gz] (x fastest, then y, then z; host
+ * or device memory) on the vertices, a simplex's value the largest of its
+ * vertices'; vertex v + (dx, dy, dz) for every non-zero 0/1 offset is joined to
+ * v.  -0 is read as +0; NaN is BAD_INPUT.  Every simplex up to maxdim (<= 3). */
+int32_t sspp_load_lowerstar(sspp_ctx* ctx, int64_t gx, int64_t gy, int64_t gz, const float* values,
+                            int32_t maxdim);
+
+/* The matrix the context reduces (after any load; a batch's is the block-
+ * diagonal concatenation) and, after sspp_load_rips / sspp_load_lowerstar,
+ * each column's filtration value.  Any output may be NULL; asking for values
+ * of a matrix that was not built is BAD_INPUT. */
+int32_t sspp_input_size(sspp_ctx* ctx, int64_t* ncols, int64_t* nnz);
+int32_t sspp_input_copy(sspp_ctx* ctx, int32_t* dims, int64_t* col_ptr, int32_t* rows, float* values);
 
 /* Replaces: SpecSeqPlusPlus::GPU_Init (include/specseq.h:513-590): dimension
  * reorder, edge collapse, guided clearing, init passes, dualization, active

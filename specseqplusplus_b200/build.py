@@ -19,7 +19,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "--extended-lambda", "-Xcompiler", "-fPIC,-O2",
                   "-I", os.path.join(ROOT, "include")]
 
-ENGINE_SRC = ["sspp_engine.cu", "sspp_init.cu", "sspp_reduce.cu", "sspp_highclear.cu", "sspp_dual.cu", "sspp_collapse.cu", "sspp_xfer.cu", "sspp_tune.cpp", "sspp_server.cpp", "sspp_phat.cpp", "sspp_noalloc.cu", "sspp_io.cpp"]
+ENGINE_SRC = ["sspp_engine.cu", "sspp_init.cu", "sspp_reduce.cu", "sspp_highclear.cu", "sspp_dual.cu", "sspp_collapse.cu", "sspp_build.cu", "sspp_xfer.cu", "sspp_tune.cpp", "sspp_server.cpp", "sspp_phat.cpp", "sspp_noalloc.cu", "sspp_io.cpp"]
 
 
 def _run(cmd):

@@ -19,6 +19,7 @@
 #include <type_traits>
 #include <vector>
 
+#include "sspp_build.h"
 #include "sspp_collapse.h"
 #include "sspp_highclear.h"
 #include "sspp_internal.h"
@@ -98,6 +99,9 @@ struct sspp_ctx {
     Xfer xfer;                     // staged copies from and to caller memory
     HighclearScratch hc;
     CollapseScratch cs;
+    BuildScratch bs;               // device complex builders (the input matrix when `built`)
+    bool built = false;
+    double build_ms = 0;
     Prof prof;
     double ph_ms[PH_NUM] = {};
     // batch: column range of each complex in the concatenated input, and the
@@ -615,6 +619,8 @@ int run_compute(sspp_ctx* ctx) {
 
 int load_common(sspp_ctx* ctx, int64_t n, int64_t nnz) {
     ctx->loaded = ctx->inited = ctx->computed = false;
+    ctx->built = false;
+    ctx->build_ms = 0;
     ctx->batch_start.clear();
     ctx->host_pairs_valid = false;
     ctx->host_ess_valid = false;
@@ -647,6 +653,43 @@ int ensure_own(sspp_ctx* ctx, int64_t n, int64_t nnz) {
         CK(grow(ctx->own_rows, c3, std::max<int64_t>(nnz, 1), ctx->stream));
         ctx->cap_own_nnz = std::max<int64_t>(nnz, 1);
     }
+    return SSPP_OK;
+}
+
+// A device pointer to `count` floats of the caller: the pointer itself when it
+// is device (or managed) memory of this context's device, else a copy in the
+// builder's input buffer.
+int stage_floats(sspp_ctx* ctx, const float* p, int64_t count, const float** out) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        a.type = cudaMemoryTypeUnregistered;
+    }
+    if (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) {
+        if (a.type == cudaMemoryTypeDevice && a.device != ctx->cfg.device)
+            return set_err(ctx, SSPP_ERR_BAD_INPUT, "input is in another device's memory");
+        *out = p;
+        return SSPP_OK;
+    }
+    void* d = nullptr;
+    const size_t bytes = sizeof(float) * size_t(count);
+    CK(build_stage(ctx->bs, bytes, ctx->stream, &d));
+    CK(ctx->xfer.h2d({{p, d, bytes}}, ctx->stream));
+    *out = static_cast<const float*>(d);
+    return SSPP_OK;
+}
+
+int finish_build(sspp_ctx* ctx, int rc, const Built& b, const std::string& msg,
+                 std::chrono::steady_clock::time_point t0) {
+    if (rc) return set_err(ctx, rc == -1 ? SSPP_ERR_BAD_INPUT : SSPP_ERR_CUDA, msg);
+    rc = load_common(ctx, b.ncols, b.nnz);
+    if (rc) return rc;
+    ctx->D.in_dims = b.dims;
+    ctx->D.in_colptr = b.col_ptr;
+    ctx->D.in_rows = b.rows;
+    ctx->loaded = true;
+    ctx->built = true;
+    ctx->build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return SSPP_OK;
 }
 
@@ -713,6 +756,7 @@ void sspp_destroy(sspp_ctx* ctx) {
     if (ctx->own_rows) cudaFree(ctx->own_rows);
     if (ctx->d_batch) cudaFree(ctx->d_batch);
     collapse_free(ctx->cs);
+    build_free(ctx->bs);
     for (auto* t : ctx->hc.tup)
         if (t) cudaFree(t);
     if (ctx->hc.deg) cudaFree(ctx->hc.deg);
@@ -781,6 +825,71 @@ int32_t sspp_load_csc_device(sspp_ctx* ctx, int64_t ncols, const int32_t* d_dims
     ctx->D.in_colptr = const_cast<int64_t*>(d_col_ptr);
     ctx->D.in_rows = const_cast<int32_t*>(d_rows);
     ctx->loaded = true;
+    return SSPP_OK;
+}
+
+int32_t sspp_load_rips(sspp_ctx* ctx, int64_t npts, int32_t space_dim, const float* points, float radius,
+                       int32_t maxdim) {
+    if (!ctx) return SSPP_ERR_BAD_INPUT;
+    cudaSetDevice(ctx->cfg.device);
+    if (npts < 0 || (npts > 0 && !points) || space_dim < 1 || space_dim > 3)
+        return set_err(ctx, SSPP_ERR_BAD_INPUT, "bad point array or space dimension");
+    const auto t0 = std::chrono::steady_clock::now();
+    ctx->loaded = false;  // the build reuses the buffers of an earlier build
+    const float* dp = nullptr;
+    if (npts > 0) {
+        int rc = stage_floats(ctx, points, npts * space_dim, &dp);
+        if (rc) return rc;
+    }
+    Built b;
+    std::string msg;
+    const int rc = build_rips(ctx->bs, dp, npts, space_dim, radius, maxdim, ctx->stream, &b, &msg);
+    return finish_build(ctx, rc, b, msg, t0);
+}
+
+int32_t sspp_load_lowerstar(sspp_ctx* ctx, int64_t gx, int64_t gy, int64_t gz, const float* values,
+                            int32_t maxdim) {
+    if (!ctx) return SSPP_ERR_BAD_INPUT;
+    cudaSetDevice(ctx->cfg.device);
+    if (gx < 1 || gy < 1 || gz < 1 || !values || gx > INT32_MAX || gy > INT32_MAX || gz > INT32_MAX ||
+        gx * gy > INT32_MAX || gx * gy * gz > INT32_MAX)
+        return set_err(ctx, SSPP_ERR_BAD_INPUT, "bad grid size or null values");
+    const auto t0 = std::chrono::steady_clock::now();
+    ctx->loaded = false;
+    const float* dv = nullptr;
+    int rc = stage_floats(ctx, values, gx * gy * gz, &dv);
+    if (rc) return rc;
+    Built b;
+    std::string msg;
+    rc = build_lowerstar(ctx->bs, dv, gx, gy, gz, maxdim, ctx->stream, &b, &msg);
+    return finish_build(ctx, rc, b, msg, t0);
+}
+
+int32_t sspp_input_size(sspp_ctx* ctx, int64_t* ncols, int64_t* nnz) {
+    if (!ctx) return SSPP_ERR_BAD_INPUT;
+    if (!ctx->loaded) return set_err(ctx, SSPP_ERR_STATE, "nothing loaded");
+    if (ncols) *ncols = ctx->D.n;
+    if (nnz) *nnz = ctx->D.nnz;
+    return SSPP_OK;
+}
+
+int32_t sspp_input_copy(sspp_ctx* ctx, int32_t* dims, int64_t* col_ptr, int32_t* rows, float* values) {
+    if (!ctx) return SSPP_ERR_BAD_INPUT;
+    cudaSetDevice(ctx->cfg.device);
+    if (!ctx->loaded) return set_err(ctx, SSPP_ERR_STATE, "nothing loaded");
+    if (values && !ctx->built)
+        return set_err(ctx, SSPP_ERR_BAD_INPUT, "filtration values exist for built complexes only");
+    const Device& D = ctx->D;
+    cudaStream_t s = ctx->stream;
+    if (dims && D.n > 0) CK(cudaMemcpyAsync(dims, D.in_dims, sizeof(int32_t) * size_t(D.n), cudaMemcpyDeviceToHost, s));
+    if (col_ptr)
+        CK(cudaMemcpyAsync(col_ptr, D.in_colptr, sizeof(int64_t) * size_t(D.n + 1), cudaMemcpyDeviceToHost, s));
+    if (rows && D.nnz > 0)
+        CK(cudaMemcpyAsync(rows, D.in_rows, sizeof(int32_t) * size_t(D.nnz), cudaMemcpyDeviceToHost, s));
+    if (values && D.n > 0)
+        CK(cudaMemcpyAsync(values, ctx->bs.p[BuildScratch::VALUES], sizeof(float) * size_t(D.n),
+                           cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
     return SSPP_OK;
 }
 
@@ -1208,6 +1317,7 @@ int32_t sspp_get_stats(const sspp_ctx* ctx, sspp_stats* o) {
     o->pairs_gpu_ms = ctx->ph_ms[PH_PAIRS];
     o->light_launches = ctx->light_launches;
     o->heavy_launches = ctx->heavy_launches;
+    o->build_ms = ctx->build_ms;
     return SSPP_OK;
 }
 

@@ -1,19 +1,20 @@
 // Synthetic filtered complexes written as PHAT boundary matrices.
 //
 // These builders produce the inputs the engine is measured and tested on:
-//   * Vietoris-Rips complexes of seeded uniform point clouds in [0,1]^D
-//     (D = 2 or 3), Euclidean float32 distances, truncated at a radius,
-//     simplices up to a maximum dimension;
+//   * Vietoris-Rips complexes of point clouds (seeded uniform in [0,1]^D, or
+//     the caller's, D = 1..3), Euclidean float32 distances, truncated at a
+//     radius, simplices up to a maximum dimension;
 //   * lower-star filtrations of the Freudenthal (Kuhn) triangulation of a
-//     G^3 grid whose vertex values are seeded Gaussian white noise smoothed
-//     by a Gaussian of width sigma voxels (float32).
+//     grid whose vertex values are seeded Gaussian white noise smoothed by a
+//     Gaussian of width sigma voxels (float32), or the caller's field.
 // Columns are ordered by (filtration value, dimension, lexicographic vertex
 // tuple), which is the order the reference's inputs use (PHAT files written in
 // filtration order, src/main.cu:90-167 reads them column by column).  Face
 // indices are int32 and each column lists its facets in ascending order.
 //
 // The builders are host code on the input side of the reduction; they are not
-// part of the measured path.  Everything is deterministic given the seed:
+// part of the measured path.  The engine's device builders (sspp_load_rips,
+// sspp_load_lowerstar) produce the same matrices bit for bit.  Everything is deterministic given the seed:
 // the random stream is SplitMix64, floating point is plain IEEE float/double
 // without contraction (built with -ffp-contract=off).
 #include <algorithm>
@@ -172,46 +173,63 @@ struct Nbr {
     float d;
 };
 
-void gen_rips(int64_t npts, int D, uint64_t seed, float radius, int maxdim, Matrix& out) {
+std::vector<float> gen_points(int64_t npts, int D, uint64_t seed) {
     SplitMix64 rng(seed);
-    std::vector<float> P(size_t(npts) * D);
+    std::vector<float> P(static_cast<size_t>(npts) * D);
     for (auto& x : P) x = rng.uniform_f();
-    // uniform grid of cells of side >= radius
-    int cells = std::max(1, int(std::floor(1.0f / radius)));
-    if (cells > 1024) cells = 1024;
-    auto cell_of = [&](float x) { int c = int(x * cells); return c >= cells ? cells - 1 : c; };
-    int64_t ncell = 1;
-    for (int d = 0; d < D; d++) ncell *= cells;
-    std::vector<int64_t> cell_id(npts);
-    for (int64_t i = 0; i < npts; i++) {
-        int64_t id = 0;
-        for (int d = D - 1; d >= 0; d--) id = id * cells + cell_of(P[i * D + d]);
-        cell_id[i] = id;
-    }
-    std::vector<int64_t> start(ncell + 1, 0);
-    for (int64_t i = 0; i < npts; i++) start[cell_id[i] + 1]++;
-    for (int64_t c = 0; c < ncell; c++) start[c + 1] += start[c];
-    std::vector<uint32_t> members(npts);
-    {
-        std::vector<int64_t> fill(start.begin(), start.end() - 1);
-        for (int64_t i = 0; i < npts; i++) members[fill[cell_id[i]]++] = uint32_t(i);
-    }
-    // upper adjacency: neighbours with larger index, ascending
-    std::vector<std::vector<Nbr>> up(npts);
-    for (int64_t i = 0; i < npts; i++) {
-        int c[3] = {0, 0, 0};
-        for (int d = 0; d < D; d++) c[d] = cell_of(P[i * D + d]);
-        int lo[3], hi[3];
-        for (int d = 0; d < 3; d++) {
-            lo[d] = d < D ? std::max(0, c[d] - 1) : 0;
-            hi[d] = d < D ? std::min(cells - 1, c[d] + 1) : 0;
+    return P;
+}
+
+// Rips complex of P (npts x D, D in 1..3).  Candidate pairs come from a grid
+// of cells of side > radius over the points' bounding box (cell coordinates in
+// double; at most ~1000 cells per axis), so every pair at float distance <=
+// radius lies in the same or adjacent cells whatever the coordinates' range.
+void gen_rips(const float* P, int64_t npts, int D, float radius, int maxdim, Matrix& out) {
+    double lo[3] = {0, 0, 0}, ext[3] = {0, 0, 0};
+    for (int d = 0; d < D; d++) {
+        float mn = P[d], mx = P[d];
+        for (int64_t i = 1; i < npts; i++) {
+            mn = std::min(mn, P[i * D + d]);
+            mx = std::max(mx, P[i * D + d]);
         }
-        for (int z = lo[2]; z <= hi[2]; z++)
-            for (int y = lo[1]; y <= hi[1]; y++)
-                for (int x = lo[0]; x <= hi[0]; x++) {
-                    int64_t id = (D == 3) ? ((int64_t(z) * cells + y) * cells + x) : (int64_t(y) * cells + x);
-                    for (int64_t m = start[id]; m < start[id + 1]; m++) {
-                        uint32_t j = members[m];
+        lo[d] = double(mn);
+        ext[d] = double(mx) - lo[d];
+    }
+    const double ext_max = std::max({ext[0], ext[1], ext[2]});
+    const double side = std::max({double(radius) * (1.0 + 1.0 / 1024.0), ext_max / 1000.0, 1e-30});
+    int32_t ncell[3] = {1, 1, 1};
+    for (int d = 0; d < D; d++) ncell[d] = int32_t(std::min(1001.0, std::floor(ext[d] / side) + 1.0));
+    auto coord = [&](int d, float x) {
+        int32_t k = int32_t(std::floor((double(x) - lo[d]) / side));
+        return k < 0 ? 0 : (k >= ncell[d] ? ncell[d] - 1 : k);
+    };
+    auto cell_id = [&](int32_t x, int32_t y, int32_t z) {
+        return (uint64_t(z) * uint64_t(ncell[1]) + uint64_t(y)) * uint64_t(ncell[0]) + uint64_t(x);
+    };
+    std::vector<std::pair<uint64_t, uint32_t>> members(static_cast<size_t>(npts));
+    for (int64_t i = 0; i < npts; i++) {
+        int32_t c[3] = {0, 0, 0};
+        for (int d = 0; d < D; d++) c[d] = coord(d, P[i * D + d]);
+        members[size_t(i)] = {cell_id(c[0], c[1], c[2]), uint32_t(i)};
+    }
+    std::sort(members.begin(), members.end());
+    // upper adjacency: neighbours with larger index, ascending
+    std::vector<std::vector<Nbr>> up(static_cast<size_t>(npts));
+    for (int64_t i = 0; i < npts; i++) {
+        int32_t c[3] = {0, 0, 0};
+        for (int d = 0; d < D; d++) c[d] = coord(d, P[i * D + d]);
+        int32_t lo_c[3], hi_c[3];
+        for (int d = 0; d < 3; d++) {
+            lo_c[d] = d < D ? std::max(0, c[d] - 1) : 0;
+            hi_c[d] = d < D ? std::min(ncell[d] - 1, c[d] + 1) : 0;
+        }
+        for (int32_t z = lo_c[2]; z <= hi_c[2]; z++)
+            for (int32_t y = lo_c[1]; y <= hi_c[1]; y++)
+                for (int32_t x = lo_c[0]; x <= hi_c[0]; x++) {
+                    const uint64_t id = cell_id(x, y, z);
+                    auto it = std::lower_bound(members.begin(), members.end(), std::make_pair(id, uint32_t(0)));
+                    for (; it != members.end() && it->first == id; ++it) {
+                        uint32_t j = it->second;
                         if (j <= uint32_t(i)) continue;
                         float s = 0.0f;
                         for (int d = 0; d < D; d++) {
@@ -219,10 +237,10 @@ void gen_rips(int64_t npts, int D, uint64_t seed, float radius, int maxdim, Matr
                             s = s + t * t;
                         }
                         float dist = std::sqrt(s);
-                        if (dist <= radius) up[i].push_back({j, dist});
+                        if (dist <= radius) up[size_t(i)].push_back({j, dist});
                     }
                 }
-        std::sort(up[i].begin(), up[i].end(), [](const Nbr& a, const Nbr& b) { return a.v < b.v; });
+        std::sort(up[size_t(i)].begin(), up[size_t(i)].end(), [](const Nbr& a, const Nbr& b) { return a.v < b.v; });
     }
     std::vector<Simplex> sx;
     sx.reserve(size_t(npts) * 8);
@@ -246,7 +264,7 @@ void gen_rips(int64_t npts, int D, uint64_t seed, float radius, int maxdim, Matr
     };
     std::vector<std::pair<uint32_t, float>> c2, c3;
     for (int64_t i = 0; i < npts; i++) {
-        for (const Nbr& e : up[i]) {
+        for (const Nbr& e : up[size_t(i)]) {
             v[0] = uint32_t(i); v[1] = e.v;
             if (maxdim >= 1) sx.push_back(make_simplex(e.d, 1, v));
             if (maxdim < 2) continue;
@@ -302,7 +320,9 @@ void smooth_axis(std::vector<double>& f, int G, int axis, const std::vector<doub
         }
 }
 
-void gen_lowerstar(int G, float sigma, uint64_t seed, Matrix& out) {
+// Seeded N(0,1) white noise on a G^3 grid (x fastest) smoothed by a Gaussian
+// of width sigma voxels, rounded to float32.
+std::vector<float> gen_field(int G, float sigma, uint64_t seed) {
     const int64_t NV = int64_t(G) * G * G;
     SplitMix64 rng(seed);
     std::vector<double> f(NV);
@@ -317,43 +337,56 @@ void gen_lowerstar(int G, float sigma, uint64_t seed, Matrix& out) {
     }
     std::vector<float> val(NV);
     for (int64_t i = 0; i < NV; i++) val[i] = float(f[i]);
-    auto idx = [G](int x, int y, int z) { return uint32_t((int64_t(z) * G + y) * G + x); };
+    return val;
+}
+
+// Lower-star filtration of the Freudenthal triangulation of a gx x gy x gz
+// grid with vertex values `values` (x fastest; -0 read as +0), simplices up
+// to maxdim.
+void gen_lowerstar(const float* values, int gx, int gy, int gz, int maxdim, Matrix& out) {
+    const int64_t NV = int64_t(gx) * gy * gz;
+    std::vector<float> val(values, values + NV);
+    for (auto& x : val)
+        if (x == 0.0f) x = 0.0f;
+    auto idx = [gx, gy](int x, int y, int z) { return uint32_t((int64_t(z) * gy + y) * gx + x); };
     // increments are non-empty subsets of {x,y,z} encoded as bit masks 1..7
-    auto step = [&](uint32_t base, int mask, int& x, int& y, int& z) -> bool {
-        (void)base;
+    auto step = [&](int mask, int& x, int& y, int& z) -> bool {
         if (mask & 1) x++;
         if (mask & 2) y++;
         if (mask & 4) z++;
-        return x < G && y < G && z < G;
+        return x < gx && y < gy && z < gz;
     };
     std::vector<Simplex> sx;
-    sx.reserve(size_t(NV) * 26);
+    sx.reserve(size_t(NV) * (maxdim >= 3 ? 26 : 8));
     uint32_t v[4];
-    for (int z = 0; z < G; z++)
-        for (int y = 0; y < G; y++)
-            for (int x = 0; x < G; x++) {
+    for (int z = 0; z < gz; z++)
+        for (int y = 0; y < gy; y++)
+            for (int x = 0; x < gx; x++) {
                 uint32_t v0 = idx(x, y, z);
                 v[0] = v0;
                 sx.push_back(make_simplex(val[v0], 0, v));
+                if (maxdim < 1) continue;
                 for (int a = 1; a < 8; a++) {
                     int x1 = x, y1 = y, z1 = z;
-                    if (!step(v0, a, x1, y1, z1)) continue;
+                    if (!step(a, x1, y1, z1)) continue;
                     uint32_t v1 = idx(x1, y1, z1);
                     v[1] = v1;
                     float f1 = std::max(val[v0], val[v1]);
                     sx.push_back(make_simplex(f1, 1, v));
+                    if (maxdim < 2) continue;
                     for (int b = 1; b < 8; b++) {
                         if (b & a) continue;
                         int x2 = x1, y2 = y1, z2 = z1;
-                        if (!step(v1, b, x2, y2, z2)) continue;
+                        if (!step(b, x2, y2, z2)) continue;
                         uint32_t v2 = idx(x2, y2, z2);
                         v[2] = v2;
                         float f2 = std::max(f1, val[v2]);
                         sx.push_back(make_simplex(f2, 2, v));
+                        if (maxdim < 3) continue;
                         int c = 7 & ~(a | b);
                         if ((a | b) == 7 || c == 0) continue;
                         int x3 = x2, y3 = y2, z3 = z2;
-                        if (!step(v2, c, x3, y3, z3)) continue;
+                        if (!step(c, x3, y3, z3)) continue;
                         // tetrahedra need all three singleton increments
                         if (__builtin_popcount(a) != 1 || __builtin_popcount(b) != 1) continue;
                         uint32_t v3 = idx(x3, y3, z3);
@@ -374,21 +407,54 @@ struct sspp_gen_matrix {
 extern "C" {
 
 sspp_gen_matrix* sspp_gen_rips(int64_t npts, int32_t space_dim, uint64_t seed, float radius, int32_t maxdim) {
-    if (npts <= 0 || npts >= (int64_t(1) << VBITS) || (space_dim != 2 && space_dim != 3) || maxdim < 0 || maxdim > 3 ||
-        !(radius > 0.0f))
+    if (npts <= 0 || npts >= (int64_t(1) << VBITS) || space_dim < 1 || space_dim > 3) return nullptr;
+    std::vector<float> P = gen_points(npts, space_dim, seed);
+    return sspp_gen_rips_points(npts, space_dim, P.data(), radius, maxdim);
+}
+
+sspp_gen_matrix* sspp_gen_rips_points(int64_t npts, int32_t space_dim, const float* points, float radius,
+                                      int32_t maxdim) {
+    if (npts <= 0 || npts >= (int64_t(1) << VBITS) || space_dim < 1 || space_dim > 3 || maxdim < 0 || maxdim > 3 ||
+        !(radius >= 0.0f) || !std::isfinite(radius) || !points)
         return nullptr;
+    for (int64_t i = 0; i < npts * space_dim; i++)
+        if (!std::isfinite(points[i])) return nullptr;
     auto* h = new (std::nothrow) sspp_gen_matrix;
     if (!h) return nullptr;
-    gen_rips(npts, space_dim, seed, radius, maxdim, h->m);
+    gen_rips(points, npts, space_dim, radius, maxdim, h->m);
     return h;
+}
+
+int32_t sspp_gen_points(int64_t npts, int32_t space_dim, uint64_t seed, float* out) {
+    if (npts < 0 || space_dim < 1 || !out) return -1;
+    std::vector<float> P = gen_points(npts, space_dim, seed);
+    std::memcpy(out, P.data(), P.size() * sizeof(float));
+    return 0;
 }
 
 sspp_gen_matrix* sspp_gen_lowerstar(int32_t grid, float sigma, uint64_t seed) {
     if (grid < 2 || int64_t(grid) * grid * grid >= (int64_t(1) << VBITS) || sigma < 0.0f) return nullptr;
+    std::vector<float> val = gen_field(grid, sigma, seed);
+    return sspp_gen_lowerstar_field(grid, grid, grid, val.data(), 3);
+}
+
+sspp_gen_matrix* sspp_gen_lowerstar_field(int32_t gx, int32_t gy, int32_t gz, const float* values, int32_t maxdim) {
+    if (gx < 1 || gy < 1 || gz < 1 || int64_t(gx) * gy * gz >= (int64_t(1) << VBITS) || maxdim < 0 || maxdim > 3 ||
+        !values)
+        return nullptr;
+    for (int64_t i = 0; i < int64_t(gx) * gy * gz; i++)
+        if (values[i] != values[i]) return nullptr;
     auto* h = new (std::nothrow) sspp_gen_matrix;
     if (!h) return nullptr;
-    gen_lowerstar(grid, sigma, seed, h->m);
+    gen_lowerstar(values, gx, gy, gz, maxdim, h->m);
     return h;
+}
+
+int32_t sspp_gen_field(int32_t grid, float sigma, uint64_t seed, float* out) {
+    if (grid < 1 || sigma < 0.0f || !out) return -1;
+    std::vector<float> val = gen_field(grid, sigma, seed);
+    std::memcpy(out, val.data(), val.size() * sizeof(float));
+    return 0;
 }
 
 int64_t sspp_gen_ncols(const sspp_gen_matrix* h) { return h ? int64_t(h->m.dims.size()) : -1; }

@@ -10,15 +10,25 @@ extern "C" {
 
 typedef struct sspp_gen_matrix sspp_gen_matrix;
 
-/* Rips complex of npts points i.i.d. uniform in [0,1]^space_dim (2 or 3),
- * edges of float32 Euclidean length <= radius, simplices up to maxdim (<= 3).
- * Returns NULL on invalid arguments. */
+/* Rips complex of npts points i.i.d. uniform in [0,1]^space_dim (1..3; the
+ * points of sspp_gen_points), edges of float32 Euclidean length <= radius,
+ * simplices up to maxdim (<= 3).  Returns NULL on invalid arguments. */
 sspp_gen_matrix* sspp_gen_rips(int64_t npts, int32_t space_dim, uint64_t seed, float radius, int32_t maxdim);
+/* Same for the caller's points (npts x space_dim, row-major, finite). */
+sspp_gen_matrix* sspp_gen_rips_points(int64_t npts, int32_t space_dim, const float* points, float radius,
+                                      int32_t maxdim);
+/* The seeded points of sspp_gen_rips: out[npts * space_dim]. */
+int32_t sspp_gen_points(int64_t npts, int32_t space_dim, uint64_t seed, float* out);
 
 /* Lower-star filtration of the Freudenthal triangulation of a grid^3 lattice
  * (all vertices, edges, triangles, tetrahedra); vertex values are N(0,1)
- * white noise smoothed by a Gaussian of width sigma voxels. */
+ * white noise smoothed by a Gaussian of width sigma voxels (sspp_gen_field). */
 sspp_gen_matrix* sspp_gen_lowerstar(int32_t grid, float sigma, uint64_t seed);
+/* Same for the caller's gx x gy x gz field (x fastest, no NaN; -0 read as +0),
+ * simplices up to maxdim. */
+sspp_gen_matrix* sspp_gen_lowerstar_field(int32_t gx, int32_t gy, int32_t gz, const float* values, int32_t maxdim);
+/* The smoothed field of sspp_gen_lowerstar: out[grid^3]. */
+int32_t sspp_gen_field(int32_t grid, float sigma, uint64_t seed, float* out);
 
 int64_t sspp_gen_ncols(const sspp_gen_matrix* m);
 int64_t sspp_gen_nnz(const sspp_gen_matrix* m);

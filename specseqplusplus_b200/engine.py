@@ -48,7 +48,7 @@ class _Stats(ctypes.Structure):
         "nessential")] + [("init_ms", ctypes.c_double), ("compute_ms", ctypes.c_double), ("launches", ctypes.c_int64)] + [
         (k, ctypes.c_double) for k in ("init_gpu_ms", "light_gpu_ms", "heavy_gpu_ms", "pairs_gpu_ms")] + [
         ("light_launches", ctypes.c_int64), ("heavy_launches", ctypes.c_int64), ("arena_ints_used", ctypes.c_int64),
-        ("tuned_candidate", ctypes.c_int64), ("heavy_additions", ctypes.c_int64)]
+        ("tuned_candidate", ctypes.c_int64), ("heavy_additions", ctypes.c_int64), ("build_ms", ctypes.c_double)]
 
 
 class _ServerConfig(ctypes.Structure):
@@ -102,6 +102,10 @@ def load_library():
         "sspp_load_phat": (i32, [vp, ctypes.c_char_p, i32]),
         "sspp_load_csc": (i32, [vp, i64, vp, vp, vp]),
         "sspp_load_csc_device": (i32, [vp, i64, vp, vp, vp]),
+        "sspp_load_rips": (i32, [vp, i64, i32, vp, ctypes.c_float, i32]),
+        "sspp_load_lowerstar": (i32, [vp, i64, i64, i64, vp, i32]),
+        "sspp_input_size": (i32, [vp, vp, vp]),
+        "sspp_input_copy": (i32, [vp, vp, vp, vp, vp]),
         "sspp_init": (i32, [vp, ctypes.POINTER(_Params), vp]),
         "sspp_compute": (i32, [vp, vp]),
         "sspp_reduce": (i32, [vp, ctypes.POINTER(_Params), vp]),
@@ -163,7 +167,8 @@ EXPORTED = ("sspp_create", "sspp_destroy", "sspp_last_error", "sspp_default_para
             "sspp_server_pairs", "sspp_server_num_essential", "sspp_server_essentials", "sspp_server_latency_ms",
             "sspp_server_release", "sspp_server_get_stats", "sspp_server_reset_stats", "sspp_phat_read",
             "sspp_phat_ncols", "sspp_phat_nnz", "sspp_phat_copy", "sspp_phat_free", "sspp_phat_write",
-            "sspp_export_preprocessed")
+            "sspp_export_preprocessed", "sspp_load_rips", "sspp_load_lowerstar", "sspp_input_size",
+            "sspp_input_copy")
 
 
 class Engine:
@@ -204,6 +209,54 @@ class Engine:
 
     def load_csc_device(self, ncols: int, d_dims: int, d_col_ptr: int, d_rows: int) -> None:
         self._check(self._lib.sspp_load_csc_device(self._h, ncols, d_dims, d_col_ptr, d_rows))
+
+    @staticmethod
+    def _float_buffer(x, shape_ndim: int):
+        """(pointer, shape, keep-alive) of a float32 array: a CUDA tensor is read in place."""
+        if hasattr(x, "data_ptr") and getattr(x, "is_cuda", False):
+            import torch
+
+            if x.dtype != torch.float32 or not x.is_contiguous() or x.dim() != shape_ndim:
+                raise ValueError(f"expected a contiguous float32 tensor of {shape_ndim} dimensions")
+            return x.data_ptr(), tuple(x.shape), x
+        a = np.ascontiguousarray(x, dtype=np.float32)
+        if a.ndim != shape_ndim:
+            raise ValueError(f"expected an array of {shape_ndim} dimensions")
+        return a.ctypes.data, a.shape, a
+
+    def load_rips(self, points, radius: float, maxdim: int = 3) -> None:
+        """Builds the Vietoris-Rips complex of ``points`` [npts, D] (float32, D = 1..3; a numpy array or a
+        CUDA tensor) on the device and loads it; same matrix as ``gen.rips_from_points``."""
+        ptr, shape, keep = self._float_buffer(points, 2)
+        self._check(self._lib.sspp_load_rips(self._h, shape[0], shape[1], ptr if shape[0] else None,
+                                             float(radius), int(maxdim)))
+        del keep
+        self._batch_k = 0
+
+    def load_lowerstar(self, values, maxdim: int = 3) -> None:
+        """Builds the Freudenthal lower-star filtration of the field ``values`` [gz, gy, gx] (float32, x
+        fastest; a numpy array or a CUDA tensor) on the device and loads it; same matrix as
+        ``gen.lowerstar_from_field``."""
+        ptr, shape, keep = self._float_buffer(values, 3)
+        gz, gy, gx = shape
+        self._check(self._lib.sspp_load_lowerstar(self._h, gx, gy, gz, ptr, int(maxdim)))
+        del keep
+        self._batch_k = 0
+
+    def input_matrix(self, values: bool = False):
+        """The loaded matrix copied back (with its filtration values for a built complex)."""
+        from .gen import BoundaryMatrix
+
+        n = ctypes.c_int64()
+        z = ctypes.c_int64()
+        self._check(self._lib.sspp_input_size(self._h, ctypes.byref(n), ctypes.byref(z)))
+        dims = np.empty(n.value, dtype=np.int32)
+        col_ptr = np.empty(n.value + 1, dtype=np.int64)
+        rows = np.empty(max(z.value, 1), dtype=np.int32)
+        vals = np.empty(max(n.value, 1), dtype=np.float32) if values else None
+        self._check(self._lib.sspp_input_copy(self._h, dims.ctypes.data, col_ptr.ctypes.data, rows.ctypes.data,
+                                              vals.ctypes.data if values else None))
+        return BoundaryMatrix(dims, col_ptr, rows[:z.value], vals[:n.value] if values else None)
 
     def load_batch(self, matrices) -> None:
         """k independent complexes reduced together (block-diagonal concatenation)."""

@@ -1,8 +1,8 @@
 """Synthetic filtered complexes as PHAT boundary matrices (input side).
 
-Thin ctypes front end of ``csrc/sspp_gen.cpp``: seeded Vietoris-Rips complexes
-of uniform point clouds and Freudenthal lower-star filtrations of smoothed
-Gaussian noise, ordered by (filtration value, dimension, lexicographic vertex
+Thin ctypes front end of ``csrc/sspp_gen.cpp``: Vietoris-Rips complexes of
+point clouds (seeded uniform, or the caller's) and Freudenthal lower-star
+filtrations of scalar fields (seeded smoothed Gaussian noise, or the caller's), ordered by (filtration value, dimension, lexicographic vertex
 tuple) with int32 face indices.  These are the synthetic stand-ins for the
 reference's PHAT input files (read by ``src/main.cu:90-167``).
 """
@@ -38,6 +38,15 @@ def _load():
         lib.sspp_gen_copy.argtypes = [ctypes.c_void_p] + [ctypes.c_void_p] * 4
         lib.sspp_gen_free.restype = None
         lib.sspp_gen_free.argtypes = [ctypes.c_void_p]
+        lib.sspp_gen_rips_points.restype = ctypes.c_void_p
+        lib.sspp_gen_rips_points.argtypes = [ctypes.c_int64, ctypes.c_int32, ctypes.c_void_p, ctypes.c_float,
+                                             ctypes.c_int32]
+        lib.sspp_gen_lowerstar_field.restype = ctypes.c_void_p
+        lib.sspp_gen_lowerstar_field.argtypes = [ctypes.c_int32] * 3 + [ctypes.c_void_p, ctypes.c_int32]
+        lib.sspp_gen_points.restype = ctypes.c_int32
+        lib.sspp_gen_points.argtypes = [ctypes.c_int64, ctypes.c_int32, ctypes.c_uint64, ctypes.c_void_p]
+        lib.sspp_gen_field.restype = ctypes.c_int32
+        lib.sspp_gen_field.argtypes = [ctypes.c_int32, ctypes.c_float, ctypes.c_uint64, ctypes.c_void_p]
         _lib = lib
     return _lib
 
@@ -100,6 +109,36 @@ def rips(npts: int, space_dim: int, seed: int, radius: float, maxdim: int = 3) -
 def lowerstar(grid: int, sigma: float, seed: int) -> BoundaryMatrix:
     """Lower-star filtration of the Freudenthal triangulation of a grid^3 lattice."""
     return _take(_load().sspp_gen_lowerstar(int(grid), float(sigma), int(seed) & (2**64 - 1)))
+
+
+def points(npts: int, space_dim: int, seed: int) -> np.ndarray:
+    """The seeded point cloud of ``rips(npts, space_dim, seed, ...)``: float32 [npts, space_dim]."""
+    out = np.empty((int(npts), int(space_dim)), dtype=np.float32)
+    if _load().sspp_gen_points(int(npts), int(space_dim), int(seed) & (2**64 - 1), out.ctypes.data):
+        raise ValueError("invalid generator arguments")
+    return out
+
+
+def field(grid: int, sigma: float, seed: int) -> np.ndarray:
+    """The smoothed noise of ``lowerstar(grid, sigma, seed)``: float32 [grid, grid, grid] as [z, y, x]."""
+    out = np.empty((int(grid),) * 3, dtype=np.float32)
+    if _load().sspp_gen_field(int(grid), float(sigma), int(seed) & (2**64 - 1), out.ctypes.data):
+        raise ValueError("invalid generator arguments")
+    return out
+
+
+def rips_from_points(pts, radius: float, maxdim: int = 3) -> BoundaryMatrix:
+    """Vietoris-Rips complex of the float32 points ``pts`` [npts, D] (D = 1..3)."""
+    pts = np.ascontiguousarray(pts, dtype=np.float32)
+    n, d = pts.shape
+    return _take(_load().sspp_gen_rips_points(n, d, pts.ctypes.data, float(radius), int(maxdim)))
+
+
+def lowerstar_from_field(values, maxdim: int = 3) -> BoundaryMatrix:
+    """Freudenthal lower-star filtration of the float32 field ``values`` [gz, gy, gx] (x fastest)."""
+    v = np.ascontiguousarray(values, dtype=np.float32)
+    gz, gy, gx = v.shape
+    return _take(_load().sspp_gen_lowerstar_field(gx, gy, gz, v.ctypes.data, int(maxdim)))
 
 
 def rips_radius_for_degree(npts: int, space_dim: int, mean_degree: float) -> float:

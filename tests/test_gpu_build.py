@@ -1,0 +1,159 @@
+"""GPU tests of the device complex builders (sspp_load_rips / sspp_load_lowerstar
+through the C ABI): the matrix built on the device equals the host generator's
+bit for bit (dims, col_ptr, rows and float32 values), and reducing it gives the
+same pairs as reducing the host matrix.  The host generator itself is pinned
+against a brute-force clique construction on the CPU (test_gen.py)."""
+import numpy as np
+import pytest
+
+import oracle
+from specseqplusplus_b200 import Engine, Params, SsppError, gen
+
+pytestmark = pytest.mark.gpu
+
+
+def _same_matrix(a, b):
+    assert a.ncols == b.ncols and a.nnz == b.nnz
+    assert np.array_equal(a.dims, b.dims)
+    assert np.array_equal(a.col_ptr, b.col_ptr)
+    assert np.array_equal(a.rows, b.rows)
+    assert np.array_equal(a.values.view(np.uint32), b.values.view(np.uint32))
+
+
+def _built_rips(e, pts, radius, maxdim):
+    e.load_rips(pts, radius, maxdim)
+    return e.input_matrix(values=True)
+
+
+def _built_lowerstar(e, f, maxdim=3):
+    e.load_lowerstar(f, maxdim)
+    return e.input_matrix(values=True)
+
+
+RIPS = [  # (npts, space_dim, seed, radius, maxdim)
+    (2000, 3, 1, 0.08, 3),        # the 2000-point 3-D Rips workload
+    (100000, 3, 7, 0.016, 3),     # the 100k-point 3-D Rips workload
+    (1500, 2, 5, 0.06, 2),
+    (1500, 3, 9, gen.rips_radius_for_degree(1500, 3, 40), 3),  # mean degree 40
+    (3000, 2, 4, 0.03, 1),
+    (500, 1, 3, 0.01, 1),
+    (700, 3, 6, 0.16, 0),
+]
+
+
+@pytest.mark.parametrize("args", RIPS)
+def test_rips_matches_host(args):
+    n, d, seed, r, maxdim = args
+    with Engine(0) as e:
+        got = _built_rips(e, gen.points(n, d, seed), r, maxdim)
+    _same_matrix(got, gen.rips(n, d, seed, r, maxdim))
+
+
+def test_rips_unusual_point_sets():
+    rng = np.random.default_rng(11)
+    clouds = [
+        (rng.normal(size=(3000, 3)).astype(np.float32) * 5.0, 0.6, 3),        # unbounded, negative
+        (np.repeat(rng.random((400, 2), dtype=np.float32), 3, axis=0), 0.05, 2),  # every point three times
+        (rng.random((40, 3), dtype=np.float32), 10.0, 3),                    # complete graph
+        (rng.random((800, 3), dtype=np.float32), 1e-4, 3),                   # (almost) no edges
+        (np.repeat(rng.random((50, 3), dtype=np.float32), 2, axis=0), 0.0, 3),   # radius 0: duplicates only
+        (rng.random((1, 2), dtype=np.float32), 0.5, 3),                      # one point
+        (rng.random((5000, 3), dtype=np.float32) * 1e4 + 1e6, 150.0, 2),     # large offset coordinates
+    ]
+    with Engine(0) as e:
+        for pts, r, maxdim in clouds:
+            _same_matrix(_built_rips(e, pts, r, maxdim), gen.rips_from_points(pts, r, maxdim))
+
+
+LOWERSTAR = [(12, 1.5, 4), (16, 2.0, 2), (32, 2.0, 2), (64, 2.0, 2)]  # the last is the 64^3 grid workload
+
+
+@pytest.mark.parametrize("args", LOWERSTAR)
+def test_lowerstar_matches_host(args):
+    g, sigma, seed = args
+    with Engine(0) as e:
+        got = _built_lowerstar(e, gen.field(g, sigma, seed))
+    _same_matrix(got, gen.lowerstar(g, sigma, seed))
+
+
+def test_lowerstar_unusual_fields():
+    rng = np.random.default_rng(12)
+    ties = rng.integers(-3, 4, size=(9, 10, 11)).astype(np.float32)
+    ties[ties == 0] = -0.0
+    fields = [
+        (rng.normal(size=(7, 5, 3)).astype(np.float32), 3),
+        (rng.normal(size=(1, 40, 30)).astype(np.float32), 3),    # a 2-D image
+        (rng.normal(size=(50, 1, 1)).astype(np.float32), 3),     # a 1-D signal
+        (ties, 3),                                               # many equal values, signed zeros
+        (ties, 2),
+        (np.zeros((6, 6, 6), dtype=np.float32), 3),              # constant field
+        (rng.normal(size=(2, 2, 2)).astype(np.float32), 1),
+    ]
+    with Engine(0) as e:
+        for f, maxdim in fields:
+            _same_matrix(_built_lowerstar(e, f, maxdim), gen.lowerstar_from_field(f, maxdim))
+
+
+def test_built_complexes_reduce_like_loaded_ones():
+    cases = [("r", (2000, 3, 1, 0.08, 3), Params()),
+             ("r", (100000, 3, 7, 0.016, 3), Params(model=3, max_iteration=100, level1_capacity=100,
+                                                    level2_capacity=250)),
+             ("l", (32, 2.0, 2), Params(model=1, max_iteration=10)),
+             ("l", (16, 1.0, 5), Params(dualize=1))]
+    with Engine(0) as e:
+        for kind, args, p in cases:
+            if kind == "r":
+                n, d, seed, r, maxdim = args
+                m = gen.rips(*args)
+                e.load_rips(gen.points(n, d, seed), r, maxdim)
+            else:
+                m = gen.lowerstar(*args)
+                e.load_lowerstar(gen.field(*args))
+            e.reduce(p)
+            built = (e.pairs(), e.essentials())
+            assert e.stats()["build_ms"] > 0
+            e.load_csc(m)
+            e.reduce(p)
+            assert np.array_equal(built[0], e.pairs()) and np.array_equal(built[1], e.essentials())
+    # and against the oracle on a small one
+    m = gen.rips(600, 3, 2, 0.15, 3)
+    ref = oracle.reduce(m)
+    with Engine(0) as e:
+        e.load_rips(gen.points(600, 3, 2), 0.15, 3)
+        e.reduce(Params())
+        assert np.array_equal(e.pairs(), ref.pairs) and np.array_equal(e.essentials(), ref.essential)
+
+
+def test_device_resident_inputs_and_buffer_reuse():
+    torch = pytest.importorskip("torch")
+    pts = gen.points(20000, 3, 21)
+    f = gen.field(24, 1.5, 22)
+    with Engine(0) as e:
+        # large, small, large again: the builder's buffers grow and are reused
+        for _ in range(2):
+            _same_matrix(_built_rips(e, torch.from_numpy(pts).cuda(), 0.03, 3),
+                         gen.rips_from_points(pts, 0.03, 3))
+            _same_matrix(_built_lowerstar(e, torch.from_numpy(f).cuda()), gen.lowerstar_from_field(f))
+            _same_matrix(_built_rips(e, pts[:300], 0.2, 2), gen.rips_from_points(pts[:300], 0.2, 2))
+
+
+def test_builders_reject_bad_input():
+    with Engine(0) as e:
+        bad = gen.points(100, 3, 1)
+        bad[17, 2] = np.inf
+        with pytest.raises(SsppError):
+            e.load_rips(bad, 0.2, 3)
+        f = gen.field(8, 1.0, 1)
+        f[3, 4, 5] = np.nan
+        with pytest.raises(SsppError):
+            e.load_lowerstar(f)
+        with pytest.raises(SsppError):
+            e.load_rips(gen.points(10, 3, 1), 0.2, 4)  # maxdim above 3
+        with pytest.raises(SsppError):
+            e.reduce(Params())  # nothing loaded after a failed build
+        # the context stays usable
+        e.load_rips(gen.points(300, 2, 3), 0.1, 2)
+        e.reduce(Params())
+        with pytest.raises(SsppError):
+            e.load_csc(gen.rips(50, 2, 1, 0.2, 2))
+            e.input_matrix(values=True)  # values exist for built complexes only
