@@ -91,6 +91,8 @@ typedef struct sspp_stats {
     int64_t heavy_additions;     /* additions done by the CTA tier                 */
     double build_ms;             /* last sspp_load_rips / sspp_load_lowerstar (host
                                     clock, input staging included), else 0          */
+    int64_t heavy_fast_inline;   /* CTA-tier additions of short apparent addends    */
+    int64_t heavy_fast_slot;     /* CTA-tier additions of short published addends   */
 } sspp_stats;
 
 /* Replaces: the SpecSeqPlusPlus constructor's allocation (include/specseq.h:486-512). */

@@ -1318,6 +1318,8 @@ int32_t sspp_get_stats(const sspp_ctx* ctx, sspp_stats* o) {
     o->light_launches = ctx->light_launches;
     o->heavy_launches = ctx->heavy_launches;
     o->build_ms = ctx->build_ms;
+    o->heavy_fast_inline = c[CNT_FAST_INLINE];
+    o->heavy_fast_slot = c[CNT_FAST_SLOT];
     return SSPP_OK;
 }
 

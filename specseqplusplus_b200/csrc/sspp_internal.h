@@ -81,6 +81,8 @@ enum CounterIdx {
     CNT_NPAIRS,
     CNT_NESS,
     CNT_HEAVY_ADDS,  // additions done by the CTA tier
+    CNT_FAST_INLINE, // CTA-tier short-addend additions whose addend was an inline apparent column
+    CNT_FAST_SLOT,   // ... whose addend was read through the pivot entry and the arena
     CNT_NUM
 };
 

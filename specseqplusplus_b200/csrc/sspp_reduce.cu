@@ -508,16 +508,20 @@ __device__ bool publish(const G& g, const ReduceArgs& A, int col, Work& w) {
 enum Outcome { OUT_OWNER, OUT_ZERO, OUT_PARKED, OUT_DEFERRED, OUT_FAIL };
 
 // Short addends in the CTA tier.  Along the long chains the CTA tier runs, the
-// working column holds hundreds of entries while the addends (owners'
-// versions) hold a handful: the two tops cancel, and the addend's other
-// entries change the column only from the lowest position where one of them
-// lands.  Warp 0 alone finds those positions by binary search in shared
-// memory, rewrites just that suffix (its xor with the addend, through the
-// spare buffer) and goes on to the next lowest row, whose pivot entry it has
-// requested before the rewrite; the rest of the CTA waits at one barrier.
-// The warp stops, leaving the step to the general path, when the row must be
-// claimed (no owner, or a larger one), the column is empty or below the band,
-// or the addend is longer than kShortAddend entries or would not fit.
+// working column holds hundreds to thousands of entries while the addends
+// (owners' versions) hold a handful, so rewriting the column for each addend
+// would cost O(column) per addition.  Warp 0 alone keeps the column as a
+// sorted bulk in shared memory plus a delta: up to 32 pending entries (sorted,
+// one per lane, in registers) whose xor with the bulk is the column.  The
+// lowest row only moves down, so it is always the larger of the two tops (equal
+// tops cancel); an addition removes that top and toggles the addend's other
+// entries in the delta (a ballot and a shuffle each).  The delta is folded
+// into the bulk when it fills and when the warp stops, by rewriting the bulk
+// from the lowest position a delta entry lands, one constant-shift segment per
+// delta entry, through the spare buffer.  The rest of the CTA waits at one
+// barrier.  The warp stops, leaving the step to the general path, when the row
+// must be claimed (no owner, or a larger one), the column is empty or below the
+// band, or the addend is longer than kShortAddend entries or would not fit.
 // Returns the additions done, or -1 after a failed self-check.
 constexpr int kShortAddend = 28;  // header + entries in one 32-lane load
 
@@ -527,16 +531,66 @@ struct FastState {
     int len, L, adds, bad;
 };
 
+// a[0..nb) xor {dv on lanes 0..d-1, ascending} back into a; returns the new
+// length (the caller keeps it within the buffer) and pads with INT_MAX.  One
+// warp; tmp is a spare buffer of the same capacity.
+__device__ int fold_delta(int32_t* a, int nb, int dv, int d, int32_t* tmp, int* err) {
+    const int lane = threadIdx.x & 31;
+    int pos = nb;
+    bool fnd = false;
+    if (lane < d) {
+        pos = lower_bound_t<false>(a, nb, dv);
+        fnd = pos < nb && lds(a + pos) == dv;
+    }
+    const int pmin = warp_min(pos);
+    const unsigned fmask = __ballot_sync(kFull, lane < d && fnd);
+    const unsigned imask = __ballot_sync(kFull, lane < d && !fnd);
+    // segment j (j = -1 .. d-1) of the bulk suffix: from delta entry j's position
+    // (past the entry it cancels) to the next delta entry's; its entries move by
+    // the insertions minus the cancellations at or before it
+    for (int j = -1; j < d; j++) {
+        const int pj = j < 0 ? pmin : __shfl_sync(kFull, pos, j);
+        const bool fj = j >= 0 && ((fmask >> j) & 1);
+        const int lo = pj + (fj ? 1 : 0);
+        const int hi = j + 1 < d ? __shfl_sync(kFull, pos, j + 1) : nb;
+        const unsigned upto = j < 0 ? 0u : (j == 31 ? kFull : ((2u << j) - 1));
+        const int shift = __popc(imask & upto) - __popc(fmask & upto);
+        for (int i = lo + lane; i < hi; i += 32) {
+            const int t = i - pmin + shift;
+            tmp[t] = lds(a + i);
+        }
+    }
+    if (lane < d && !fnd) {  // inserted delta entries land before the bulk entry at their position
+        const unsigned lt = lanemask_lt();
+        const int t = pos - pmin + __popc(imask & lt) - __popc(fmask & lt);
+        tmp[t] = dv;
+    }
+    __syncwarp();
+    const int outl = nb - pmin + __popc(imask) - __popc(fmask);
+    for (int i = lane; i < outl; i += 32) a[pmin + i] = tmp[i];
+    const int nn = pmin + outl;
+    if (lane < int(pad4(nn) - nn)) a[nn + lane] = INT_MAX;
+    __syncwarp();
+    (void)err;
+    return nn;
+}
+
 template <int T>
 __device__ int fast_adds(const BlockG<T>& g, const ReduceArgs& A, int col, Work& w, int& L, uint64_t& e,
                          int32_t* tmp, int32_t* sb, long long& adds, long long& add_ints, int iters_left) {
     __shared__ FastState fs;
+    (void)sb;
     if (threadIdx.x < 32) {
         const int lane = threadIdx.x;
         int32_t* a = w.buf;
-        int n = w.len, Lc = L, done = 0, bad = 0;
+        int nb = w.len;         // bulk a[0..nb), ascending; its top is a[nb-1]
+        int d = 0;              // delta: dv on lanes 0..d-1, ascending, INT_MAX above
+        int dv = INT_MAX;
+        int Lc = L, done = 0, bad = 0;
+        bool top_in_bulk = true;  // Lc is a[nb-1] (else the delta's top)
         uint64_t ec = e;
         long long ai = 0;
+        int n_inline = 0;
         // inline copy of the current row's apparent column, if it has one
         int4 ap = make_int4(-1, 0, 0, 0);
         if (lane == 31 && Lc >= 0 && Lc < A.ncols) ap = __ldg(A.app + Lc);
@@ -545,12 +599,11 @@ __device__ int fast_adds(const BlockG<T>& g, const ReduceArgs& A, int col, Work&
         ap.z = __shfl_sync(kFull, ap.z, 31);
         ap.w = __shfl_sync(kFull, ap.w, 31);
         bool have_e = true;  // ec is the pivot entry of Lc
-        while (done < iters_left && n > 0 && Lc >= A.minrow) {
+        while (done < iters_left && nb + d > 0 && Lc >= A.minrow) {
             int plen, bj;
             if (ap.x >= 0) {  // apparent owner: permanent, its entries are at hand
                 plen = ap.x + 1;
                 bj = lane == 0 ? ap.y : (lane == 1 ? ap.z : ap.w);
-                if (n + plen > A.cap) break;
             } else {
                 if (!have_e) {
                     uint64_t t = 0;
@@ -563,90 +616,85 @@ __device__ int fast_adds(const BlockG<T>& g, const ReduceArgs& A, int col, Work&
                 const int v = __ldcg(A.arena + pv_slot(ec) + lane);      // header and the first 28 entries
                 plen = __shfl_sync(kFull, v, 0);
                 const int hcol = __shfl_sync(kFull, v, 1);
-                if (plen < 1 || plen > kShortAddend || hcol != pv_col(ec) || n + plen > A.cap) break;
+                if (plen < 1 || plen > kShortAddend || hcol != pv_col(ec)) break;
                 if (__shfl_sync(kFull, v, (kHdr + plen - 1) & 31) != Lc) break;  // the general path reports it
                 bj = __shfl_sync(kFull, v, (lane + kHdr) & 31);
             }
             const int m = plen - 1;  // addend entries below the common top
-            if (lane < m) sb[lane] = bj;
-            if (lane == 0) sb[m] = Lc;
-            __syncwarp();
-            // the next lowest row is known now: request its inline apparent column
-            int4 apn = make_int4(-1, 0, 0, 0);
-            int L2 = -1;
-            if (lane == 31) {
-                L2 = next_low(a, n, false, sb, plen, false);
-                if (L2 >= 0 && L2 < A.ncols && L2 >= A.minrow) apn = __ldg(A.app + L2);
+            if (nb + d + m > A.cap) break;  // the folded column might not fit
+            if (top_in_bulk) {  // the tops cancel
+                nb--;
+            } else {
+                d--;
+                if (lane == d) dv = INT_MAX;
             }
-            // lane j < m: where addend entry j lands below the top, and whether it cancels
-            int pos = n - 1;
-            bool fnd = false;
-            if (lane < m) {
-                pos = lower_bound_t<false>(a, n - 1, bj);
-                fnd = pos < n - 1 && lds(a + pos) == bj;
-            }
-            const int pmin = warp_min(pos);
-            const int sl = n - 1 - pmin;  // suffix below the top that the addend touches
-            const unsigned fmask = __ballot_sync(kFull, fnd);
-            const unsigned imask = __ballot_sync(kFull, lane < m && !fnd);
-            // suffix entries: shifted right by the insertions before them, left by the cancellations
-            for (int base = pmin; base < n - 1; base += 32) {
-                const int i = base + lane;
-                const bool in = i < n - 1;
-                const int x = in ? lds(a + i) : 0;
-                int shift = 0;
-                bool drop = false;
-                for (int j = 0; j < m; j++) {
-                    const int pj = __shfl_sync(kFull, pos, j);
-                    if ((fmask >> j) & 1) {
-                        if (pj < i) shift--;
-                        else if (pj == i) drop = true;
-                    } else if (pj <= i) {
-                        shift++;
+            // toggle the addend's other entries in the delta
+            for (int j = 0; j < m; j++) {
+                const int x = __shfl_sync(kFull, bj, j);
+                const unsigned eq = __ballot_sync(kFull, lane < d && dv == x);
+                if (eq) {
+                    const int q = __ffs(eq) - 1;
+                    const int nx = __shfl_down_sync(kFull, dv, 1);
+                    if (lane >= q) dv = lane + 1 < d ? nx : INT_MAX;
+                    d--;
+                } else {
+                    if (d == 32) {  // full: the bulk absorbs the delta
+                        nb = fold_delta(a, nb, dv, d, tmp, A.err);
+                        d = 0;
+                        dv = INT_MAX;
                     }
-                }
-                if (in && !drop) {
-                    const int t = i - pmin + shift;
-                    if (t >= 0 && t < A.cap) tmp[t] = x;
-                    else atomicOr(A.err, ERRB_BAD_INPUT);  // addend not strictly increasing
+                    const int q = __popc(__ballot_sync(kFull, lane < d && dv < x));
+                    const int pv = __shfl_up_sync(kFull, dv, 1);
+                    if (lane > q && lane <= d) dv = pv;
+                    if (lane == q) dv = x;
+                    d++;
                 }
             }
-            if (lane < m && !fnd) {  // inserted addend entries
-                const unsigned lt = lanemask_lt();
-                const int t = pos - pmin + __popc(imask & lt) - __popc(fmask & lt);
-                if (t >= 0 && t < A.cap) tmp[t] = bj;
-                else atomicOr(A.err, ERRB_BAD_INPUT);
+            // the next lowest row: the larger top; equal tops cancel
+            int nl = -1;
+            while (true) {
+                const int tb = nb > 0 ? lds(a + nb - 1) : -1;
+                const int td = d > 0 ? __shfl_sync(kFull, dv, d - 1) : -1;
+                if (tb >= 0 && tb == td) {
+                    nb--;
+                    d--;
+                    if (lane == d) dv = INT_MAX;
+                    continue;
+                }
+                top_in_bulk = tb > td;
+                nl = top_in_bulk ? tb : td;
+                break;
             }
-            __syncwarp();
-            const int outl = sl + __popc(imask) - __popc(fmask);
-            for (int i = lane; i < outl; i += 32) a[pmin + i] = tmp[i];
-            const int nn = pmin + outl;
-            if (lane < int(pad4(nn) - nn)) a[nn + lane] = INT_MAX;
-            __syncwarp();
-            ai += n + plen + nn;
-            n = nn;
+            ai += 2 * (nb + d) + plen + 1;
             done++;
-            Lc = n ? lds(a + n - 1) : -1;
-            L2 = __shfl_sync(kFull, L2, 31);
-            if (Lc >= A.ncols || Lc != L2) {  // self-check: row index, next-low prediction
+            if (ap.x >= 0) n_inline++;
+            if (nl >= Lc || nl >= A.ncols) {  // self-check: the lowest row only moves down
                 bad = 1;
                 break;
             }
-            ap.x = __shfl_sync(kFull, apn.x, 31);
-            ap.y = __shfl_sync(kFull, apn.y, 31);
-            ap.z = __shfl_sync(kFull, apn.z, 31);
-            ap.w = __shfl_sync(kFull, apn.w, 31);
+            Lc = nl;
+            ap = make_int4(-1, 0, 0, 0);
+            if (lane == 31 && Lc >= 0 && Lc >= A.minrow) ap = __ldg(A.app + Lc);
+            ap.x = __shfl_sync(kFull, ap.x, 31);
+            ap.y = __shfl_sync(kFull, ap.y, 31);
+            ap.z = __shfl_sync(kFull, ap.z, 31);
+            ap.w = __shfl_sync(kFull, ap.w, 31);
             have_e = false;
             ec = kNoOwner;  // unknown; the general path's claim retries with the real entry
         }
+        if (d > 0) nb = fold_delta(a, nb, dv, d, tmp, A.err);
         if (lane == 0) {
-            fs.len = n;
-            fs.L = Lc;
+            fs.len = nb;
+            fs.L = nb > 0 ? lds(a + nb - 1) : -1;
             fs.e = ec;
             fs.adds = done;
             fs.add_ints = ai;
-            fs.bad = bad;
-            if (bad) atomicOr(A.err, ERRB_CHECK);
+            fs.bad = bad || (fs.L != (nb > 0 ? Lc : -1) && done > 0);
+            if (fs.bad) atomicOr(A.err, ERRB_CHECK);
+            if (done) {
+                cnt_add(&A.counters[CNT_FAST_INLINE], n_inline);
+                cnt_add(&A.counters[CNT_FAST_SLOT], done - n_inline);
+            }
         }
     }
     __syncthreads();

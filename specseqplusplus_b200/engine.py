@@ -48,7 +48,8 @@ class _Stats(ctypes.Structure):
         "nessential")] + [("init_ms", ctypes.c_double), ("compute_ms", ctypes.c_double), ("launches", ctypes.c_int64)] + [
         (k, ctypes.c_double) for k in ("init_gpu_ms", "light_gpu_ms", "heavy_gpu_ms", "pairs_gpu_ms")] + [
         ("light_launches", ctypes.c_int64), ("heavy_launches", ctypes.c_int64), ("arena_ints_used", ctypes.c_int64),
-        ("tuned_candidate", ctypes.c_int64), ("heavy_additions", ctypes.c_int64), ("build_ms", ctypes.c_double)]
+        ("tuned_candidate", ctypes.c_int64), ("heavy_additions", ctypes.c_int64), ("build_ms", ctypes.c_double),
+        ("heavy_fast_inline", ctypes.c_int64), ("heavy_fast_slot", ctypes.c_int64)]
 
 
 class _ServerConfig(ctypes.Structure):
