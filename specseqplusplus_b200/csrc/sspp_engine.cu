@@ -84,6 +84,10 @@ struct sspp_ctx {
     double init_ms = 0, compute_ms = 0;
     int64_t ss_steps = 0;
     int* h_err = nullptr;          // pinned
+    int* h_gate = nullptr;         // mapped pinned: CTA-tier pool columns finished (mirror)
+    int* d_gate = nullptr;         // its device address
+    int* h_tail = nullptr;         // pinned: the pool tail after a dimension's sweep
+    cudaEvent_t gate_ev = nullptr;
     long long* h_counters = nullptr;
     DimInfo* h_info = nullptr;
     unsigned long long* h_top = nullptr;
@@ -148,7 +152,8 @@ cudaError_t grow(T*& p, int64_t& cap, int64_t want, cudaStream_t s) {
 void free_device(Device& D) {
     void* ptrs[] = {D.dim, D.perm, D.newidx, D.scratch64, D.arena, D.arena_top,
                     D.desc, D.low, D.pivot, D.state, D.cleared, D.negative, D.leftmost, D.active, D.blk, D.dimcnt,
-                    D.diminfo, D.err, D.counters, D.step_ctr, D.heavy, D.pool_tail, D.death_of, D.pairs, D.ess, D.misc, D.app};
+                    D.diminfo, D.err, D.counters, D.step_ctr, D.heavy, D.pool_tail, D.heavy_done, D.death_of, D.pairs,
+                    D.ess, D.misc, D.app};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     D = Device();
@@ -194,6 +199,7 @@ int ensure_columns(sspp_ctx* ctx, int64_t n, int64_t nnz) {
         CK(cudaMalloc(&D.counters, sizeof(long long) * CNT_NUM));
         CK(cudaMalloc(&D.arena_top, sizeof(unsigned long long)));
         CK(cudaMalloc(&D.pool_tail, sizeof(int)));
+        CK(cudaMalloc(&D.heavy_done, sizeof(int)));
         CK(cudaMalloc(&D.misc, sizeof(int64_t) * 8));
     }
     return SSPP_OK;
@@ -452,6 +458,44 @@ int run_init(sspp_ctx* ctx) {
 
 // Runs one spectral-sequence schedule: per step a light-tier launch on the
 // main stream and a heavy-tier launch for the columns it deferred.
+// Dimension gate.  The next dimension's columns are cleared by the claims of
+// this one, so it used to start only once every CTA-tier column of this
+// dimension was done; on large grids the last few of them are single long
+// chains that leave the GPU idle for milliseconds.  Instead the host waits
+// (after the sweep, which leaves only CTA-tier columns) until at most
+// kGateLeft pool columns are unfinished, then goes on.  A column of the next
+// dimension reduced before its row is cleared is a positive column: it
+// reduces to zero, or any row it claims is taken back by the smaller column
+// whose reduced lowest row it is (the pivots of a reduced matrix are unique),
+// so the pairs do not change; only that column's work is wasted, and at most
+// kGateLeft rows can be cleared late.  Progress comes from the CTA tier's
+// mirror in mapped host memory (a lower bound); the wait also ends when every
+// side stream is idle, or after kGateMaxMs.
+constexpr int64_t kGateMinCols = int64_t(1) << 17;
+constexpr int kGateLeft = 16;
+constexpr double kGateMaxMs = 30000.0;
+
+int dimension_gate(sspp_ctx* ctx) {
+    cudaStream_t s = ctx->stream;
+    CK(cudaMemcpyAsync(ctx->h_tail, ctx->D.pool_tail, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaEventRecord(ctx->gate_ev, s));
+    CK(cudaEventSynchronize(ctx->gate_ev));
+    const int tail = *ctx->h_tail;
+    const auto t0 = std::chrono::steady_clock::now();
+    for (int it = 1;; it++) {
+        const int done = *reinterpret_cast<volatile int*>(ctx->h_gate);
+        if (tail - done <= kGateLeft) break;
+        if ((it & 63) == 0) {
+            bool idle = true;
+            for (int q = 0; q < sspp_ctx::kSide && idle; q++) idle = cudaStreamQuery(ctx->side[q]) != cudaErrorNotReady;
+            if (idle) break;
+            if (std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count() > kGateMaxMs)
+                break;
+        }
+    }
+    return SSPP_OK;
+}
+
 int run_steps(sspp_ctx* ctx, const std::vector<Step>& steps, int cap1, int cap2, int ht) {
     Device& D = ctx->D;
     cudaStream_t s = ctx->stream;
@@ -481,8 +525,15 @@ int run_steps(sspp_ctx* ctx, const std::vector<Step>& steps, int cap1, int cap2,
     // they overlap the following light steps and each other, so long chains of
     // different steps run concurrently.  Each dimension's completion sweep, and
     // the next dimension, wait for all of them (twist clearing needs the
-    // finished dimension).
+    // finished dimension) -- on large inputs only until few of them are left
+    // (the dimension gate below).
     const bool overlap = true;
+    const bool gate = D.n >= kGateMinCols && ctx->h_gate;
+    D.gate_host = gate ? ctx->d_gate : nullptr;
+    if (gate) {
+        *reinterpret_cast<volatile int*>(ctx->h_gate) = 0;  // no CTA-tier launch of this context is running
+        CK(cudaMemsetAsync(D.heavy_done, 0, sizeof(int), s));
+    }
     while (ctx->step_ev.size() < steps.size() + 1) {
         cudaEvent_t ev;
         CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
@@ -498,7 +549,7 @@ int run_steps(sspp_ctx* ctx, const std::vector<Step>& steps, int cap1, int cap2,
     for (size_t k = 0; k < steps.size(); k++) {
         const Step& st = steps[k];
         const bool last_of_dim = st.minrow == INT32_MIN;
-        if (overlap && last_of_dim) {  // join: everything heavy of this dimension is done
+        if (overlap && last_of_dim && !gate) {  // join: everything heavy of this dimension is done
             int rcj = join_sides();
             if (rcj) return rcj;
         }
@@ -511,7 +562,7 @@ int run_steps(sspp_ctx* ctx, const std::vector<Step>& steps, int cap1, int cap2,
         reduce_light_launch(D, D.active, st.beg, st.end, st.minrow, cap1, chunk, ctr, grid, s);
         span_end(ctx, PH_LIGHT, a);
         heavy_slice_mark(D, ctr, k + 1 < steps.size() ? ctr + 4 : nullptr, s);
-        if (overlap && !last_of_dim) {
+        if (overlap && (!last_of_dim || gate)) {
             cudaStream_t hs = ctx->side[k % sspp_ctx::kSide];
             CK(cudaEventRecord(ctx->step_ev[k], s));
             CK(cudaStreamWaitEvent(hs, ctx->step_ev[k], 0));
@@ -526,6 +577,10 @@ int run_steps(sspp_ctx* ctx, const std::vector<Step>& steps, int cap1, int cap2,
         ctx->light_launches++;
         ctx->heavy_launches++;
         ctx->launches += 3;
+        if (gate && last_of_dim && k + 1 < steps.size()) {
+            int rcg = dimension_gate(ctx);
+            if (rcg) return rcg;
+        }
     }
     if (overlap) {  // nothing may still run on a side stream past this point
         int rcj = join_sides();
@@ -734,6 +789,13 @@ sspp_ctx* sspp_create(const sspp_config* cfg) {
             cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
         }
     }
+    if (cudaHostAlloc(&ctx->h_gate, sizeof(int), cudaHostAllocMapped) != cudaSuccess ||
+        cudaHostGetDevicePointer(reinterpret_cast<void**>(&ctx->d_gate), ctx->h_gate, 0) != cudaSuccess ||
+        cudaMallocHost(&ctx->h_tail, sizeof(int)) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->gate_ev, cudaEventDisableTiming) != cudaSuccess) {
+        delete ctx;
+        return nullptr;
+    }
     if (cudaMallocHost(&ctx->h_err, sizeof(int)) != cudaSuccess ||
         cudaMallocHost(&ctx->h_counters, sizeof(long long) * CNT_NUM) != cudaSuccess ||
         cudaMallocHost(&ctx->h_info, sizeof(DimInfo)) != cudaSuccess ||
@@ -773,6 +835,9 @@ void sspp_destroy(sspp_ctx* ctx) {
     }
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     if (ctx->h_err) cudaFreeHost(ctx->h_err);
+    if (ctx->h_gate) cudaFreeHost(ctx->h_gate);
+    if (ctx->h_tail) cudaFreeHost(ctx->h_tail);
+    if (ctx->gate_ev) cudaEventDestroy(ctx->gate_ev);
     if (ctx->h_counters) cudaFreeHost(ctx->h_counters);
     if (ctx->h_info) cudaFreeHost(ctx->h_info);
     if (ctx->h_top) cudaFreeHost(ctx->h_top);

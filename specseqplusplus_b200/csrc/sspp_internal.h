@@ -124,6 +124,9 @@ struct Device {
     int32_t* heavy = nullptr;    // pool of columns handed to the CTA tier, appended step after step
     int64_t pool_cap = 0;
     int* pool_tail = nullptr;
+    int* heavy_done = nullptr;   // pool columns the CTA tier has finished (this run)
+    int* gate_host = nullptr;    // device view of a mapped host word that mirrors heavy_done
+                                 // (owned by the context; null: no mirror)
     int64_t cap_steps = 0;
     // pairs output (input indices)
     int64_t* death_of = nullptr;   // [n]

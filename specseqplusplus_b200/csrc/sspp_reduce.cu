@@ -63,6 +63,8 @@ struct ReduceArgs {
     int* ctr;             // per step: [0] chunk counter, [1] [2] heavy pool range, [3] heavy pull counter
     int32_t* heavy;       // heavy pool (columns handed to the CTA tier, appended in step order)
     int* pool_tail;
+    int* heavy_done;      // pool columns finished by the CTA tier
+    int* gate_host;       // mapped host mirror of heavy_done, or null
     int64_t pool_cap;
     int* err;
     long long* counters;
@@ -219,6 +221,12 @@ __device__ __forceinline__ int ld(const int32_t* p) {
     else return lds(p);
 }
 __device__ __forceinline__ int ldv(const int32_t* p, bool global) { return global ? __ldcg(p) : lds(p); }
+
+// A store the host sees without synchronising (mapped pinned memory); stores
+// of different CTAs may land out of order, so the host reads a lower bound.
+__device__ __forceinline__ void st_relaxed_sys(int* p, int v) {
+    asm volatile("st.relaxed.sys.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
 
 // calls F<ga, gb>(...) with the spaces known at compile time
 #define SSPP_DISPATCH2(ga, gb, CALL) \
@@ -507,6 +515,9 @@ __device__ bool publish(const G& g, const ReduceArgs& A, int col, Work& w) {
 
 enum Outcome { OUT_OWNER, OUT_ZERO, OUT_PARKED, OUT_DEFERRED, OUT_FAIL };
 
+// additions between two looks at a column's cleared flag
+constexpr int kClearCheck = 64;
+
 // Short addends in the CTA tier.  Along the long chains the CTA tier runs, the
 // working column holds hundreds to thousands of entries while the addends
 // (owners' versions) hold a handful, so rewriting the column for each addend
@@ -769,7 +780,25 @@ __device__ Outcome reduce_column(const G& g, const ReduceArgs& A, int col, int32
     }
     // speculative first staging round: header + as many entries as one pass of the group reads
     const int first4 = min(G::kSize, (kHdr + A.cap) >> 2);
+    int next_check = 0;
     for (int iter = 0;; iter++) {
+        if (iter >= next_check) {
+            // Cleared meanwhile: a column of the next higher dimension claimed this
+            // column's row, so the column is positive and zero once reduced (and a row
+            // never loses its owner, so it stays cleared).  It owns no row now (a claim
+            // ends the reduction), so it stops here as zero.
+            next_check = iter + kClearCheck;
+            int c = 0;
+            if (g.leader()) c = int(ld_acquire_u8(A.cleared + col));
+            if (g.bcast(c)) {
+                if (g.leader()) {
+                    A.desc[col] = pack_desc(0, 0);
+                    A.low[col] = -1;
+                }
+                res = OUT_ZERO;
+                break;
+            }
+        }
         if (w.len == 0) {
             if (g.leader()) {
                 A.desc[col] = pack_desc(0, 0);
@@ -831,7 +860,7 @@ __device__ Outcome reduce_column(const G& g, const ReduceArgs& A, int col, int32
         if constexpr (G::kSize > 32) {  // CTA tier: short addends by one warp
             if (!w.global) {
                 const int done = fast_adds(g, A, col, w, L, e, w.buf == sw0 ? sw1 : sw0, sp, adds, add_ints,
-                                           kMaxMergesPerColumn - iter);
+                                           min(kClearCheck, kMaxMergesPerColumn - iter));
                 if (done < 0) break;
                 if (done > 0) {
                     iter += done;
@@ -1060,6 +1089,10 @@ __global__ void __launch_bounds__(T, 1) k_reduce_heavy(ReduceArgs A) {
             if (!settle(g, A, col, o)) return;
             col = next;
         }
+        if (g.leader() && A.heavy_done) {  // progress for the host's dimension gate
+            const int v = atomicAdd(A.heavy_done, 1) + 1;
+            if (A.gate_host) st_relaxed_sys(A.gate_host, v);
+        }
     }
 }
 
@@ -1094,6 +1127,8 @@ static ReduceArgs make_args(const Device& D, const int32_t* active, int32_t beg,
     A.ctr = ctr;
     A.heavy = D.heavy;
     A.pool_tail = D.pool_tail;
+    A.heavy_done = D.heavy_done;
+    A.gate_host = D.gate_host;
     A.pool_cap = D.pool_cap;
     A.err = D.err;
     A.counters = D.counters;
