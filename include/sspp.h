@@ -64,6 +64,9 @@ typedef struct sspp_params {
     int32_t level2_capacity;  /* per-block on-chip column capacity (ints)             */
     int32_t autotune;         /* 0 off, 1 launch parameters, 2 also dualization     */
     int32_t heavy_threads;    /* threads per heavy-tier column: 128 or 256 (0 = 256)  */
+    int32_t representatives;  /* 1: keep whole reduced columns so that sspp_representative
+                                 can return each pair's cycle (dualize 0 only; skips the
+                                 negative-row compression, so the reduction does more work) */
 } sspp_params;
 
 /* Per-run counters (device-side counters plus host timings). */
@@ -228,6 +231,17 @@ int32_t sspp_export_preprocessed(sspp_ctx* ctx, const sspp_params* p, const char
 
 /* Replaces: writeVectorToFile (src/main.cu:191-229). */
 int32_t sspp_write_pairs(sspp_ctx* ctx, const char* path, int32_t fmt);
+
+/* No counterpart in the reference (PHAT's python binding returns pairs only).
+ * A representative cycle of the pair whose death is `death` (an input index),
+ * after a reduction with representatives = 1 and dualize = 0: the simplices of
+ * the death column's reduced column, as input indices, ascending.  Over Z2 it
+ * is the boundary of a chain whose youngest simplex is `death`, so it is a
+ * cycle, and its youngest simplex is the pair's birth.  With edge collapse it
+ * lies in the collapsed complex.  Copies up to cap entries to out and returns
+ * the cycle's length, or -1 (sspp_last_error) when `death` kills no class, the
+ * reduction kept no representatives, or the context holds a batch. */
+int64_t sspp_representative(sspp_ctx* ctx, int64_t death, int64_t* out, int64_t cap);
 
 int32_t sspp_get_stats(const sspp_ctx* ctx, sspp_stats* out);
 /* The parameters the last sspp_init ran with (autotuned values included). */

@@ -114,6 +114,8 @@ struct sspp_ctx {
     std::vector<int64_t> host_pairs;
     bool host_pairs_valid = false;
     std::vector<int64_t> host_ess;     // essentials, copied back once for slicing
+    std::vector<int32_t> host_perm;    // reordered -> input index, copied back for representatives
+    bool host_perm_valid = false;
     std::vector<int64_t> batch_bounds; // per-complex pair and essential slice starts
     bool host_ess_valid = false;
     int64_t launches = 0, light_launches = 0, heavy_launches = 0;
@@ -271,8 +273,15 @@ int check_params(sspp_ctx* ctx, const sspp_params* p) {
     if (p->level1_capacity < 0 || p->level2_capacity < 0)
         return set_err(ctx, SSPP_ERR_BAD_INPUT, "level capacities must be >= 0");
     if (p->autotune < 0 || p->autotune > 2) return set_err(ctx, SSPP_ERR_BAD_INPUT, "autotune must be 0, 1 or 2");
+    if (p->representatives < 0 || p->representatives > 1)
+        return set_err(ctx, SSPP_ERR_BAD_INPUT, "representatives must be 0 or 1");
+    if (p->representatives && p->dualize)
+        return set_err(ctx, SSPP_ERR_BAD_INPUT, "representatives need dualize 0 (the dual reduces cocycles)");
     return SSPP_OK;
 }
+
+// autotune 2 may switch to dualization mode 2, which representative cycles rule out
+bool tune_allows_dual(const sspp_params& u) { return u.autotune == 2 && !u.representatives; }
 
 // Shared-memory capacities (ints) of the two tiers: a warp holds three
 // buffers of level1 ints, a CTA three of level2 ints.
@@ -378,7 +387,7 @@ int autotune_choose(sspp_ctx* ctx) {
     ctx->tune_shape = top * 4 + std::min(3, int(frac * 4.0));
     const sspp_params& u = ctx->user_params;
     Knobs k;
-    ctx->tune_cand = tune_choose(D.n, ctx->tune_shape, u.model, u.dualize, u.autotune == 2, &k);
+    ctx->tune_cand = tune_choose(D.n, ctx->tune_shape, u.model, u.dualize, tune_allows_dual(u), &k);
     sspp_params& q = ctx->params;
     q.ss_block_size = k.ss_block_size;
     q.growth = k.growth;
@@ -431,7 +440,7 @@ int run_init(sspp_ctx* ctx) {
         int rc2 = run_highclear(ctx);
         if (rc2) return rc2;
     }
-    ctx->launches += init_compress(D, dropped_of(ctx), s);
+    ctx->launches += init_compress(D, dropped_of(ctx), ctx->params.representatives != 0, s);
     if (ctx->params.dualize == 1) ctx->launches += dualize(D, 1, s);
     ctx->launches += build_apparent(D, s);
     ctx->launches += active_list(D, s);
@@ -594,6 +603,7 @@ int run_compute(sspp_ctx* ctx) {
     ctx->err.clear();
     ctx->host_pairs_valid = false;
     ctx->host_ess_valid = false;
+    ctx->host_perm_valid = false;
     Device& D = ctx->D;
     cudaStream_t s = ctx->stream;
     auto t0 = std::chrono::steady_clock::now();
@@ -755,6 +765,7 @@ extern "C" {
 void sspp_default_params(sspp_params* p) {
     if (!p) return;
     p->dualize = 0;
+    p->representatives = 0;
     p->model = 0;
     p->max_iteration = 0;
     p->ss_block_size = 102400;
@@ -1212,7 +1223,7 @@ int32_t sspp_compute(sspp_ctx* ctx, void* stream) {
         if (rc == SSPP_OK && ctx->tune_cand >= 0) {
             const sspp_params& u = ctx->user_params;
             const double base = double(ctx->D.nnz + (kHdr + 3) * ctx->D.n + 4);
-            tune_record(ctx->D.n, ctx->tune_shape, u.model, u.dualize, u.autotune == 2, ctx->tune_cand,
+            tune_record(ctx->D.n, ctx->tune_shape, u.model, u.dualize, tune_allows_dual(u), ctx->tune_cand,
                         ctx->init_ms + ctx->compute_ms, double(ctx->arena_used) / base);
         }
         if (rc != SSPP_ERR_CAPACITY || !ctx->err.empty()) return rc;
@@ -1350,6 +1361,57 @@ int32_t sspp_get_params(const sspp_ctx* ctx, sspp_params* out) {
     if (!ctx || !out) return SSPP_ERR_BAD_INPUT;
     *out = ctx->params;
     return SSPP_OK;
+}
+
+int64_t sspp_representative(sspp_ctx* ctx, int64_t death, int64_t* out, int64_t cap) {
+    if (!ctx) return -1;
+    cudaSetDevice(ctx->cfg.device);
+    auto fail = [&](int code, const char* msg) -> int64_t {
+        set_err(ctx, code, msg);
+        return -1;
+    };
+    if (!ctx->computed) return fail(SSPP_ERR_STATE, "no completed reduction");
+    if (!ctx->params.representatives) return fail(SSPP_ERR_STATE, "the reduction ran without representatives = 1");
+    if (!ctx->batch_start.empty()) return fail(SSPP_ERR_STATE, "representatives are not kept for batches");
+    const Device& D = ctx->D;
+    if (death < 0 || death >= D.n) return fail(SSPP_ERR_BAD_INPUT, "death index out of range");
+    if (cap > 0 && !out) return fail(SSPP_ERR_BAD_INPUT, "null output");
+    cudaStream_t s = ctx->stream;
+    // the death's reordered column, its descriptor, and the owner of its lowest row
+    int32_t c = 0;
+    uint64_t d = 0;
+    if (cudaMemcpyAsync(&c, D.newidx + death, sizeof(int32_t), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess || c < 0 || c >= D.n ||
+        cudaMemcpyAsync(&d, D.desc + c, sizeof(uint64_t), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return fail(SSPP_ERR_CUDA, "reading the death column failed");
+    const uint32_t len = desc_len(d);
+    if (len == 0) return fail(SSPP_ERR_BAD_INPUT, "not a death: the column reduced to zero");
+    std::vector<int32_t> rows(len);
+    uint64_t e = 0;
+    if (cudaMemcpyAsync(rows.data(), D.arena + desc_off(d) + kHdr, sizeof(int32_t) * len, cudaMemcpyDeviceToHost, s) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess || rows.back() < 0 || rows.back() >= D.n ||
+        cudaMemcpyAsync(&e, D.pivot + rows.back(), sizeof(uint64_t), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return fail(SSPP_ERR_CUDA, "reading the reduced column failed");
+    if (e == kNoOwner || pv_col(e) != c) return fail(SSPP_ERR_BAD_INPUT, "not a death: the column owns no row");
+    if (!ctx->host_perm_valid) {
+        ctx->host_perm.resize(size_t(D.n));
+        if (cudaMemcpyAsync(ctx->host_perm.data(), D.perm, sizeof(int32_t) * size_t(D.n), cudaMemcpyDeviceToHost, s) !=
+                cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess)
+            return fail(SSPP_ERR_CUDA, "reading the index map failed");
+        ctx->host_perm_valid = true;
+    }
+    std::vector<int64_t> cyc(len);
+    for (uint32_t k = 0; k < len; k++) {
+        if (rows[k] < 0 || rows[k] >= D.n) return fail(SSPP_ERR_BAD_INPUT, "row index out of range");
+        cyc[k] = ctx->host_perm[size_t(rows[k])];
+    }
+    std::sort(cyc.begin(), cyc.end());
+    for (int64_t k = 0; k < std::min<int64_t>(cap, len); k++) out[k] = cyc[size_t(k)];
+    return int64_t(len);
 }
 
 int32_t sspp_get_stats(const sspp_ctx* ctx, sspp_stats* o) {

@@ -350,7 +350,7 @@ __global__ void k_init_apparent(int64_t n, const int32_t* arena, const uint64_t*
 // Clears positive columns and removes negative rows in place.
 __global__ void k_init_compress(int64_t n, int32_t* arena, uint64_t* desc, int32_t* low, const uint64_t* pivot,
                                 const uint8_t* cleared, const uint8_t* negative, uint8_t* state,
-                                const uint8_t* dropped, long long* counters, int* err) {
+                                const uint8_t* dropped, bool keep_rows, long long* counters, int* err) {
     long long ncl = 0, nact = 0;
     for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
         uint64_t d = desc[i];
@@ -374,9 +374,13 @@ __global__ void k_init_compress(int64_t n, int32_t* arena, uint64_t* desc, int32
             continue;
         }
         uint32_t m = 0;
-        for (uint32_t k = 0; k < len; k++) {
-            int32_t r = c[k];
-            if (!negative[r]) c[m++] = r;
+        if (keep_rows) {
+            m = len;
+        } else {
+            for (uint32_t k = 0; k < len; k++) {
+                int32_t r = c[k];
+                if (!negative[r]) c[m++] = r;
+            }
         }
         for (uint32_t k = m; k < len; k++) c[k] = INT_MAX;
         desc[i] = pack_desc(desc_off(d), m);
@@ -431,11 +435,11 @@ int init_passes(Device& D, cudaStream_t s) {
     return 2;
 }
 
-int init_compress(Device& D, const uint8_t* dropped, cudaStream_t s) {
+int init_compress(Device& D, const uint8_t* dropped, bool keep_rows, cudaStream_t s) {
     const int64_t n = D.n;
     const unsigned g = grid_for(n, 256) > 65536 ? 65536 : grid_for(n, 256);
     k_init_compress<<<g, 256, 0, s>>>(n, D.arena, D.desc, D.low, D.pivot, D.cleared, D.negative, D.state, dropped,
-                                      D.counters, D.err);
+                                      keep_rows, D.counters, D.err);
     return 1;
 }
 

@@ -30,7 +30,9 @@ int batch_localize(int64_t npairs, int64_t ness, int32_t k, const int64_t* d_cst
                    const int64_t* ess, int64_t* lpairs, int64_t* less, cudaStream_t s);
 
 int init_passes(Device& D, cudaStream_t s);
-int init_compress(Device& D, const uint8_t* dropped, cudaStream_t s);
+// keep_rows: leave negative rows in the columns (whole reduced columns, for
+// representative cycles); otherwise they are removed.
+int init_compress(Device& D, const uint8_t* dropped, bool keep_rows, cudaStream_t s);
 int active_list(Device& D, cudaStream_t s);
 // D.app from the pivot table as it stands (apparent pairs only)
 int build_apparent(Device& D, cudaStream_t s);

@@ -38,7 +38,7 @@ class _Params(ctypes.Structure):
     _fields_ = [("dualize", ctypes.c_int32), ("model", ctypes.c_int32), ("max_iteration", ctypes.c_int32),
                 ("ss_block_size", ctypes.c_int32), ("growth", ctypes.c_float), ("queue_size", ctypes.c_int32),
                 ("level1_capacity", ctypes.c_int32), ("level2_capacity", ctypes.c_int32),
-                ("autotune", ctypes.c_int32), ("heavy_threads", ctypes.c_int32)]
+                ("autotune", ctypes.c_int32), ("heavy_threads", ctypes.c_int32), ("representatives", ctypes.c_int32)]
 
 
 class _Stats(ctypes.Structure):
@@ -78,6 +78,7 @@ class Params:
     level2_capacity: int = 8000
     autotune: int = 0
     heavy_threads: int = 0
+    representatives: int = 0
 
     def _c(self) -> _Params:
         return _Params(*(getattr(self, f.name) for f in fields(self)))
@@ -107,6 +108,7 @@ def load_library():
         "sspp_load_lowerstar": (i32, [vp, i64, i64, i64, vp, i32]),
         "sspp_input_size": (i32, [vp, vp, vp]),
         "sspp_input_copy": (i32, [vp, vp, vp, vp, vp]),
+        "sspp_representative": (i64, [vp, i64, vp, i64]),
         "sspp_init": (i32, [vp, ctypes.POINTER(_Params), vp]),
         "sspp_compute": (i32, [vp, vp]),
         "sspp_reduce": (i32, [vp, ctypes.POINTER(_Params), vp]),
@@ -169,7 +171,7 @@ EXPORTED = ("sspp_create", "sspp_destroy", "sspp_last_error", "sspp_default_para
             "sspp_server_release", "sspp_server_get_stats", "sspp_server_reset_stats", "sspp_phat_read",
             "sspp_phat_ncols", "sspp_phat_nnz", "sspp_phat_copy", "sspp_phat_free", "sspp_phat_write",
             "sspp_export_preprocessed", "sspp_load_rips", "sspp_load_lowerstar", "sspp_input_size",
-            "sspp_input_copy")
+            "sspp_input_copy", "sspp_representative")
 
 
 class Engine:
@@ -243,6 +245,16 @@ class Engine:
         self._check(self._lib.sspp_load_lowerstar(self._h, gx, gy, gz, ptr, int(maxdim)))
         del keep
         self._batch_k = 0
+
+    def representative(self, death: int) -> np.ndarray:
+        """Representative cycle (input indices, ascending) of the pair whose death is ``death``;
+        needs a reduction with ``Params(representatives=1)`` (dualize 0)."""
+        n = self._lib.sspp_representative(self._h, int(death), None, 0)
+        if n < 0:
+            raise SsppError(ERR_BAD_INPUT, self._lib.sspp_last_error(self._h).decode(errors="replace"))
+        out = np.empty(max(n, 1), dtype=np.int64)
+        self._lib.sspp_representative(self._h, int(death), out.ctypes.data, n)
+        return out[:n]
 
     def input_matrix(self, values: bool = False):
         """The loaded matrix copied back (with its filtration values for a built complex)."""
