@@ -361,7 +361,62 @@ def leg_served(count=48, rates=(100.0, None)):
                              "plain_cols_per_s": cp, "plain_p50_ms": float(lp[0]), "plain_p95_ms": float(lp[1]),
                              "plain_p99_ms": float(lp[2]), "speedup_vs_plain": st["cols_per_s"] / cp,
                              "results_equal_plain": bool(same)})
+    out["built"] = served_built(stream, N, plain_results)
     return out
+
+
+def served_built(stream, N, want):
+    """The same requests given as point clouds and fields (the complexes are built on the device), all at
+    once: the server against a serial one-at-a-time loop of device build + reduction."""
+    from specseqplusplus_b200 import Engine, Params, Server, gen
+
+    inputs = []
+    for _, kind, _, d in stream:
+        if kind == "rips":
+            inputs.append(("r", gen.points(d["npts"], d["space_dim"], d["seed"]), d["radius"],
+                           2 if d["space_dim"] == 2 else 3))
+        else:
+            inputs.append(("l", gen.field(d["grid"], d["sigma"], d["seed"]), None, 3))
+
+    def load(e, x):
+        if x[0] == "r":
+            e.load_rips(x[1], x[2], x[3])
+        else:
+            e.load_lowerstar(x[1], x[3])
+
+    with Engine(0) as e:
+        for x in inputs[:8]:
+            load(e, x)
+            e.reduce(Params())
+        lat, res = [], []
+        t0 = time.perf_counter()
+        for x in inputs:
+            load(e, x)
+            e.reduce(Params())
+            res.append((e.pairs(), e.essentials()))
+            lat.append(1000 * (time.perf_counter() - t0))
+        plain = N / (time.perf_counter() - t0)
+    with Server(Params(autotune=2), workers=2) as srv:
+        for _ in range(2):
+            ids = [srv.submit_rips(x[1], x[2], x[3], copy=False) if x[0] == "r" else
+                   srv.submit_lowerstar(x[1], x[3], copy=False) for x in inputs[:16]]
+            for i in ids:
+                srv.wait(i)
+                srv.release(i)
+        srv.reset_stats()
+        ids = [srv.submit_rips(x[1], x[2], x[3], copy=False) if x[0] == "r" else
+               srv.submit_lowerstar(x[1], x[3], copy=False) for x in inputs]
+        for i in ids:
+            srv.wait(i)
+        st = srv.stats()
+        same = all(np.array_equal(srv.pairs(i), w[0]) and np.array_equal(srv.essentials(i), w[1])
+                   for i, w in zip(ids, want))
+    same = same and all(np.array_equal(r[0], w[0]) and np.array_equal(r[1], w[1]) for r, w in zip(res, want))
+    lp = np.percentile(lat, [50, 99])
+    return {"workload": "the same requests as point clouds and fields, all at once; complexes built on the device",
+            "served_cols_per_s": st["cols_per_s"], "served_p50_ms": st["p50_ms"], "served_p99_ms": st["p99_ms"],
+            "plain_cols_per_s": plain, "plain_p50_ms": float(lp[0]), "plain_p99_ms": float(lp[1]),
+            "speedup_vs_plain": st["cols_per_s"] / plain, "results_equal_boundary_matrix_path": bool(same)}
 
 
 def oracle_module():

@@ -291,6 +291,9 @@ typedef struct sspp_server_stats {
 /* submit flag: the caller keeps dims / col_ptr / rows valid and unmodified
  * until the request is done (no copy at submission) */
 #define SSPP_SUBMIT_NOCOPY 1
+/* submit flag (point clouds and fields): keep the built matrix's filtration
+ * values for sspp_server_values */
+#define SSPP_SUBMIT_VALUES 2
 
 /* params: as for sspp_init (autotune applies per batch). */
 sspp_server* sspp_server_create(const sspp_server_config* cfg, const sspp_params* params);
@@ -300,6 +303,21 @@ const char* sspp_server_last_error(sspp_server* srv);
 /* Returns the request id (>= 0), or -SSPP_ERR_* when refused. */
 int64_t sspp_server_submit(sspp_server* srv, int64_t ncols, const int32_t* dims, const int64_t* col_ptr,
                            const int32_t* rows, int32_t flags);
+/* A request given as a point cloud or a scalar field (as sspp_load_rips /
+ * sspp_load_lowerstar): the worker builds the complex on the device and
+ * reduces it alone (not batched with others); its pairs and essentials are
+ * indices of the built matrix, whose column values sspp_server_values returns
+ * when submitted with SSPP_SUBMIT_VALUES.  A field's request is admitted by an
+ * upper bound of its size (26 columns and 74 entries per vertex); a point
+ * cloud's size is known only once built, and one that does not fit the
+ * device fails with SSPP_ERR_CAPACITY.  The reference builds such complexes
+ * with external tools (phat-highclear/addons/rips.cpp) and serves nothing. */
+int64_t sspp_server_submit_rips(sspp_server* srv, int64_t npts, int32_t space_dim, const float* points, float radius,
+                                int32_t maxdim, int32_t flags);
+int64_t sspp_server_submit_lowerstar(sspp_server* srv, int64_t gx, int64_t gy, int64_t gz, const float* values,
+                                     int32_t maxdim, int32_t flags);
+/* Copies up to cap values and returns the built matrix's column count, or -1. */
+int64_t sspp_server_values(sspp_server* srv, int64_t id, float* out, int64_t cap);
 /* SSPP_OK once the request is done or failed, SSPP_ERR_TIMEOUT if timeout_ms
  * passed first (timeout_ms < 0 waits for ever), SSPP_ERR_STATE for an unknown id. */
 int32_t sspp_server_wait(sspp_server* srv, int64_t id, double timeout_ms);

@@ -32,9 +32,20 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 
+enum Kind { KIND_MATRIX = 0, KIND_RIPS = 1, KIND_LOWERSTAR = 2 };
+
 struct Request {
     int64_t id = 0;
-    int64_t ncols = 0, nnz = 0;
+    int64_t ncols = 0, nnz = 0;       // built requests: estimates until built
+    int kind = KIND_MATRIX;
+    // built requests: the point cloud or field, and the builder's arguments
+    std::vector<float> fin_copy;
+    const float* fin = nullptr;
+    int64_t g[3] = {0, 0, 0};        // Rips: points, space dimension; lower-star: grid sizes
+    float radius = 0.0f;
+    int32_t maxdim = 3;
+    bool want_values = false;
+    std::unique_ptr<float[]> values;  // the built matrix's filtration values, if asked for
     std::vector<int32_t> dims_copy;
     std::vector<int64_t> colptr_copy;
     std::vector<int32_t> rows_copy;
@@ -82,6 +93,10 @@ struct sspp_server {
 };
 
 namespace {
+
+int64_t reject(sspp_server* S, const char* why);
+void take_floats(Request* r, const float* p, int64_t n, int32_t flags);
+int64_t enqueue(sspp_server* S, std::unique_ptr<Request> r);
 
 // device bytes one request adds to a batch
 double estimate(const sspp_params& p, int64_t ncols, int64_t nnz) {
@@ -143,6 +158,41 @@ int32_t try_batch(sspp_ctx* ctx, const sspp_params& params, const std::vector<Re
     return rc;
 }
 
+// A request given as a point cloud or a field: built on the device, reduced
+// alone; pairs are indices of the built matrix.
+int32_t try_built(sspp_ctx* ctx, const sspp_params& params, Request* r, Phases& ph) {
+    if (!ctx) {
+        set_result(r, SSPP_ERR_CUDA, "no usable CUDA device");
+        return SSPP_ERR_CUDA;
+    }
+    const Clock::time_point t0 = Clock::now();
+    int32_t rc = r->kind == KIND_RIPS
+                     ? sspp_load_rips(ctx, r->g[0], int32_t(r->g[1]), r->fin, r->radius, r->maxdim)
+                     : sspp_load_lowerstar(ctx, r->g[0], r->g[1], r->g[2], r->fin, r->maxdim);
+    const Clock::time_point t1 = Clock::now();
+    if (rc == SSPP_OK) rc = sspp_reduce(ctx, &params, nullptr);
+    const Clock::time_point t2 = Clock::now();
+    ph.load += ms_between(t0, t1) / 1000.0;
+    ph.reduce += ms_between(t1, t2) / 1000.0;
+    if (rc == SSPP_OK) rc = sspp_input_size(ctx, &r->ncols, &r->nnz);
+    if (rc == SSPP_OK) {
+        r->npairs = sspp_num_pairs(ctx);
+        r->ness = sspp_num_essential(ctx);
+        r->pairs.reset(new int64_t[size_t(std::max<int64_t>(2 * r->npairs, 1))]);
+        r->ess.reset(new int64_t[size_t(std::max<int64_t>(r->ness, 1))]);
+        if (r->npairs < 0 || r->ness < 0 || sspp_pairs(ctx, r->pairs.get(), r->npairs) != r->npairs ||
+            sspp_essentials(ctx, r->ess.get(), r->ness) != r->ness)
+            rc = SSPP_ERR_CUDA;
+    }
+    if (rc == SSPP_OK && r->want_values) {
+        r->values.reset(new float[size_t(std::max<int64_t>(r->ncols, 1))]);
+        rc = sspp_input_copy(ctx, nullptr, nullptr, nullptr, r->values.get());
+    }
+    ph.results += ms_between(t2, Clock::now()) / 1000.0;
+    set_result(r, rc, rc == SSPP_OK ? nullptr : sspp_last_error(ctx));
+    return rc;
+}
+
 void worker_main(sspp_server* S, int host_threads) {
     sspp_config c;
     std::memset(&c, 0, sizeof(c));
@@ -170,7 +220,9 @@ void worker_main(sspp_server* S, int host_threads) {
             int64_t cols = 0;
             while (!S->queue.empty()) {
                 Request* r = S->queue.front();
-                if (!batch.empty() && (est + r->est > S->share || cols + r->ncols > max_cols ||
+                // built requests run alone
+                if (!batch.empty() && (r->kind != KIND_MATRIX || batch[0]->kind != KIND_MATRIX ||
+                                       est + r->est > S->share || cols + r->ncols > max_cols ||
                                        batch.size() >= max_req || cols >= fair))
                     break;
                 S->queue.pop_front();
@@ -182,9 +234,13 @@ void worker_main(sspp_server* S, int host_threads) {
             }
         }
         Phases ph;
-        int32_t rc = try_batch(ctx, S->params, batch, ph);
-        if (rc != SSPP_OK && batch.size() > 1)  // isolate the request that failed
-            for (Request* r : batch) try_batch(ctx, S->params, {r}, ph);
+        if (batch[0]->kind != KIND_MATRIX) {
+            try_built(ctx, S->params, batch[0], ph);
+        } else {
+            int32_t rc = try_batch(ctx, S->params, batch, ph);
+            if (rc != SSPP_OK && batch.size() > 1)  // isolate the request that failed
+                for (Request* r : batch) try_batch(ctx, S->params, {r}, ph);
+        }
         {
             std::lock_guard<std::mutex> l(S->mu);
             S->phases.load += ph.load;
@@ -205,6 +261,8 @@ void worker_main(sspp_server* S, int host_threads) {
                 std::vector<int32_t>().swap(r->dims_copy);
                 std::vector<int64_t>().swap(r->colptr_copy);
                 std::vector<int32_t>().swap(r->rows_copy);
+                std::vector<float>().swap(r->fin_copy);
+                r->fin = nullptr;
                 r->dims = nullptr;
                 r->colptr = nullptr;
                 r->rows = nullptr;
@@ -303,6 +361,83 @@ int64_t sspp_server_submit(sspp_server* S, int64_t ncols, const int32_t* dims, c
         r->rows = r->rows_copy.data();
     }
     r->est = estimate(S->params, ncols, r->nnz);
+    return enqueue(S, std::move(r));
+}
+
+int64_t sspp_server_submit_rips(sspp_server* S, int64_t npts, int32_t space_dim, const float* points, float radius,
+                                int32_t maxdim, int32_t flags) {
+    if (!S) return -SSPP_ERR_BAD_INPUT;
+    if (npts < 0 || (npts > 0 && !points) || space_dim < 1 || space_dim > 3 || !(radius >= 0.0f) ||
+        !std::isfinite(radius) || maxdim < 0 || maxdim > 3)
+        return reject(S, "bad point cloud request");
+    auto r = std::make_unique<Request>();
+    r->kind = KIND_RIPS;
+    r->g[0] = npts;
+    r->g[1] = space_dim;
+    r->radius = radius;
+    r->maxdim = maxdim;
+    r->want_values = (flags & SSPP_SUBMIT_VALUES) != 0;
+    take_floats(r.get(), points, npts * space_dim, flags);
+    // the size is known once built; the queue counts 16 columns per point
+    r->ncols = 16 * npts;
+    r->nnz = 40 * npts;
+    r->est = 0;
+    return enqueue(S, std::move(r));
+}
+
+int64_t sspp_server_submit_lowerstar(sspp_server* S, int64_t gx, int64_t gy, int64_t gz, const float* values,
+                                     int32_t maxdim, int32_t flags) {
+    if (!S) return -SSPP_ERR_BAD_INPUT;
+    if (gx < 1 || gy < 1 || gz < 1 || !values || gx > INT32_MAX || gy > INT32_MAX || gz > INT32_MAX ||
+        gx * gy > INT32_MAX || gx * gy * gz > INT32_MAX || maxdim < 0 || maxdim > 3)
+        return reject(S, "bad field request");
+    auto r = std::make_unique<Request>();
+    r->kind = KIND_LOWERSTAR;
+    r->g[0] = gx;
+    r->g[1] = gy;
+    r->g[2] = gz;
+    r->maxdim = maxdim;
+    r->want_values = (flags & SSPP_SUBMIT_VALUES) != 0;
+    const int64_t nv = gx * gy * gz;
+    take_floats(r.get(), values, nv, flags);
+    // at most 7 edges, 12 triangles and 6 tetrahedra start at each vertex
+    r->ncols = 26 * nv;
+    r->nnz = 74 * nv;
+    r->est = estimate(S->params, r->ncols, r->nnz);
+    return enqueue(S, std::move(r));
+}
+
+int64_t sspp_server_values(sspp_server* S, int64_t id, float* out, int64_t cap) {
+    if (!S || cap < 0 || (!out && cap > 0)) return -1;
+    std::lock_guard<std::mutex> l(S->mu);
+    Request* r = find(S, id);
+    if (!r || r->state != SSPP_REQ_DONE || !r->values) return -1;
+    const int64_t n = std::min<int64_t>(cap, r->ncols);
+    if (n > 0) std::memcpy(out, r->values.get(), sizeof(float) * size_t(n));
+    return r->ncols;
+}
+
+}  // extern "C"
+
+namespace {
+
+int64_t reject(sspp_server* S, const char* why) {
+    std::lock_guard<std::mutex> l(S->mu);
+    S->err = why;
+    S->rejected++;
+    return -SSPP_ERR_BAD_INPUT;
+}
+
+void take_floats(Request* r, const float* p, int64_t n, int32_t flags) {
+    if (flags & SSPP_SUBMIT_NOCOPY) {
+        r->fin = p;
+    } else {
+        r->fin_copy.assign(p, p + n);
+        r->fin = r->fin_copy.data();
+    }
+}
+
+int64_t enqueue(sspp_server* S, std::unique_ptr<Request> r) {
     std::lock_guard<std::mutex> l(S->mu);
     if (r->est > S->budget) {
         S->err = "request larger than the device-memory budget";
@@ -323,6 +458,10 @@ int64_t sspp_server_submit(sspp_server* S, int64_t ncols, const int32_t* dims, c
     S->cv_work.notify_one();
     return id;
 }
+
+}  // namespace
+
+extern "C" {
 
 int32_t sspp_server_wait(sspp_server* S, int64_t id, double timeout_ms) {
     if (!S) return SSPP_ERR_BAD_INPUT;

@@ -109,6 +109,9 @@ def load_library():
         "sspp_input_size": (i32, [vp, vp, vp]),
         "sspp_input_copy": (i32, [vp, vp, vp, vp, vp]),
         "sspp_representative": (i64, [vp, i64, vp, i64]),
+        "sspp_server_submit_rips": (i64, [vp, i64, i32, vp, ctypes.c_float, i32, i32]),
+        "sspp_server_submit_lowerstar": (i64, [vp, i64, i64, i64, vp, i32, i32]),
+        "sspp_server_values": (i64, [vp, i64, vp, i64]),
         "sspp_init": (i32, [vp, ctypes.POINTER(_Params), vp]),
         "sspp_compute": (i32, [vp, vp]),
         "sspp_reduce": (i32, [vp, ctypes.POINTER(_Params), vp]),
@@ -171,7 +174,8 @@ EXPORTED = ("sspp_create", "sspp_destroy", "sspp_last_error", "sspp_default_para
             "sspp_server_release", "sspp_server_get_stats", "sspp_server_reset_stats", "sspp_phat_read",
             "sspp_phat_ncols", "sspp_phat_nnz", "sspp_phat_copy", "sspp_phat_free", "sspp_phat_write",
             "sspp_export_preprocessed", "sspp_load_rips", "sspp_load_lowerstar", "sspp_input_size",
-            "sspp_input_copy", "sspp_representative")
+            "sspp_input_copy", "sspp_representative", "sspp_server_submit_rips", "sspp_server_submit_lowerstar",
+            "sspp_server_values")
 
 
 class Engine:
@@ -489,6 +493,40 @@ class Server:
         if not copy:
             self._keep[rid] = (dims, col_ptr, rows)
         return int(rid)
+
+    def _submitted(self, rid: int, keep) -> int:
+        if rid < 0:
+            raise SsppError(-rid, self._lib.sspp_server_last_error(self._h).decode(errors="replace"))
+        if keep is not None:
+            self._keep[rid] = keep
+        return int(rid)
+
+    def submit_rips(self, points, radius: float, maxdim: int = 3, values: bool = False, copy: bool = True) -> int:
+        """A point cloud [npts, D] (float32) whose Rips complex the server builds and reduces."""
+        pts = np.ascontiguousarray(points, dtype=np.float32)
+        flags = (0 if copy else 1) | (2 if values else 0)
+        rid = self._lib.sspp_server_submit_rips(self._h, pts.shape[0], pts.shape[1], pts.ctypes.data if pts.size else None,
+                                                float(radius), int(maxdim), flags)
+        return self._submitted(rid, None if copy else pts)
+
+    def submit_lowerstar(self, field, maxdim: int = 3, values: bool = False, copy: bool = True) -> int:
+        """A field [gz, gy, gx] (float32, x fastest) whose Freudenthal lower-star filtration the server builds
+        and reduces."""
+        f = np.ascontiguousarray(field, dtype=np.float32)
+        gz, gy, gx = f.shape
+        flags = (0 if copy else 1) | (2 if values else 0)
+        rid = self._lib.sspp_server_submit_lowerstar(self._h, gx, gy, gz, f.ctypes.data, int(maxdim), flags)
+        return self._submitted(rid, None if copy else f)
+
+    def values(self, rid: int) -> np.ndarray:
+        """Filtration values of a built request's matrix (submitted with values=True)."""
+        self.wait(rid)
+        n = self._lib.sspp_server_values(self._h, rid, None, 0)
+        if n < 0:
+            raise SsppError(ERR_STATE, "no values kept for this request")
+        out = np.empty(max(n, 1), dtype=np.float32)
+        self._lib.sspp_server_values(self._h, rid, out.ctypes.data, n)
+        return out[:n]
 
     def wait(self, rid: int, timeout_ms: float = -1.0) -> bool:
         rc = self._lib.sspp_server_wait(self._h, rid, timeout_ms)

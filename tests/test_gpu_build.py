@@ -157,3 +157,50 @@ def test_builders_reject_bad_input():
         with pytest.raises(SsppError):
             e.load_csc(gen.rips(50, 2, 1, 0.2, 2))
             e.input_matrix(values=True)  # values exist for built complexes only
+
+
+def test_server_builds_point_cloud_and_field_requests():
+    from specseqplusplus_b200 import Server
+
+    rng = np.random.default_rng(13)
+    clouds = [(gen.points(int(n), d, int(s)), float(r), 2 if d == 2 else 3)
+              for n, d, s, r in [(900, 2, 1, 0.06), (1500, 3, 2, 0.09), (400, 3, 3, 0.2), (2500, 2, 4, 0.03)]]
+    fields = [gen.field(12, 1.5, 5), gen.field(20, 2.0, 6), rng.normal(size=(7, 9, 5)).astype(np.float32)]
+    mats = [gen.rips(700, 3, 7, 0.15, 3), gen.lowerstar(10, 1.0, 8)]
+    want = {}
+    with Engine(0) as e:
+        for i, (pts, r, md) in enumerate(clouds):
+            e.load_rips(pts, r, md)
+            e.reduce(Params())
+            want[("r", i)] = (e.pairs(), e.essentials(), e.input_matrix(values=True).values)
+        for i, f in enumerate(fields):
+            e.load_lowerstar(f)
+            e.reduce(Params())
+            want[("l", i)] = (e.pairs(), e.essentials(), e.input_matrix(values=True).values)
+        for i, m in enumerate(mats):
+            e.load_csc(m)
+            e.reduce(Params())
+            want[("m", i)] = (e.pairs(), e.essentials(), None)
+    with Server(Params(autotune=2), workers=2) as srv:
+        ids = {}
+        for rep in range(2):  # interleaved kinds, twice
+            for i, (pts, r, md) in enumerate(clouds):
+                ids[("r", i, rep)] = srv.submit_rips(pts, r, md, values=(rep == 0))
+            for i, m in enumerate(mats):
+                ids[("m", i, rep)] = srv.submit(m)
+            for i, f in enumerate(fields):
+                ids[("l", i, rep)] = srv.submit_lowerstar(f, values=(rep == 1), copy=(rep == 0))
+        bad = gen.field(6, 1.0, 9)
+        bad[1, 2, 3] = np.nan
+        bad_id = srv.submit_lowerstar(bad)
+        for (k, i, rep), rid in ids.items():
+            p, es, vals = want[(k, i)]
+            assert np.array_equal(srv.pairs(rid), p), (k, i, rep)
+            assert np.array_equal(srv.essentials(rid), es), (k, i, rep)
+            if (k == "r" and rep == 0) or (k == "l" and rep == 1):
+                assert np.array_equal(srv.values(rid).view(np.uint32), vals.view(np.uint32))
+        with pytest.raises(SsppError):
+            srv.pairs(bad_id)
+    with Server(Params(), workers=1, memory_budget=1 << 20) as small:
+        with pytest.raises(SsppError):
+            small.submit_lowerstar(gen.field(40, 1.0, 1))  # larger than the budget: refused at submit

@@ -42,7 +42,9 @@ def test_autotune_cycles_candidates_with_identical_pairs(autotune):
                 assert st["tuned_candidate"] >= 0
                 assert np.array_equal(e.pairs(), ref.pairs), (rep, p)
                 assert np.array_equal(e.essentials(), ref.essential)
-    assert len(seen) >= (8 if autotune == 2 else 4)
+    # several settings tried, all with the oracle's pairs (how many depends on the
+    # process-wide history: candidates measured twice as slow on similar inputs are skipped)
+    assert len(seen) >= 4
 
 
 def _mix(seed):
