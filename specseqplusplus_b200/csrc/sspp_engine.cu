@@ -537,7 +537,7 @@ int run_steps(sspp_ctx* ctx, const std::vector<Step>& steps, int cap1, int cap2,
     // finished dimension) -- on large inputs only until few of them are left
     // (the dimension gate below).
     const bool overlap = true;
-    const bool gate = D.n >= kGateMinCols && ctx->h_gate;
+    const bool gate = D.n >= kGateMinCols && ctx->h_gate && ctx->d_gate && ctx->h_tail && ctx->gate_ev;
     D.gate_host = gate ? ctx->d_gate : nullptr;
     if (gate) {
         *reinterpret_cast<volatile int*>(ctx->h_gate) = 0;  // no CTA-tier launch of this context is running
@@ -800,12 +800,17 @@ sspp_ctx* sspp_create(const sspp_config* cfg) {
             cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
         }
     }
+    // the dimension gate's progress word; without it the dimensions simply join
     if (cudaHostAlloc(&ctx->h_gate, sizeof(int), cudaHostAllocMapped) != cudaSuccess ||
         cudaHostGetDevicePointer(reinterpret_cast<void**>(&ctx->d_gate), ctx->h_gate, 0) != cudaSuccess ||
         cudaMallocHost(&ctx->h_tail, sizeof(int)) != cudaSuccess ||
         cudaEventCreateWithFlags(&ctx->gate_ev, cudaEventDisableTiming) != cudaSuccess) {
-        delete ctx;
-        return nullptr;
+        cudaGetLastError();
+        if (ctx->h_gate) cudaFreeHost(ctx->h_gate);
+        if (ctx->h_tail) cudaFreeHost(ctx->h_tail);
+        if (ctx->gate_ev) cudaEventDestroy(ctx->gate_ev);
+        ctx->h_gate = ctx->d_gate = ctx->h_tail = nullptr;
+        ctx->gate_ev = nullptr;
     }
     if (cudaMallocHost(&ctx->h_err, sizeof(int)) != cudaSuccess ||
         cudaMallocHost(&ctx->h_counters, sizeof(long long) * CNT_NUM) != cudaSuccess ||
