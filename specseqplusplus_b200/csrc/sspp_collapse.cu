@@ -245,6 +245,31 @@ __global__ void __launch_bounds__(kWarpsA * 32) k_arrival(const int32_t* misc, c
     }
 }
 
+// An arrival re-examines only earlier edges that are not critical, and an edge
+// is critical from its arrival on if it was kept then (criticality only ever
+// grows).  So an arrival whose triangles' other edges were all kept at their
+// own arrival pushes nothing and re-examines nothing: it leaves the cascade
+// list (arr 2 -> 1).  Arrivals whose common neighbourhood does not fit in
+// shared memory stay in it.  Concurrent writes only turn 2 into 1, which the
+// test (arr == 0) does not see.
+__global__ void __launch_bounds__(kWarpsA * 32) k_prefilter(const int32_t* misc, const int32_t* eu, const int32_t* ev,
+                                                           const uint64_t* adj, const int64_t* off, uint8_t* arr) {
+    __shared__ int32_t sC[kWarpsA][kCapA], sA[kWarpsA][kCapA], sB[kWarpsA][kCapA];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t gw = int64_t(blockIdx.x) * kWarpsA + w, nw = int64_t(gridDim.x) * kWarpsA;
+    const int64_t E = misc[kMiscE];
+    for (int64_t t = gw; t < E; t += nw) {
+        if (arr[t] != 2) continue;
+        const Valid ok{int32_t(t), int32_t(t), nullptr};
+        const int c = common_nbrs(adj, off, eu[t], ev[t], ok, sC[w], sA[w], sB[w], kCapA);
+        if (c > kCapA) continue;
+        bool open = false;
+        for (int k = lane; k < c; k += 32) open |= arr[sA[w][k]] == 0 || arr[sB[w][k]] == 0;
+        if (!__any_sync(kFull, open) && lane == 0) arr[t] = 1;
+        __syncwarp();
+    }
+}
+
 // max-heap of edge ids (one thread)
 __device__ void heap_push(int32_t* h, int& size, int32_t x) {
     int i = size++;
@@ -489,6 +514,8 @@ int collapse(Device& D, const DimInfo& info, uint8_t* dropped, CollapseScratch& 
     }
     k_arrival<<<unsigned(warps_a / kWarpsA), kWarpsA * 32, 0, s>>>(
         S.misc, S.eu, S.ev, S.adj, S.adj_off, S.arr, S.crit, S.cbuf, per_warp);
+    k_prefilter<<<unsigned(warps_a / kWarpsA), kWarpsA * 32, 0, s>>>(S.misc, S.eu, S.ev, S.adj, S.adj_off, S.arr);
+    launches++;
     {
         const uint8_t* arr = S.arr;
         int32_t* cas = S.cas;
