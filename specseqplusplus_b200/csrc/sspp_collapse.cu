@@ -300,21 +300,69 @@ __device__ int32_t heap_pop(int32_t* h, int& size) {
     return top;
 }
 
-// the earlier non-critical edges uw, vw of the triangles of edge th go into the set
+// The pending set: a max-heap of edge ids, kept by lane 0 in shared memory
+// until it would overflow, then (for the rest of the launch) in global memory.
+constexpr int kHeapS = 4096;
+
+struct Pending {
+    int32_t* h;
+    int cap;
+    int size;
+    int32_t* global;  // room for every edge
+};
+
+__device__ __forceinline__ void pending_push(Pending& P, int32_t x) {
+    if (P.size == P.cap && P.h != P.global) {
+        for (int i = 0; i < P.size; i++) P.global[i] = P.h[i];
+        P.h = P.global;
+        P.cap = INT_MAX;
+    }
+    heap_push(P.h, P.size, x);
+}
+
+// The earlier non-critical edges uw, vw of the triangles of edge th go into
+// the set: the lanes test them (no edge appears twice: uw != vw' for common
+// neighbours w, w' of u and v), then lane 0 pushes the ones taken, from
+// `list` (kCapB entries of shared memory; larger lists are pushed by lane 0
+// directly).
 __device__ void push_partners(const int32_t* A, const int32_t* B, int c, int32_t th, const uint8_t* crit, uint8_t* ins,
-                              int32_t* heap, int& size) {
-    if (lane_id() == 0) {
-        for (int k = 0; k < c; k++) {
-            const int32_t ab[2] = {A[k], B[k]};
-            for (int q = 0; q < 2; q++) {
-                const int32_t x = ab[q];
-                if (x < th && !crit[x] && !ins[x]) {
-                    ins[x] = 1;
-                    heap_push(heap, size, x);
+                              int32_t* list, Pending& P) {
+    const int lane = lane_id();
+    if (2 * c > kCapB) {
+        if (lane == 0) {
+            for (int k = 0; k < c; k++) {
+                const int32_t ab[2] = {A[k], B[k]};
+                for (int q = 0; q < 2; q++) {
+                    const int32_t x = ab[q];
+                    if (x < th && !crit[x] && !ins[x]) {
+                        ins[x] = 1;
+                        pending_push(P, x);
+                    }
                 }
             }
         }
+        __syncwarp();
+        return;
     }
+    int m = 0;
+    for (int base = 0; base < 2 * c; base += 32) {
+        const int k = base + lane;
+        int32_t x = -1;
+        bool want = false;
+        if (k < 2 * c) {
+            x = k < c ? A[k] : B[k - c];
+            want = x < th && !crit[x] && !ins[x];
+        }
+        const unsigned bm = __ballot_sync(kFull, want);
+        if (want) {
+            list[m + __popc(bm & lanemask_lt())] = x;
+            ins[x] = 1;
+        }
+        m += __popc(bm);
+    }
+    __syncwarp();
+    if (lane == 0)
+        for (int j = 0; j < m; j++) pending_push(P, list[j]);
     __syncwarp();
 }
 
@@ -324,9 +372,11 @@ __global__ void __launch_bounds__(32) k_cascade(const int32_t* cas, int32_t* mis
                                                int32_t* heap, int32_t* gC, int32_t* gA, int32_t* gB, int64_t gcap,
                                                long long max_steps, int* err) {
     __shared__ int32_t sC[kCapB], sA[kCapB], sB[kCapB];
+    __shared__ int32_t sheap[kHeapS];
     const int lane = lane_id();
     const int ncas = misc[kMiscCascades];
-    int size = 0;  // heap size, meaningful in lane 0 and broadcast
+    Pending P{sheap, kHeapS, 0, heap};  // kept by lane 0
+    int size = 0;                        // P.size, broadcast
     long long steps = 0;
     bool fail = false;
     for (int i = 0; i < ncas && !fail; i++) {
@@ -340,8 +390,8 @@ __global__ void __launch_bounds__(32) k_cascade(const int32_t* cas, int32_t* mis
                 A = gA;
                 B = gB;
             }
-            push_partners(A, B, c, t, crit, ins, heap, size);
-            size = __shfl_sync(kFull, size, 0);
+            push_partners(A, B, c, t, crit, ins, sC, P);
+            size = __shfl_sync(kFull, P.size, 0);
         }
         while (size > 0) {
             if (++steps > max_steps) {
@@ -350,11 +400,11 @@ __global__ void __launch_bounds__(32) k_cascade(const int32_t* cas, int32_t* mis
             }
             int32_t e = 0;
             if (lane == 0) {
-                e = heap_pop(heap, size);
+                e = heap_pop(P.h, P.size);
                 ins[e] = 0;
             }
             e = __shfl_sync(kFull, e, 0);
-            size = __shfl_sync(kFull, size, 0);
+            size = __shfl_sync(kFull, P.size, 0);
             __syncwarp();
             if (crit[e]) continue;
             const Valid ok{e, t, crit};
@@ -370,8 +420,8 @@ __global__ void __launch_bounds__(32) k_cascade(const int32_t* cas, int32_t* mis
             if (dom) continue;
             if (lane == 0) crit[e] = 1;
             __syncwarp();
-            push_partners(A, B, c, e, crit, ins, heap, size);
-            size = __shfl_sync(kFull, size, 0);
+            push_partners(A, B, c, e, crit, ins, sC, P);
+            size = __shfl_sync(kFull, P.size, 0);
         }
     }
     if (lane == 0) {
