@@ -38,6 +38,7 @@ constexpr int kWarpsA = 8;     // arrival kernel: warps per block
 constexpr int kCapA = 256;     // common neighbours in shared memory per warp (arrival kernel)
 constexpr int kCapB = 2048;    // common neighbours in shared memory (re-examination kernel)
 constexpr int kMiscE = 0, kMiscMaxDeg = 1, kMiscCascades = 2, kMiscSteps = 3;
+constexpr int kOpen = 8;       // partners listed per arrival by the prefilter
 
 unsigned grid_of(int64_t n, int threads, int64_t cap = 65536) {
     int64_t g = (n + threads - 1) / threads;
@@ -252,8 +253,11 @@ __global__ void __launch_bounds__(kWarpsA * 32) k_arrival(const int32_t* misc, c
 // list (arr 2 -> 1).  Arrivals whose common neighbourhood does not fit in
 // shared memory stay in it.  Concurrent writes only turn 2 into 1, which the
 // test (arr == 0) does not see.
+// The partners that can be pushed at all (at most kOpen of them) are listed
+// for the cascade, which then does not recompute the arrival's triangles.
 __global__ void __launch_bounds__(kWarpsA * 32) k_prefilter(const int32_t* misc, const int32_t* eu, const int32_t* ev,
-                                                           const uint64_t* adj, const int64_t* off, uint8_t* arr) {
+                                                           const uint64_t* adj, const int64_t* off, uint8_t* arr,
+                                                           int32_t* open, int8_t* nopen) {
     __shared__ int32_t sC[kWarpsA][kCapA], sA[kWarpsA][kCapA], sB[kWarpsA][kCapA];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t gw = int64_t(blockIdx.x) * kWarpsA + w, nw = int64_t(gridDim.x) * kWarpsA;
@@ -262,10 +266,28 @@ __global__ void __launch_bounds__(kWarpsA * 32) k_prefilter(const int32_t* misc,
         if (arr[t] != 2) continue;
         const Valid ok{int32_t(t), int32_t(t), nullptr};
         const int c = common_nbrs(adj, off, eu[t], ev[t], ok, sC[w], sA[w], sB[w], kCapA);
-        if (c > kCapA) continue;
-        bool open = false;
-        for (int k = lane; k < c; k += 32) open |= arr[sA[w][k]] == 0 || arr[sB[w][k]] == 0;
-        if (!__any_sync(kFull, open) && lane == 0) arr[t] = 1;
+        if (c > kCapA) {
+            if (lane == 0) nopen[t] = -1;
+            continue;
+        }
+        int cnt = 0;
+        for (int base = 0; base < 2 * c; base += 32) {
+            const int k = base + lane;
+            int32_t x = -1;
+            bool o = false;
+            if (k < 2 * c) {
+                x = k < c ? sA[w][k] : sB[w][k - c];
+                o = arr[x] == 0;
+            }
+            const unsigned bm = __ballot_sync(kFull, o);
+            const int p = cnt + __popc(bm & lanemask_lt());
+            if (o && p < kOpen) open[t * kOpen + p] = x;
+            cnt += __popc(bm);
+        }
+        if (lane == 0) {
+            if (cnt == 0) arr[t] = 1;
+            nopen[t] = int8_t(cnt <= kOpen ? cnt : -1);
+        }
         __syncwarp();
     }
 }
@@ -369,8 +391,8 @@ __device__ void push_partners(const int32_t* A, const int32_t* B, int c, int32_t
 // Re-examinations, in arrival order, by one warp.
 __global__ void __launch_bounds__(32) k_cascade(const int32_t* cas, int32_t* misc, const int32_t* eu, const int32_t* ev,
                                                const uint64_t* adj, const int64_t* off, uint8_t* crit, uint8_t* ins,
-                                               int32_t* heap, int32_t* gC, int32_t* gA, int32_t* gB, int64_t gcap,
-                                               long long max_steps, int* err) {
+                                               int32_t* heap, const int32_t* open, const int8_t* nopen, int32_t* gC,
+                                               int32_t* gA, int32_t* gB, int64_t gcap, long long max_steps, int* err) {
     __shared__ int32_t sC[kCapB], sA[kCapB], sB[kCapB];
     __shared__ int32_t sheap[kHeapS];
     const int lane = lane_id();
@@ -381,7 +403,21 @@ __global__ void __launch_bounds__(32) k_cascade(const int32_t* cas, int32_t* mis
     bool fail = false;
     for (int i = 0; i < ncas && !fail; i++) {
         const int32_t t = cas[i];
-        {
+        const int no = nopen[t];
+        if (no >= 0) {  // the prefilter's list: edges before t, dominated at their own arrival
+            const int32_t x = lane < no ? open[int64_t(t) * kOpen + lane] : -1;
+            const bool want = lane < no && !crit[x] && !ins[x];
+            const unsigned bm = __ballot_sync(kFull, want);
+            if (want) {
+                sC[__popc(bm & lanemask_lt())] = x;
+                ins[x] = 1;
+            }
+            __syncwarp();
+            if (lane == 0)
+                for (int j = 0; j < __popc(bm); j++) pending_push(P, sC[j]);
+            __syncwarp();
+            size = __shfl_sync(kFull, P.size, 0);
+        } else {
             const Valid ok{t, t, nullptr};
             int c = common_nbrs(adj, off, eu[t], ev[t], ok, sC, sA, sB, kCapB);
             const int32_t *A = sA, *B = sB;
@@ -475,7 +511,8 @@ cudaError_t grow_buf(T*& p, int64_t want, cudaStream_t s) {
 }  // namespace
 
 void collapse_free(CollapseScratch& S) {
-    void* ptrs[] = {S.eu, S.ev, S.ecol, S.deg, S.adj_off, S.adj, S.arr, S.crit, S.ins, S.heap, S.cas, S.cbuf, S.misc};
+    void* ptrs[] = {S.eu, S.ev, S.ecol, S.deg, S.adj_off, S.adj, S.arr, S.crit, S.ins, S.heap, S.cas, S.open, S.nopen,
+                    S.cbuf, S.misc};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     S = CollapseScratch();
@@ -494,7 +531,7 @@ int collapse(Device& D, const DimInfo& info, uint8_t* dropped, CollapseScratch& 
     if (ne > S.cap_e) {
         if (grow_buf(S.eu, ne, s) || grow_buf(S.ev, ne, s) || grow_buf(S.ecol, ne, s) || grow_buf(S.adj, 2 * ne, s) ||
             grow_buf(S.arr, ne, s) || grow_buf(S.crit, ne, s) || grow_buf(S.ins, ne, s) || grow_buf(S.heap, ne, s) ||
-            grow_buf(S.cas, ne, s))
+            grow_buf(S.cas, ne, s) || grow_buf(S.open, ne * kOpen, s) || grow_buf(S.nopen, ne, s))
             return -1;
         S.cap_e = ne;
     }
@@ -564,7 +601,8 @@ int collapse(Device& D, const DimInfo& info, uint8_t* dropped, CollapseScratch& 
     }
     k_arrival<<<unsigned(warps_a / kWarpsA), kWarpsA * 32, 0, s>>>(
         S.misc, S.eu, S.ev, S.adj, S.adj_off, S.arr, S.crit, S.cbuf, per_warp);
-    k_prefilter<<<unsigned(warps_a / kWarpsA), kWarpsA * 32, 0, s>>>(S.misc, S.eu, S.ev, S.adj, S.adj_off, S.arr);
+    k_prefilter<<<unsigned(warps_a / kWarpsA), kWarpsA * 32, 0, s>>>(S.misc, S.eu, S.ev, S.adj, S.adj_off, S.arr,
+                                                                      S.open, S.nopen);
     launches++;
     {
         const uint8_t* arr = S.arr;
@@ -582,8 +620,8 @@ int collapse(Device& D, const DimInfo& info, uint8_t* dropped, CollapseScratch& 
     // by a kept edge's triangles; the bound only guards against a corrupted set
     const double bound = 64.0 * double(E) * double(maxdeg + 1) + double(1 << 20);
     const long long max_steps = bound > 4.0e18 ? (long long)4e18 : (long long)bound;
-    k_cascade<<<1, 32, 0, s>>>(S.cas, S.misc, S.eu, S.ev, S.adj, S.adj_off, S.crit, S.ins, S.heap, S.cbuf,
-                               S.cbuf + gcap, S.cbuf + 2 * gcap, gcap, max_steps, D.err);
+    k_cascade<<<1, 32, 0, s>>>(S.cas, S.misc, S.eu, S.ev, S.adj, S.adj_off, S.crit, S.ins, S.heap, S.open, S.nopen,
+                               S.cbuf, S.cbuf + gcap, S.cbuf + 2 * gcap, gcap, max_steps, D.err);
     k_drop_edges<<<grid_of(E, 256), 256, 0, s>>>(S.misc, S.crit, S.ecol, dropped);
     launches += 7;
     for (int d = 2; d <= kMaxDim; d++) {

@@ -18,6 +18,8 @@ struct CollapseScratch {
     uint8_t* ins = nullptr;      // [E] in the re-examination set
     int32_t* heap = nullptr;     // [E] re-examination set, max-heap
     int32_t* cas = nullptr;      // [E] arrivals with re-examinations, ascending
+    int32_t* open = nullptr;     // [E * kOpen] per arrival: its triangles' edges dominated at their arrival
+    int8_t* nopen = nullptr;     // [E] how many (-1: more than kOpen, or not listed)
     int32_t* cbuf = nullptr;     // overflow buffers of the common neighbourhoods
     int32_t* misc = nullptr;     // [8] device scalars
     int64_t cap_e = 0, cap_v = 0, cap_cbuf = 0;
