@@ -79,3 +79,15 @@ def test_cpp_mirror_header_compiles(tmp_path):
                         "-L", os.path.dirname(LIB), "-lsspp", "-Wl,-rpath," + os.path.dirname(LIB)],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+def test_c_abi_null_handles(tmp_path):
+    # include/sspp.h as plain C99; null handles fail cleanly without a GPU
+    out = tmp_path / "abi_null"
+    r = subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-Werror", "-I", os.path.join(ROOT, "include"),
+                        os.path.join(ROOT, "tests", "cpp", "abi_null.c"), "-o", str(out),
+                        "-L", os.path.dirname(LIB), "-lsspp", "-Wl,-rpath," + os.path.dirname(LIB)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([str(out)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0 and r.stdout.strip() == "ok", r.stdout + r.stderr
