@@ -437,11 +437,17 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the batched, served, 2000-point Rips and 100k-point VR legs")
+    ap.add_argument("--only", choices=["vr100k"],
+                    help="profiling runs: run one extra leg alone and print its JSON")
     args = ap.parse_args()
     if args.grid != GRID:
         globals()["GRID"] = args.grid
     if args.impl == "reference":
         return reference_arm(args)
+    if args.only == "vr100k":
+        peak = float(load_peaks()[0].get("hbm_gbs", 6650.0))
+        print(json.dumps({"vr100k": leg_vr100k(args.steps, peak), "profiling_run": True}))
+        return 0
 
     import numpy as np
     import torch
