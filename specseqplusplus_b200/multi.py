@@ -62,3 +62,51 @@ def reduce_batch(mats, params, group=None, device: int = 0, dst: int = 0, reduce
         for i, p, e in part:
             out[i] = (p, e)
     return out
+
+
+def _size_of(req) -> int:
+    """Work estimate of a point-cloud or field request: its vertex count."""
+    kind, data = req[0], req[1]
+    return int(np.asarray(data).shape[0]) if kind == "rips" else int(np.asarray(data).size)
+
+
+def _reduce_built_local(reqs, params, device):
+    from .engine import Engine
+
+    out = []
+    if not reqs:
+        return out
+    with Engine(device) as e:
+        for req in reqs:
+            if req[0] == "rips":
+                e.load_rips(req[1], req[2], req[3])
+            else:
+                e.load_lowerstar(req[1], req[2])
+            e.reduce(params)
+            out.append((e.pairs(), e.essentials()))
+    return out
+
+
+def reduce_requests(reqs, params, group=None, device: int = 0, dst: int = 0, reduce_fn=None):
+    """Point clouds and fields across the ranks of `group`: each rank builds (on its GPU) and
+    reduces its share.  reqs: ("rips", points [npts, D], radius, maxdim) or ("lowerstar",
+    field [gz, gy, gx], maxdim), the same list on every rank.  Returns [(pairs, essentials)]
+    in input order on rank `dst` (indices of the built matrices), None elsewhere;
+    reduce_fn(local_reqs, params, device) replaces the single-GPU loop."""
+    import torch.distributed as dist
+
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    parts = shard([_size_of(r) for r in reqs], world)
+    mine = parts[rank]
+    res = (reduce_fn or _reduce_built_local)([reqs[i] for i in mine], params, device)
+    payload = [(i, np.asarray(p), np.asarray(e)) for i, (p, e) in zip(mine, res)]
+    gathered = [None] * world if rank == dst else None
+    dist.gather_object(payload, gathered, dst=dst, group=group)
+    if rank != dst:
+        return None
+    out = [None] * len(reqs)
+    for part in gathered:
+        for i, p, e in part:
+            out[i] = (p, e)
+    return out
+

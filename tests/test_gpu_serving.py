@@ -175,5 +175,16 @@ def test_multi_gpu_dispatcher_single_rank_runs_the_engine():
         for (p, e), m in zip(res, mats):
             ref = oracle.reduce(m)
             assert np.array_equal(p, ref.pairs) and np.array_equal(e, ref.essential)
+        # point clouds and fields: built on the device by the rank that takes them
+        from specseqplusplus_b200 import gen
+        from specseqplusplus_b200.multi import reduce_requests
+
+        reqs = [("rips", gen.points(300, 3, 3), 0.2, 3), ("lowerstar", gen.field(9, 1.5, 4), 3),
+                ("rips", gen.points(500, 2, 5), 0.08, 2)]
+        res = reduce_requests(reqs, Params())
+        for (p, e), q in zip(res, reqs):
+            m = gen.rips_from_points(q[1], q[2], q[3]) if q[0] == "rips" else gen.lowerstar_from_field(q[1], q[2])
+            ref = oracle.reduce(m)
+            assert np.array_equal(p, ref.pairs) and np.array_equal(e, ref.essential)
     finally:
         dist.destroy_process_group()
