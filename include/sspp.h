@@ -346,10 +346,14 @@ int32_t sspp_server_reset_stats(sspp_server* srv);
  * device pointers: d_pairs receives up to ncols (birth, death) int64 pairs
  * sorted by birth (room for 2 * ncols int64), *d_npairs their number.  Limits:
  * ncols <= 1048576 and 3 * ncols + nnz <= 12582896, else SSPP_ERR_BAD_INPUT;
- * fill-in beyond the array gives SSPP_ERR_CAPACITY.  The first call on a device
- * looks up the array's address (make it before any stream capture); calls that
- * overlap on the GPU share the array and race, so serialise them.  Blocks until
- * done; a message is written to err_msg (may be NULL) when it fails. */
+ * fill-in beyond the array gives SSPP_ERR_CAPACITY; a col_ptr that does not
+ * run from 0 to nnz without decreasing, a dimension outside 0..7, or faces that
+ * are unsorted, out of range or not one dimension lower give
+ * SSPP_ERR_BAD_INPUT.  The first call on a device looks up the array's address
+ * (make it before any stream capture); calls that overlap on the GPU share the
+ * array and race, so serialise them.  Each call copies the status word back and
+ * synchronises the stream, so it returns once the reduction has finished; a
+ * message is written to err_msg (may be NULL) when it fails. */
 int32_t sspp_reduce_noalloc(int64_t ncols, int64_t nnz, const int32_t* d_dims, const int64_t* d_col_ptr,
                             const int32_t* d_rows, int64_t* d_pairs, int64_t* d_npairs, void* stream, char* err_msg,
                             int32_t err_cap);

@@ -16,6 +16,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <type_traits>
 #include <vector>
 
@@ -479,10 +480,14 @@ int run_init(sspp_ctx* ctx) {
 // so the pairs do not change; only that column's work is wasted, and at most
 // kGateLeft rows can be cleared late.  Progress comes from the CTA tier's
 // mirror in mapped host memory (a lower bound); the wait also ends when every
-// side stream is idle, or after kGateMaxMs.
+// side stream is idle, or after kGateMaxMs.  The polling thread yields its core
+// between reads, and after kGateSpinMs of waiting sleeps kGateNapUs between
+// them, so a server's workers do not each hold a spinning core.
 constexpr int64_t kGateMinCols = int64_t(1) << 17;
 constexpr int kGateLeft = 16;
 constexpr double kGateMaxMs = 30000.0;
+constexpr double kGateSpinMs = 2.0;
+constexpr int kGateNapUs = 50;
 
 int dimension_gate(sspp_ctx* ctx) {
     cudaStream_t s = ctx->stream;
@@ -498,9 +503,15 @@ int dimension_gate(sspp_ctx* ctx) {
             bool idle = true;
             for (int q = 0; q < sspp_ctx::kSide && idle; q++) idle = cudaStreamQuery(ctx->side[q]) != cudaErrorNotReady;
             if (idle) break;
-            if (std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count() > kGateMaxMs)
-                break;
+            const double waited =
+                std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+            if (waited > kGateMaxMs) break;
+            if (waited > kGateSpinMs) {
+                std::this_thread::sleep_for(std::chrono::microseconds(kGateNapUs));
+                continue;
+            }
         }
+        std::this_thread::yield();
     }
     return SSPP_OK;
 }

@@ -20,11 +20,18 @@
 // The array's device address is looked up with cudaGetSymbolAddress the
 // first time the entry point runs on a device (with that device current) and
 // cached per device, so the first call on each device should be made before
-// any stream capture begins.  Every call reuses the same array and leaves its
+// any stream capture begins.  Every call then copies the kernel's status word
+// back to the host and synchronises the stream, so it returns only once the
+// reduction has finished.  Every call reuses the same array and leaves its
 // contents behind; the kernel clears what must start empty (the pivot table,
 // the arena cursor, the error word) itself.  Two calls that overlap on the
 // GPU - on two streams, or from two threads - share the array and corrupt each
 // other: serialise them.
+//
+// Validation happens in the kernel before any reduction: col_ptr must start
+// at 0, end at nnz and never decrease (every column's range inside [0, nnz]),
+// dimensions must lie in 0..7, and each column's faces must be ascending, in
+// range and one dimension lower; anything else is SSPP_ERR_BAD_INPUT.
 //
 // The reduction is the standard twist (clearing) reduction, dimensions from
 // high to low, run by one thread block: columns one after another, each
@@ -45,6 +52,7 @@ constexpr int64_t kFillReserve = int64_t(4) << 20;   // ints kept free for fill-
 constexpr int kCtl = 16;                            // control words at the start of the array
 constexpr int kMaxDevices = 64;
 constexpr int kThreads = 256;
+constexpr int kMaxDim = 7;                          // dimensions 0..7, as the context API
 
 // control words
 enum { C_ERR = 0, C_TOP_LO = 1, C_TOP_HI = 2, C_NPAIRS_LO = 3, C_NPAIRS_HI = 4, C_MAXDIM = 5 };
@@ -149,7 +157,9 @@ __global__ void __launch_bounds__(kThreads) k_reduce_noalloc(int32_t* S, int64_t
         pivot[j] = -1;
         const int64_t b = col_ptr[j], e = col_ptr[j + 1];
         const int d = dims[j];
-        bool bad = e < b || e > nnz || d < 0;
+        // every column's range must lie inside [0, nnz] before any entry is
+        // read or copied (the copy runs in the same pass as the checks)
+        bool bad = b < 0 || e < b || e > nnz || d < 0 || d > kMaxDim;
         for (int64_t k = b; k < e && !bad; k++) {
             const int32_t r = rows[k];
             if (r < 0 || r >= n || (k > b && r <= rows[k - 1]) || dims[r] != d - 1) bad = true;

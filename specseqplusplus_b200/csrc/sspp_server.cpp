@@ -466,9 +466,13 @@ extern "C" {
 int32_t sspp_server_wait(sspp_server* S, int64_t id, double timeout_ms) {
     if (!S) return SSPP_ERR_BAD_INPUT;
     std::unique_lock<std::mutex> l(S->mu);
-    Request* r = find(S, id);
-    if (!r) return SSPP_ERR_STATE;
-    auto done = [&] { return finished(r); };
+    if (!find(S, id)) return SSPP_ERR_STATE;
+    // the request is looked up again on every wake-up: another thread may
+    // release it (and free it) while this one waits with the lock released
+    auto done = [&] {
+        Request* r = find(S, id);
+        return !r || finished(r);
+    };
     if (timeout_ms < 0) S->cv_done.wait(l, done);
     else if (!S->cv_done.wait_for(l, std::chrono::duration<double, std::milli>(timeout_ms), done))
         return SSPP_ERR_TIMEOUT;

@@ -16,6 +16,23 @@ import heapq
 import numpy as np
 
 
+def local_device() -> int:
+    """This process's GPU under one process per GPU: LOCAL_RANK (set by torchrun),
+    else the current CUDA device once CUDA is initialised, else 0."""
+    import os
+
+    if "LOCAL_RANK" in os.environ:
+        return int(os.environ["LOCAL_RANK"])
+    try:
+        import torch
+
+        if torch.cuda.is_available() and torch.cuda.is_initialized():
+            return torch.cuda.current_device()
+    except ImportError:
+        pass
+    return 0
+
+
 def shard(ncols, world: int) -> list:
     """Complex indices of each rank (largest complexes first, to the least loaded rank)."""
     order = sorted(range(len(ncols)), key=lambda i: (-int(ncols[i]), i))
@@ -39,14 +56,18 @@ def _reduce_local(mats, params, device):
         return e.batch_results()
 
 
-def reduce_batch(mats, params, group=None, device: int = 0, dst: int = 0, reduce_fn=None):
+def reduce_batch(mats, params, group=None, device: int | None = None, dst: int = 0, reduce_fn=None):
     """Reduces `mats` (the same list on every rank) across the ranks of `group`.
 
     Returns [(pairs, essentials)] in input order on rank `dst`, None elsewhere.
     reduce_fn(local_mats, params, device) replaces the single-GPU batch reduction
-    (the default runs the engine on `device`).
+    (the default runs the engine on `device`).  `device` defaults to this
+    process's GPU (see local_device); with the nccl backend, call
+    torch.cuda.set_device(local_rank) first, as the object gather needs it.
     """
     import torch.distributed as dist
+
+    device = local_device() if device is None else device
 
     rank, world = dist.get_rank(group), dist.get_world_size(group)
     parts = shard([m.ncols for m in mats], world)
@@ -87,13 +108,16 @@ def _reduce_built_local(reqs, params, device):
     return out
 
 
-def reduce_requests(reqs, params, group=None, device: int = 0, dst: int = 0, reduce_fn=None):
+def reduce_requests(reqs, params, group=None, device: int | None = None, dst: int = 0, reduce_fn=None):
     """Point clouds and fields across the ranks of `group`: each rank builds (on its GPU) and
     reduces its share.  reqs: ("rips", points [npts, D], radius, maxdim) or ("lowerstar",
     field [gz, gy, gx], maxdim), the same list on every rank.  Returns [(pairs, essentials)]
     in input order on rank `dst` (indices of the built matrices), None elsewhere;
-    reduce_fn(local_reqs, params, device) replaces the single-GPU loop."""
+    reduce_fn(local_reqs, params, device) replaces the single-GPU loop.  `device`
+    defaults to this process's GPU, as for reduce_batch."""
     import torch.distributed as dist
+
+    device = local_device() if device is None else device
 
     rank, world = dist.get_rank(group), dist.get_world_size(group)
     parts = shard([_size_of(r) for r in reqs], world)

@@ -11,7 +11,9 @@ import os
 import struct
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_PAIRS = "/root/reference/phat-highclear/examples/single_triangle_persistence_pairs.dat"
+# the reference tree's root comes from SSPP_REFERENCE (checked only when set)
+REF_PAIRS = os.path.join(os.environ.get("SSPP_REFERENCE", ""),
+                         "phat-highclear/examples/single_triangle_persistence_pairs.dat")
 
 COLUMNS = [(0, []), (0, []), (0, []), (1, [0, 1]), (1, [0, 2]), (1, [1, 2]), (2, [3, 4, 5])]
 PAIRS = [(1, 3), (2, 4), (5, 6)]
@@ -30,7 +32,7 @@ def main():
         f.write(f"{len(PAIRS)}\n")
         for b, d in PAIRS:
             f.write(f"{b} {d}\n")
-    if os.path.exists(REF_PAIRS):
+    if os.environ.get("SSPP_REFERENCE") and os.path.exists(REF_PAIRS):
         ref = [ln.split() for ln in open(REF_PAIRS).read().split("\n") if ln.strip()]
         assert int(ref[0][0]) == len(PAIRS)
         assert [(int(a), int(b)) for a, b in ref[1:]] == PAIRS, "fixture disagrees with the reference's answer"

@@ -255,3 +255,26 @@ def test_batch_device_concatenation():
         e.reduce(Params())
         for i, m in enumerate(mats):
             assert np.array_equal(e.batch_pairs(i), oracle.reduce(m).pairs)
+
+
+@pytest.fixture(scope="module")
+def lowerstar64_model1():
+    # the benched workload: 64^3 Freudenthal lower-star, sigma 2, seed 2;
+    # model 1 (guided clearing), max_iteration 10 -- the oracle runs once
+    m = gen.lowerstar(64, 2.0, 2)
+    return m, oracle.reduce(m, model=1, max_iteration=10)
+
+
+@pytest.mark.parametrize("l1,l2", [(32, 8192), (1000, 8000)])
+def test_lowerstar_64_model1_as_benched(lowerstar64_model1, l1, l2):
+    # exactly the bench's configuration (ss_block_size 102400, growth 1.05,
+    # queue 65536) with the bench's level capacities and the reference defaults
+    m, ref = lowerstar64_model1
+    p = Params(model=1, max_iteration=10, ss_block_size=102400, growth=1.05, queue_size=65536, level1_capacity=l1,
+               level2_capacity=l2)
+    pairs, ess, st = run(m, p)
+    assert np.array_equal(pairs, ref.pairs)
+    assert np.array_equal(ess, ref.essential)
+    assert st["highclear_cleared"] == ref.stats["highclear"]
+    assert st["active_after_init"] == ref.stats["active_after_init"]
+    assert 2 * len(pairs) + len(ess) == m.ncols

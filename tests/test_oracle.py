@@ -143,10 +143,11 @@ def test_collapse_keeps_homology_of_flag_complex():
     assert b0[0] == b2[0]
 
 
-REF_ALPHA = "/root/reference/data/Alpha"
+# the reference tree's root comes from SSPP_REFERENCE; the check is skipped without it
+REF_ALPHA = os.path.join(os.environ.get("SSPP_REFERENCE", "/nonexistent"), "data", "Alpha")
 
 
-@pytest.mark.skipif(not os.path.isdir(REF_ALPHA), reason="reference tree absent")
+@pytest.mark.skipif(not os.path.isdir(REF_ALPHA), reason="reference tree absent (set SSPP_REFERENCE)")
 def test_reference_highclear_artefacts_keep_the_pairs():
     # The reference's HIGHOUT build wrote each Alpha input again with its guided
     # clearing applied (cleared columns as dimension-only lines,
