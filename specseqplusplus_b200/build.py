@@ -36,15 +36,37 @@ def _stale(target, sources):
     return any(os.path.getmtime(s) > t for s in sources)
 
 
-def build(force: bool = False, verbose: bool = False) -> None:
+def _objects(srcs, headers, objdir, flags, force, verbose):
+    """Compiles each source to its own object in parallel (every object
+    depends on all headers); returns the object paths."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    os.makedirs(objdir, exist_ok=True)
+    jobs = []
+    for src in srcs:
+        obj = os.path.join(objdir, os.path.basename(src) + ".o")
+        if force or _stale(obj, [src] + headers):
+            jobs.append([NVCC] + flags + ["-c", "-o", obj, src])
+    with ThreadPoolExecutor(max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        for out in ex.map(_run, jobs):
+            if verbose:
+                print(out)
+    return [os.path.join(objdir, os.path.basename(s) + ".o") for s in srcs]
+
+
+def build_engine(lib: str, objdir: str, extra_flags=(), force: bool = False, verbose: bool = False) -> None:
+    """libsspp.so from per-file objects in objdir, compiled with NVFLAGS + extra_flags."""
     srcs = [os.path.join(CSRC, s) for s in ENGINE_SRC]
-    deps = srcs + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
-    deps.append(os.path.join(ROOT, "include", "sspp.h"))
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
+    headers.append(os.path.join(ROOT, "include", "sspp.h"))
+    objs = _objects(srcs, headers, objdir, NVFLAGS + list(extra_flags), force, verbose)
+    if force or _stale(lib, objs):
+        _run([NVCC] + ARCH + ["-shared", "-o", lib] + objs)
+
+
+def build(force: bool = False, verbose: bool = False) -> None:
     lib = os.path.join(HERE, "libsspp.so")
-    if force or _stale(lib, deps):
-        out = _run([NVCC] + NVFLAGS + ["-shared", "-o", lib] + srcs)
-        if verbose:
-            print(out)
+    build_engine(lib, os.path.join(HERE, "_build"), force=force, verbose=verbose)
     gen = os.path.join(HERE, "libsspp_gen.so")
     gsrc = [os.path.join(CSRC, "sspp_gen.cpp")]
     if force or _stale(gen, gsrc + [os.path.join(CSRC, "sspp_gen.h")]):

@@ -25,6 +25,8 @@
 // one w in C and counts its valid neighbours in C.
 #include <algorithm>
 #include <climits>
+#include <mutex>
+#include <type_traits>
 
 #include "sspp_collapse.h"
 #include "sspp_kernels.cuh"
@@ -50,21 +52,42 @@ unsigned grid_of(int64_t n, int threads, int64_t cap = 65536) {
 __device__ __forceinline__ int32_t key_nbr(uint64_t k) { return int32_t(k >> 32); }
 __device__ __forceinline__ int32_t key_edge(uint64_t k) { return int32_t(uint32_t(k)); }
 
+// Per-edge flags of the re-examinations (critical, in the pending set): one
+// byte per edge in global memory, or one bit per edge in shared memory when
+// the edge count allows (a bit test costs a shared-memory read instead of a
+// global one on the cascade's sequential path).  Only the cascade's one warp
+// writes them.
+struct FlagsG {
+    uint8_t* p;
+    __device__ __forceinline__ bool get(int32_t x) const { return p[x] != 0; }
+    __device__ __forceinline__ void set(int32_t x) const { p[x] = 1; }
+    __device__ __forceinline__ void clr(int32_t x) const { p[x] = 0; }
+};
+struct FlagsS {
+    uint32_t* w;
+    __device__ __forceinline__ bool get(int32_t x) const { return (w[x >> 5] >> (x & 31)) & 1u; }
+    __device__ __forceinline__ void set(int32_t x) const { atomicOr(w + (x >> 5), 1u << (x & 31)); }
+    __device__ __forceinline__ void clr(int32_t x) const { atomicAnd(w + (x >> 5), ~(1u << (x & 31))); }
+};
+
 // Edge x takes part in the test of edge e while edges 0..tcur have arrived:
 // it precedes e, or it is critical (crit == nullptr: an arrival test, where
 // only the edges before e have arrived).
-struct Valid {
+template <class F>
+struct ValidT {
     int32_t e, tcur;
-    const uint8_t* crit;
+    const F* crit;
     __device__ __forceinline__ bool operator()(int32_t x) const {
-        return x < e || (crit != nullptr && x <= tcur && crit[x] != 0);
+        return x < e || (crit != nullptr && x <= tcur && crit->get(x));
     }
 };
+using Valid = ValidT<FlagsG>;
 
 // Common neighbours w of u and v through valid edges, ascending.  The first
 // `cap` go to C (and the ids of edges uw, vw to ea, eb when given); returns
 // how many there are.
-__device__ int common_nbrs(const uint64_t* adj, const int64_t* off, int32_t u, int32_t v, const Valid& ok, int32_t* C,
+template <class V>
+__device__ int common_nbrs(const uint64_t* adj, const int64_t* off, int32_t u, int32_t v, const V& ok, int32_t* C,
                            int32_t* ea, int32_t* eb, int64_t cap) {
     const int lane = lane_id();
     int64_t a0 = off[u], a1 = off[u + 1], b0 = off[v], b1 = off[v + 1];
@@ -117,7 +140,8 @@ __device__ int common_nbrs(const uint64_t* adj, const int64_t* off, int32_t u, i
 
 // Some w in C (sorted, c >= 2) is adjacent through valid edges to every other
 // vertex of C.
-__device__ bool dominated_by_one(const uint64_t* adj, const int64_t* off, const Valid& ok, const int32_t* C, int c) {
+template <class V>
+__device__ bool dominated_by_one(const uint64_t* adj, const int64_t* off, const V& ok, const int32_t* C, int c) {
     const int lane = lane_id();
     bool any = false;
     for (int base = 0; base < c && !any; base += 32) {
@@ -347,7 +371,8 @@ __device__ __forceinline__ void pending_push(Pending& P, int32_t x) {
 // neighbours w, w' of u and v), then lane 0 pushes the ones taken, from
 // `list` (kCapB entries of shared memory; larger lists are pushed by lane 0
 // directly).
-__device__ void push_partners(const int32_t* A, const int32_t* B, int c, int32_t th, const uint8_t* crit, uint8_t* ins,
+template <class F>
+__device__ void push_partners(const int32_t* A, const int32_t* B, int c, int32_t th, const F& crit, const F& ins,
                               int32_t* list, Pending& P) {
     const int lane = lane_id();
     if (2 * c > kCapB) {
@@ -356,8 +381,8 @@ __device__ void push_partners(const int32_t* A, const int32_t* B, int c, int32_t
                 const int32_t ab[2] = {A[k], B[k]};
                 for (int q = 0; q < 2; q++) {
                     const int32_t x = ab[q];
-                    if (x < th && !crit[x] && !ins[x]) {
-                        ins[x] = 1;
+                    if (x < th && !crit.get(x) && !ins.get(x)) {
+                        ins.set(x);
                         pending_push(P, x);
                     }
                 }
@@ -373,12 +398,12 @@ __device__ void push_partners(const int32_t* A, const int32_t* B, int c, int32_t
         bool want = false;
         if (k < 2 * c) {
             x = k < c ? A[k] : B[k - c];
-            want = x < th && !crit[x] && !ins[x];
+            want = x < th && !crit.get(x) && !ins.get(x);
         }
         const unsigned bm = __ballot_sync(kFull, want);
         if (want) {
             list[m + __popc(bm & lanemask_lt())] = x;
-            ins[x] = 1;
+            ins.set(x);
         }
         m += __popc(bm);
     }
@@ -388,77 +413,138 @@ __device__ void push_partners(const int32_t* A, const int32_t* B, int c, int32_t
     __syncwarp();
 }
 
-// Re-examinations, in arrival order, by one warp.
-__global__ void __launch_bounds__(32) k_cascade(const int32_t* cas, int32_t* misc, const int32_t* eu, const int32_t* ev,
-                                               const uint64_t* adj, const int64_t* off, uint8_t* crit, uint8_t* ins,
-                                               int32_t* heap, const int32_t* open, const int8_t* nopen, int32_t* gC,
-                                               int32_t* gA, int32_t* gB, int64_t gcap, long long max_steps, int* err) {
+// Arrivals of the cascade list read ahead per round of one warp: the arrival,
+// its listed partner count and its partners.
+constexpr int kAhead = 32;
+
+// Re-examinations, in arrival order, by one warp (warp 0; with flags in shared
+// memory the block's other warps only help load the critical flags and exit).
+// The flags live in F (FlagsS: bitsets in dynamic shared memory, crit words
+// then pending words; FlagsG: the global byte arrays).  An edge the cascade
+// keeps is also marked in the global byte array, which k_drop_edges reads.
+template <class F>
+__global__ void __launch_bounds__(256) k_cascade(const int32_t* cas, int32_t* misc, const int32_t* eu,
+                                                  const int32_t* ev, const uint64_t* adj, const int64_t* off,
+                                                  uint8_t* crit_g, uint8_t* ins_g, int32_t* heap, const int32_t* open,
+                                                  const int8_t* nopen, int32_t* gC, int32_t* gA, int32_t* gB,
+                                                  int64_t gcap, long long max_steps, int* err) {
+    extern __shared__ uint32_t sbits[];
     __shared__ int32_t sC[kCapB], sA[kCapB], sB[kCapB];
     __shared__ int32_t sheap[kHeapS];
+    __shared__ int32_t s_t[kAhead], s_no[kAhead];
+    __shared__ int32_t s_open[kAhead][kOpen];
     const int lane = lane_id();
+    const int64_t E = misc[kMiscE];
+    F crit, ins;
+    if constexpr (std::is_same<F, FlagsS>::value) {
+        const int64_t nw = (E + 31) >> 5;
+        crit.w = sbits;
+        ins.w = sbits + nw;
+        for (int64_t k = threadIdx.x; k < nw; k += blockDim.x) {
+            uint32_t word = 0;
+            const int64_t e0 = 32 * k;
+            if (e0 + 32 <= E) {
+                const uint4* q = reinterpret_cast<const uint4*>(crit_g + e0);
+                const uint4 lo = q[0], hi = q[1];
+                const uint32_t parts[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
+#pragma unroll
+                for (int b = 0; b < 32; b++) word |= ((parts[b >> 2] >> (8 * (b & 3))) & 0xffu ? 1u : 0u) << b;
+            } else {
+                for (int64_t e = e0; e < E; e++) word |= (crit_g[e] ? 1u : 0u) << (e - e0);
+            }
+            sbits[k] = word;
+            sbits[nw + k] = 0;
+        }
+        __syncthreads();
+    } else {
+        crit.p = crit_g;
+        ins.p = ins_g;
+    }
+    if (threadIdx.x >= 32) return;
     const int ncas = misc[kMiscCascades];
     Pending P{sheap, kHeapS, 0, heap};  // kept by lane 0
     int size = 0;                        // P.size, broadcast
     long long steps = 0;
     bool fail = false;
-    for (int i = 0; i < ncas && !fail; i++) {
-        const int32_t t = cas[i];
-        const int no = nopen[t];
-        if (no >= 0) {  // the prefilter's list: edges before t, dominated at their own arrival
-            const int32_t x = lane < no ? open[int64_t(t) * kOpen + lane] : -1;
-            const bool want = lane < no && !crit[x] && !ins[x];
-            const unsigned bm = __ballot_sync(kFull, want);
-            if (want) {
-                sC[__popc(bm & lanemask_lt())] = x;
-                ins[x] = 1;
+    for (int i0 = 0; i0 < ncas && !fail; i0 += kAhead) {
+        const int nb = ncas - i0 < kAhead ? ncas - i0 : kAhead;
+        if (lane < nb) {  // read ahead: nothing here changes while the cascade runs
+            const int32_t t = cas[i0 + lane];
+            const int no = nopen[t];
+            s_t[lane] = t;
+            s_no[lane] = no;
+            if (no > 0) {
+                const int4* q = reinterpret_cast<const int4*>(open + int64_t(t) * kOpen);
+                const int4 a = q[0], b = q[1];
+                s_open[lane][0] = a.x; s_open[lane][1] = a.y; s_open[lane][2] = a.z; s_open[lane][3] = a.w;
+                s_open[lane][4] = b.x; s_open[lane][5] = b.y; s_open[lane][6] = b.z; s_open[lane][7] = b.w;
             }
-            __syncwarp();
-            if (lane == 0)
-                for (int j = 0; j < __popc(bm); j++) pending_push(P, sC[j]);
-            __syncwarp();
-            size = __shfl_sync(kFull, P.size, 0);
-        } else {
-            const Valid ok{t, t, nullptr};
-            int c = common_nbrs(adj, off, eu[t], ev[t], ok, sC, sA, sB, kCapB);
-            const int32_t *A = sA, *B = sB;
-            if (c > kCapB) {
-                common_nbrs(adj, off, eu[t], ev[t], ok, gC, gA, gB, gcap);
-                A = gA;
-                B = gB;
-            }
-            push_partners(A, B, c, t, crit, ins, sC, P);
-            size = __shfl_sync(kFull, P.size, 0);
         }
-        while (size > 0) {
-            if (++steps > max_steps) {
-                fail = true;
-                break;
+        __syncwarp();
+        for (int j = 0; j < nb && !fail; j++) {
+            const int32_t t = s_t[j];
+            const int no = s_no[j];
+            if (no >= 0) {  // the prefilter's list: edges before t, dominated at their own arrival
+                const int32_t x = lane < no ? s_open[j][lane] : -1;
+                const bool want = lane < no && !crit.get(x) && !ins.get(x);
+                const unsigned bm = __ballot_sync(kFull, want);
+                if (!bm) continue;  // nothing pushed, and the set is empty between arrivals
+                if (want) {
+                    sC[__popc(bm & lanemask_lt())] = x;
+                    ins.set(x);
+                }
+                __syncwarp();
+                if (lane == 0)
+                    for (int q = 0; q < __popc(bm); q++) pending_push(P, sC[q]);
+                __syncwarp();
+                size = __shfl_sync(kFull, P.size, 0);
+            } else {
+                const ValidT<F> ok{t, t, nullptr};
+                int c = common_nbrs(adj, off, eu[t], ev[t], ok, sC, sA, sB, kCapB);
+                const int32_t *A = sA, *B = sB;
+                if (c > kCapB) {
+                    common_nbrs(adj, off, eu[t], ev[t], ok, gC, gA, gB, gcap);
+                    A = gA;
+                    B = gB;
+                }
+                push_partners(A, B, c, t, crit, ins, sC, P);
+                size = __shfl_sync(kFull, P.size, 0);
             }
-            int32_t e = 0;
-            if (lane == 0) {
-                e = heap_pop(P.h, P.size);
-                ins[e] = 0;
+            while (size > 0) {
+                if (++steps > max_steps) {
+                    fail = true;
+                    break;
+                }
+                int32_t e = 0;
+                if (lane == 0) {
+                    e = heap_pop(P.h, P.size);
+                    ins.clr(e);
+                }
+                e = __shfl_sync(kFull, e, 0);
+                size = __shfl_sync(kFull, P.size, 0);
+                __syncwarp();
+                if (crit.get(e)) continue;
+                const ValidT<F> ok{e, t, &crit};
+                int c = common_nbrs(adj, off, eu[e], ev[e], ok, sC, sA, sB, kCapB);
+                const int32_t *C = sC, *A = sA, *B = sB;
+                if (c > kCapB) {
+                    common_nbrs(adj, off, eu[e], ev[e], ok, gC, gA, gB, gcap);
+                    C = gC;
+                    A = gA;
+                    B = gB;
+                }
+                const bool dom = (c == 1) || (c >= 2 && dominated_by_one(adj, off, ok, C, c));
+                if (dom) continue;
+                if (lane == 0) {
+                    crit.set(e);
+                    crit_g[e] = 1;
+                }
+                __syncwarp();
+                push_partners(A, B, c, e, crit, ins, sC, P);
+                size = __shfl_sync(kFull, P.size, 0);
             }
-            e = __shfl_sync(kFull, e, 0);
-            size = __shfl_sync(kFull, P.size, 0);
-            __syncwarp();
-            if (crit[e]) continue;
-            const Valid ok{e, t, crit};
-            int c = common_nbrs(adj, off, eu[e], ev[e], ok, sC, sA, sB, kCapB);
-            const int32_t *C = sC, *A = sA, *B = sB;
-            if (c > kCapB) {
-                common_nbrs(adj, off, eu[e], ev[e], ok, gC, gA, gB, gcap);
-                C = gC;
-                A = gA;
-                B = gB;
-            }
-            const bool dom = (c == 1) || (c >= 2 && dominated_by_one(adj, off, ok, C, c));
-            if (dom) continue;
-            if (lane == 0) crit[e] = 1;
-            __syncwarp();
-            push_partners(A, B, c, e, crit, ins, sC, P);
-            size = __shfl_sync(kFull, P.size, 0);
         }
+        __syncwarp();  // s_t / s_no / s_open are rewritten by the next round
     }
     if (lane == 0) {
         misc[kMiscSteps] = int32_t(steps > INT_MAX ? INT_MAX : steps);
@@ -498,6 +584,31 @@ __global__ void k_empty_dropped(int64_t n, int32_t* arena, uint64_t* desc, const
     }
     cnt = warp_sum(cnt);
     if ((threadIdx.x & 31) == 0 && cnt) cnt_add(&counters[CNT_DROPPED], cnt);
+}
+
+// Dynamic shared memory the bitset cascade may take on this device (the
+// opt-in maximum less its static buffers), raised once per device.
+size_t cascade_shared_limit() {
+    static std::mutex mu;
+    static int limit[64] = {};
+    static bool done[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!done[dev]) {
+        int optin = 0;
+        cudaFuncAttributes fa{};
+        if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) == cudaSuccess &&
+            cudaFuncGetAttributes(&fa, k_cascade<FlagsS>) == cudaSuccess && optin > int(fa.sharedSizeBytes)) {
+            const int want = optin - int(fa.sharedSizeBytes);
+            if (cudaFuncSetAttribute(k_cascade<FlagsS>, cudaFuncAttributeMaxDynamicSharedMemorySize, want) ==
+                cudaSuccess)
+                limit[dev] = want;
+        }
+        cudaGetLastError();
+        done[dev] = true;
+    }
+    return size_t(limit[dev]);
 }
 
 // stream-ordered, like the engine's other buffers
@@ -615,13 +726,23 @@ int collapse(Device& D, const DimInfo& info, uint8_t* dropped, CollapseScratch& 
     }
     // count of arrivals with re-examinations (fits in int32: E does)
     cudaMemcpyAsync(S.misc + kMiscCascades, D.blk + scan_blocks(E), sizeof(int32_t), cudaMemcpyDeviceToDevice, s);
-    cudaMemsetAsync(S.ins, 0, size_t(E), s);
     // every pop either keeps an edge (at most E times) or discards one inserted
     // by a kept edge's triangles; the bound only guards against a corrupted set
     const double bound = 64.0 * double(E) * double(maxdeg + 1) + double(1 << 20);
     const long long max_steps = bound > 4.0e18 ? (long long)4e18 : (long long)bound;
-    k_cascade<<<1, 32, 0, s>>>(S.cas, S.misc, S.eu, S.ev, S.adj, S.adj_off, S.crit, S.ins, S.heap, S.open, S.nopen,
-                               S.cbuf, S.cbuf + gcap, S.cbuf + 2 * gcap, gcap, max_steps, D.err);
+    // flags as shared-memory bitsets while they fit next to the kernel's
+    // static buffers, else the global byte arrays
+    const size_t bits_bytes = size_t(2) * size_t((E + 31) >> 5) * sizeof(uint32_t);
+    if (bits_bytes <= cascade_shared_limit()) {
+        k_cascade<FlagsS><<<1, 256, bits_bytes, s>>>(S.cas, S.misc, S.eu, S.ev, S.adj, S.adj_off, S.crit, S.ins,
+                                                      S.heap, S.open, S.nopen, S.cbuf, S.cbuf + gcap,
+                                                      S.cbuf + 2 * gcap, gcap, max_steps, D.err);
+    } else {
+        cudaMemsetAsync(S.ins, 0, size_t(E), s);
+        k_cascade<FlagsG><<<1, 32, 0, s>>>(S.cas, S.misc, S.eu, S.ev, S.adj, S.adj_off, S.crit, S.ins, S.heap,
+                                           S.open, S.nopen, S.cbuf, S.cbuf + gcap, S.cbuf + 2 * gcap, gcap,
+                                           max_steps, D.err);
+    }
     k_drop_edges<<<grid_of(E, 256), 256, 0, s>>>(S.misc, S.crit, S.ecol, dropped);
     launches += 7;
     for (int d = 2; d <= kMaxDim; d++) {

@@ -540,7 +540,10 @@ int run_steps(sspp_ctx* ctx, const std::vector<Step>& steps, int cap1, int cap2,
     const int light_max = std::max(1, ctx->num_sms * ctx->light_blocks_per_sm);
     const int heavy_grid = std::max(1, std::min(ctx->num_sms * ctx->heavy_blocks_per_sm, 2 * ctx->num_sms));
     const int q_blocks = std::max(1, (P.queue_size + 3) / 4);
-    const int chunk = 8;
+#ifndef SSPP_LIGHT_CHUNK
+#define SSPP_LIGHT_CHUNK 8
+#endif
+    const int chunk = SSPP_LIGHT_CHUNK;  // window entries a warp takes per fetch
     // Heavy launches go to side streams (round robin) after their light step:
     // they overlap the following light steps and each other, so long chains of
     // different steps run concurrently.  Each dimension's completion sweep, and

@@ -586,6 +586,23 @@ __device__ int fold_delta(int32_t* a, int nb, int dv, int d, int32_t* tmp, int* 
     return nn;
 }
 
+// Runs of additions.  Lane j keeps the bulk entry a[cb-1-j] (cb: the bulk
+// length when the cache was filled) and that row's inline apparent column, all
+// loaded at once.  While the current low is the bulk top at cache lane h and
+// its owner is an inline apparent column, the additions of the bulk rows at
+// lanes h, h+1, ... follow one another without a look at the column: row
+// r_{i+1} is the next low after the additions of r_h..r_i exactly when every
+// entry those addends toggle, and the delta's top, lie below r_{i+1} (equal
+// would cancel it).  Such a run removes its rows from the bulk top at once and
+// toggles the addends' other entries into the delta; no dependent load waits
+// between its additions.
+constexpr int kCacheRefill = 16;  // cache lanes used before the cache is filled again
+
+// largest entry of an inline apparent column below its top (-1 if none)
+__device__ __forceinline__ int app_max_below(int4 q) {
+    return q.x <= 0 ? -1 : (q.x == 1 ? q.y : (q.x == 2 ? q.z : q.w));
+}
+
 template <int T>
 __device__ int fast_adds(const BlockG<T>& g, const ReduceArgs& A, int col, Work& w, int& L, uint64_t& e,
                          int32_t* tmp, int32_t* sb, long long& adds, long long& add_ints, int iters_left) {
@@ -602,15 +619,134 @@ __device__ int fast_adds(const BlockG<T>& g, const ReduceArgs& A, int col, Work&
         uint64_t ec = e;
         long long ai = 0;
         int n_inline = 0;
-        // inline copy of the current row's apparent column, if it has one
-        int4 ap = make_int4(-1, 0, 0, 0);
-        if (lane == 31 && Lc >= 0 && Lc < A.ncols) ap = __ldg(A.app + Lc);
-        ap.x = __shfl_sync(kFull, ap.x, 31);
-        ap.y = __shfl_sync(kFull, ap.y, 31);
-        ap.z = __shfl_sync(kFull, ap.z, 31);
-        ap.w = __shfl_sync(kFull, ap.w, 31);
+        // bulk cache: lane j holds cr = a[cb - 1 - j] and its inline apparent column ca
+        int cb = -1;
+        int cr = -1;
+        int4 ca = make_int4(-1, 0, 0, 0);
         bool have_e = true;  // ec is the pivot entry of Lc
+        // toggles x in the delta (a fold into the bulk when the delta is full
+        // invalidates the bulk cache)
+        auto toggle = [&](int x) {
+            const unsigned eq = __ballot_sync(kFull, lane < d && dv == x);
+            if (eq) {
+                const int q = __ffs(eq) - 1;
+                const int nx = __shfl_down_sync(kFull, dv, 1);
+                if (lane >= q) dv = lane + 1 < d ? nx : INT_MAX;
+                d--;
+            } else {
+                if (d == 32) {  // full: the bulk absorbs the delta
+                    nb = fold_delta(a, nb, dv, d, tmp, A.err);
+                    d = 0;
+                    dv = INT_MAX;
+                    cb = -1;
+                }
+                const int q = __popc(__ballot_sync(kFull, lane < d && dv < x));
+                const int pv = __shfl_up_sync(kFull, dv, 1);
+                if (lane > q && lane <= d) dv = pv;
+                if (lane == q) dv = x;
+                d++;
+            }
+        };
         while (done < iters_left && nb + d > 0 && Lc >= A.minrow) {
+            // the inline apparent column of the current low: from the bulk
+            // cache when the low is the bulk top, else one load
+            int4 ap;
+            int h = -1;
+            if (top_in_bulk) {
+                if (cb < 0 || cb - nb >= kCacheRefill) {
+                    cb = nb;
+                    const int idx = nb - 1 - lane;
+                    cr = idx >= 0 ? lds(a + idx) : -1;
+                    ca = (cr >= 0 && cr < A.ncols) ? __ldg(A.app + cr) : make_int4(-1, 0, 0, 0);
+                }
+                h = cb - nb;
+                ap.x = __shfl_sync(kFull, ca.x, h);
+                ap.y = __shfl_sync(kFull, ca.y, h);
+                ap.z = __shfl_sync(kFull, ca.z, h);
+                ap.w = __shfl_sync(kFull, ca.w, h);
+                if (__shfl_sync(kFull, cr, h) != Lc) {  // self-check: the cache lane holds the bulk top
+                    bad = 1;
+                    break;
+                }
+            } else {
+                ap = make_int4(-1, 0, 0, 0);
+                if (lane == 31 && Lc >= 0 && Lc < A.ncols) ap = __ldg(A.app + Lc);
+                ap.x = __shfl_sync(kFull, ap.x, 31);
+                ap.y = __shfl_sync(kFull, ap.y, 31);
+                ap.z = __shfl_sync(kFull, ap.z, 31);
+                ap.w = __shfl_sync(kFull, ap.w, 31);
+            }
+            if (top_in_bulk && ap.x >= 0) {
+                // a run from cache lane h: lane l (> h) joins while lanes h..l-1
+                // all joined, its row has an inline apparent column, and the
+                // delta top and every entry the run toggled so far lie below it
+                const int td = d > 0 ? __shfl_sync(kFull, dv, d - 1) : -1;
+                const bool mine = lane >= h && cr >= 0 && ca.x >= 0;
+                int mx = mine ? app_max_below(ca) : -1;
+                mx = mx > td ? mx : td;
+                int M = mx;  // inclusive prefix max over lanes h..lane
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int t = __shfl_up_sync(kFull, M, o);
+                    if (lane >= o && lane - o >= h) M = t > M ? t : M;
+                }
+                const int mprev = __shfl_up_sync(kFull, M, 1);   // prefix max up to lane - 1
+                const int mcnt = mine ? ca.x : 0;
+                // entries toggled by lanes h..lane (inclusive), for the capacity bound
+                int csum = mcnt;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int t = __shfl_up_sync(kFull, csum, o);
+                    if (lane >= o && lane - o >= h) csum += t;
+                }
+                const bool join = lane == h || (lane > h && mine && mprev < cr);
+                const bool fits = nb + d + csum <= A.cap && lane - h < iters_left - done;
+                const unsigned stop = __ballot_sync(kFull, lane >= h && !(join && fits));
+                // lanes h .. first stopping lane - 1 form the run; lane h always
+                // joins, so the run is empty only when lane h does not fit
+                const unsigned above = stop & (kFull << h);
+                const int end = above ? __ffs(above) - 1 : 32;
+                const int P = end - h;
+                if (P > 0) {
+                    const int rlast = __shfl_sync(kFull, cr, end - 1);
+                    nb -= P;
+                    for (int i = h; i < end; i++) {
+                        const int qx = __shfl_sync(kFull, ca.x, i);
+                        const int qy = __shfl_sync(kFull, ca.y, i);
+                        const int qz = __shfl_sync(kFull, ca.z, i);
+                        const int qw = __shfl_sync(kFull, ca.w, i);
+                        if (qx > 0) toggle(qy);
+                        if (qx > 1) toggle(qz);
+                        if (qx > 2) toggle(qw);
+                        ai += 2 * (nb + d) + qx + 2;
+                    }
+                    done += P;
+                    n_inline += P;
+                    // the next lowest row: the larger top; equal tops cancel
+                    int nl = -1;
+                    while (true) {
+                        const int tb = nb > 0 ? lds(a + nb - 1) : -1;
+                        const int tdd = d > 0 ? __shfl_sync(kFull, dv, d - 1) : -1;
+                        if (tb >= 0 && tb == tdd) {
+                            nb--;
+                            d--;
+                            if (lane == d) dv = INT_MAX;
+                            continue;
+                        }
+                        top_in_bulk = tb > tdd;
+                        nl = top_in_bulk ? tb : tdd;
+                        break;
+                    }
+                    if (nl >= rlast || nl >= A.ncols) {  // self-check: the lowest row only moves down
+                        bad = 1;
+                        break;
+                    }
+                    Lc = nl;
+                    have_e = false;
+                    ec = kNoOwner;  // unknown; the general path's claim retries with the real entry
+                    continue;
+                }
+            }
             int plen, bj;
             if (ap.x >= 0) {  // apparent owner: permanent, its entries are at hand
                 plen = ap.x + 1;
@@ -640,27 +776,7 @@ __device__ int fast_adds(const BlockG<T>& g, const ReduceArgs& A, int col, Work&
                 if (lane == d) dv = INT_MAX;
             }
             // toggle the addend's other entries in the delta
-            for (int j = 0; j < m; j++) {
-                const int x = __shfl_sync(kFull, bj, j);
-                const unsigned eq = __ballot_sync(kFull, lane < d && dv == x);
-                if (eq) {
-                    const int q = __ffs(eq) - 1;
-                    const int nx = __shfl_down_sync(kFull, dv, 1);
-                    if (lane >= q) dv = lane + 1 < d ? nx : INT_MAX;
-                    d--;
-                } else {
-                    if (d == 32) {  // full: the bulk absorbs the delta
-                        nb = fold_delta(a, nb, dv, d, tmp, A.err);
-                        d = 0;
-                        dv = INT_MAX;
-                    }
-                    const int q = __popc(__ballot_sync(kFull, lane < d && dv < x));
-                    const int pv = __shfl_up_sync(kFull, dv, 1);
-                    if (lane > q && lane <= d) dv = pv;
-                    if (lane == q) dv = x;
-                    d++;
-                }
-            }
+            for (int j = 0; j < m; j++) toggle(__shfl_sync(kFull, bj, j));
             // the next lowest row: the larger top; equal tops cancel
             int nl = -1;
             while (true) {
@@ -684,12 +800,6 @@ __device__ int fast_adds(const BlockG<T>& g, const ReduceArgs& A, int col, Work&
                 break;
             }
             Lc = nl;
-            ap = make_int4(-1, 0, 0, 0);
-            if (lane == 31 && Lc >= 0 && Lc >= A.minrow) ap = __ldg(A.app + Lc);
-            ap.x = __shfl_sync(kFull, ap.x, 31);
-            ap.y = __shfl_sync(kFull, ap.y, 31);
-            ap.z = __shfl_sync(kFull, ap.z, 31);
-            ap.w = __shfl_sync(kFull, ap.w, 31);
             have_e = false;
             ec = kNoOwner;  // unknown; the general path's claim retries with the real entry
         }
@@ -1104,7 +1214,10 @@ int heavy_smem_bytes(int cap) { return (3 * cap + kHdr) * 4; }
 // lasts as long as its longest chain, while CTA-tier launches overlap later
 // steps on side streams.  Handing chains over while the window still has work
 // would only move parallel work onto the (fewer) CTAs.
-constexpr int32_t kLightChain = 16;
+#ifndef SSPP_LIGHT_CHAIN
+#define SSPP_LIGHT_CHAIN 8
+#endif
+constexpr int32_t kLightChain = SSPP_LIGHT_CHAIN;
 
 static ReduceArgs make_args(const Device& D, const int32_t* active, int32_t beg, int32_t end, int32_t minrow, int cap,
                             int chunk, int* ctr) {
