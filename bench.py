@@ -139,9 +139,17 @@ def reference_arm(args):
     rank, world, _ = dist_info()
     if rank != 0:
         return 0
-    from specseqplusplus_b200 import gen
+    # the input is built with numpy (same sizes and value distribution as the
+    # engine's generator), so this arm loads none of the engine's libraries
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import lowerstar_np
 
-    m = gen.lowerstar(GRID, SIGMA, SEED)
+    class _M:
+        pass
+
+    m = _M()
+    m.dims, m.col_ptr, m.rows = lowerstar_np.lowerstar(GRID, SIGMA, SEED)
+    m.ncols, m.nnz = int(m.dims.shape[0]), int(m.rows.shape[0])
     for _ in range(args.warmup):
         oracle_run(m)
     times = []
@@ -150,7 +158,8 @@ def reference_arm(args):
         times.append(dt)
     total = sum(times)
     value = m.ncols * len(times) / total
-    sample = f"full workload ({m.ncols} columns) per step, single-threaded C++ restatement (oracle/sspp_oracle.cpp)"
+    sample = (f"full workload ({m.ncols} columns, built with numpy: oracle/lowerstar_np.py) per step, "
+              f"single-threaded C++ restatement (oracle/sspp_oracle.cpp)")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / len(times),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
@@ -361,6 +370,15 @@ def leg_served(count=48, rates=(100.0, None)):
                              "plain_cols_per_s": cp, "plain_p50_ms": float(lp[0]), "plain_p95_ms": float(lp[1]),
                              "plain_p99_ms": float(lp[2]), "speedup_vs_plain": st["cols_per_s"] / cp,
                              "results_equal_plain": bool(same)})
+    # the serial loop's results (which every served result equals) against the
+    # oracle on a sample: every 6th request by size, up to 5 M columns each
+    orc = oracle_module()
+    by_size = sorted(range(count), key=lambda i: mats[i].ncols)
+    sample = [i for i in by_size[::6] if mats[i].ncols <= 5_000_000]
+    out["plain_vs_oracle"] = {"sample": f"{len(sample)} of {count} requests (every 6th by size, <= 5 M columns)",
+                              "exact": bool(all(np.array_equal(plain_results[i][0], r.pairs) and
+                                                np.array_equal(plain_results[i][1], r.essential)
+                                                for i, r in ((i, orc.reduce(mats[i])) for i in sample)))}
     out["built"] = served_built(stream, N, plain_results)
     return out
 

@@ -41,6 +41,9 @@ typedef struct sspp_config {
     int32_t verbose;         /* 0 = silent                                           */
     int32_t profile;         /* 1 = time every device phase with CUDA events         */
     int32_t host_threads;    /* host threads for staged copies; 0 = all cores         */
+    int32_t sm_share;        /* persistent reduction launches use 1/sm_share of the
+                                GPU (contexts that run side by side, e.g. a server's
+                                workers); 0 or 1 = the whole GPU                     */
 } sspp_config;
 
 /* The reference's 12 positional CLI values (src/main.cu:281-294) minus file
@@ -67,6 +70,12 @@ typedef struct sspp_params {
     int32_t representatives;  /* 1: keep whole reduced columns so that sspp_representative
                                  can return each pair's cycle (dualize 0 only; skips the
                                  negative-row compression, so the reduction does more work) */
+    int32_t schedule;         /* how the spectral-sequence blocks are driven: 1 a host
+                                 loop of per-block launches (as the reference's
+                                 GPU_Compute); 2 one persistent launch draining a device
+                                 queue of (complex, block) items, each complex with its
+                                 own block order and dimension gate; 0 = 1.  The
+                                 pairs are the same either way */
 } sspp_params;
 
 /* Per-run counters (device-side counters plus host timings). */
@@ -104,7 +113,7 @@ void sspp_destroy(sspp_ctx* ctx);
 const char* sspp_last_error(const sspp_ctx* ctx);
 /* Fills *p with the reference's defaults (README.md:26-51): no dualize,
  * model 0, max_iteration 0, ss_block_size 102400, growth 1.05,
- * queue_size 65536, level capacities 1000 / 8000. */
+ * queue_size 65536, level capacities 1000 / 8000 (and schedule 0). */
 void sspp_default_params(sspp_params* p);
 
 /* Replaces: processFiles (src/main.cu:90-167).  fmt = SSPP_ASCII / SSPP_BINARY.
@@ -146,6 +155,30 @@ int32_t sspp_load_rips(sspp_ctx* ctx, int64_t npts, int32_t space_dim, const flo
  * v.  -0 is read as +0; NaN is BAD_INPUT.  Every simplex up to maxdim (<= 3). */
 int32_t sspp_load_lowerstar(sspp_ctx* ctx, int64_t gx, int64_t gy, int64_t gz, const float* values,
                             int32_t maxdim);
+
+/* A complex to build on the device: a point cloud's Vietoris-Rips complex
+ * (kind SSPP_BUILD_RIPS: size[0] points of size[1] coordinates in `data`,
+ * `radius`) or a grid field's lower-star filtration (SSPP_BUILD_LOWERSTAR:
+ * size[0] x size[1] x size[2] values in `data`), each as sspp_load_rips /
+ * sspp_load_lowerstar describe; `data` in host memory or in device memory of
+ * the context's device. */
+#define SSPP_BUILD_RIPS 0
+#define SSPP_BUILD_LOWERSTAR 1
+typedef struct sspp_build_spec {
+    int32_t kind;
+    int32_t maxdim;
+    int64_t size[3];
+    const float* data;
+    float radius;
+} sspp_build_spec;
+
+/* Builds k complexes on the device, one after another, and loads them as one
+ * batch (as sspp_load_batch_device: block-diagonal, results per complex in
+ * its own indices).  No counterpart in the reference, which reads one file per
+ * process.  sspp_batch_values copies complex i's column filtration values and
+ * returns its column count (-1 on error). */
+int32_t sspp_load_built_batch(sspp_ctx* ctx, int32_t k, const sspp_build_spec* specs);
+int64_t sspp_batch_values(sspp_ctx* ctx, int32_t i, float* out, int64_t cap);
 
 /* The matrix the context reduces (after any load; a batch's is the block-
  * diagonal concatenation) and, after sspp_load_rips / sspp_load_lowerstar,
@@ -304,9 +337,11 @@ const char* sspp_server_last_error(sspp_server* srv);
 int64_t sspp_server_submit(sspp_server* srv, int64_t ncols, const int32_t* dims, const int64_t* col_ptr,
                            const int32_t* rows, int32_t flags);
 /* A request given as a point cloud or a scalar field (as sspp_load_rips /
- * sspp_load_lowerstar): the worker builds the complex on the device and
- * reduces it alone (not batched with others); its pairs and essentials are
- * indices of the built matrix, whose column values sspp_server_values returns
+ * sspp_load_lowerstar): a worker builds the point-cloud and field requests it
+ * takes together on the device, one after another, and reduces them as one
+ * block-diagonal batch (sspp_load_built_batch; matrices and built requests are
+ * never mixed in a batch); a request's pairs and essentials are
+ * indices of its built matrix, whose column values sspp_server_values returns
  * when submitted with SSPP_SUBMIT_VALUES.  A field's request is admitted by an
  * upper bound of its size (26 columns and 74 entries per vertex); a point
  * cloud's size is known only once built, and one that does not fit the

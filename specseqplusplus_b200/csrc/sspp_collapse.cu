@@ -172,6 +172,114 @@ __device__ bool dominated_by_one(const uint64_t* adj, const int64_t* off, const 
     return any;
 }
 
+// The same two tests for the cascade's single warp, with fewer dependent
+// global loads: common_nbrs_s first copies the longer neighbour list into
+// shared memory (one coalesced pass; lists longer than `slcap` take the global
+// form), and dominated_by_one_s spreads the (w in C, neighbour of w) pairs over
+// the lanes, so every lane loads independent entries instead of walking one
+// list (C of at most 32 vertices; larger ones take the global form).
+template <class V>
+__device__ int common_nbrs_s(const uint64_t* adj, const int64_t* off, int32_t u, int32_t v, const V& ok, int32_t* C,
+                             int32_t* ea, int32_t* eb, int64_t cap, uint64_t* sl, int slcap) {
+    const int lane = lane_id();
+    int64_t a0 = off[u], a1 = off[u + 1], b0 = off[v], b1 = off[v + 1];
+    if (a1 - a0 > b1 - b0) {  // walk the shorter list
+        int64_t x = a0; a0 = b0; b0 = x;
+        x = a1; a1 = b1; b1 = x;
+    }
+    const int nb = int(b1 - b0);
+    if (b1 - b0 > slcap) return common_nbrs(adj, off, u, v, ok, C, ea, eb, cap);
+    for (int i = lane; i < nb; i += 32) sl[i] = adj[b0 + i];
+    __syncwarp();
+    int count = 0;
+    for (int64_t base = a0; base < a1; base += 32) {
+        const int64_t i = base + lane;
+        bool hit = false;
+        int32_t w = 0, e1 = 0, e2 = 0;
+        if (i < a1) {
+            const uint64_t k = adj[i];
+            w = key_nbr(k);
+            e1 = key_edge(k);
+            if (ok(e1)) {
+                const uint64_t target = uint64_t(uint32_t(w)) << 32;
+                int lo = 0, hi = nb;
+                while (lo < hi) {
+                    const int mid = (lo + hi) >> 1;
+                    if (sl[mid] < target) lo = mid + 1;
+                    else hi = mid;
+                }
+                if (lo < nb) {
+                    const uint64_t k2 = sl[lo];
+                    if (key_nbr(k2) == w) {
+                        e2 = key_edge(k2);
+                        hit = ok(e2);
+                    }
+                }
+            }
+        }
+        const unsigned m = __ballot_sync(kFull, hit);
+        if (hit) {
+            const int p = count + __popc(m & lanemask_lt());
+            if (p < cap) {
+                C[p] = w;
+                if (ea) {
+                    ea[p] = e1;
+                    eb[p] = e2;
+                }
+            }
+        }
+        count += __popc(m);
+    }
+    __syncwarp();  // sl is rewritten by the next call
+    return count;
+}
+
+template <class V>
+__device__ bool dominated_by_one_s(const uint64_t* adj, const int64_t* off, const V& ok, const int32_t* C, int c,
+                                   int32_t* spre, int64_t* sbase, int32_t* scnt) {
+    if (c > 32) return dominated_by_one(adj, off, ok, C, c);
+    const int lane = lane_id();
+    int deg = 0;
+    if (lane < c) {
+        const int32_t w = C[lane];
+        const int64_t s0 = off[w], s1 = off[w + 1];
+        deg = s1 - s0 >= c - 1 ? int(s1 - s0) : 0;  // fewer neighbours than c - 1: cannot dominate
+        sbase[lane] = s0;
+        scnt[lane] = 0;
+    }
+    const int inc = warp_inclusive_scan(deg);
+    const int tot = __shfl_sync(kFull, inc, 31);
+    spre[lane] = inc - deg;
+    __syncwarp();
+    for (int base = 0; base < tot; base += 32) {
+        const int p = base + lane;
+        if (p < tot) {
+            int lo = 0, hi = c - 1;  // the last k with spre[k] <= p
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (spre[mid] <= p) lo = mid;
+                else hi = mid - 1;
+            }
+            const uint64_t key = adj[sbase[lo] + (p - spre[lo])];
+            if (ok(key_edge(key))) {
+                const int32_t x = key_nbr(key);
+                int a = 0, b = c;
+                while (a < b) {
+                    const int mid = (a + b) >> 1;
+                    if (C[mid] < x) a = mid + 1;
+                    else b = mid;
+                }
+                if (a < c && C[a] == x) atomicAdd(scnt + lo, 1);
+            }
+        }
+    }
+    __syncwarp();
+    const bool dom = lane < c && scnt[lane] >= c - 1;
+    const bool any = __any_sync(kFull, dom);
+    __syncwarp();  // the scratch is rewritten by the next call
+    return any;
+}
+
 __global__ void k_cdeg(const int32_t* misc, const int32_t* eu, const int32_t* ev, int32_t* deg) {
     const int64_t E = misc[kMiscE];
     for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < E; e += int64_t(gridDim.x) * blockDim.x) {
@@ -416,6 +524,7 @@ __device__ void push_partners(const int32_t* A, const int32_t* B, int c, int32_t
 // Arrivals of the cascade list read ahead per round of one warp: the arrival,
 // its listed partner count and its partners.
 constexpr int kAhead = 32;
+constexpr int kListS = 512;  // neighbour-list entries the cascade stages in shared memory
 
 // Re-examinations, in arrival order, by one warp (warp 0; with flags in shared
 // memory the block's other warps only help load the critical flags and exit).
@@ -433,6 +542,9 @@ __global__ void __launch_bounds__(256) k_cascade(const int32_t* cas, int32_t* mi
     __shared__ int32_t sheap[kHeapS];
     __shared__ int32_t s_t[kAhead], s_no[kAhead];
     __shared__ int32_t s_open[kAhead][kOpen];
+    __shared__ uint64_t s_list[kListS];
+    __shared__ int64_t s_base[32];
+    __shared__ int32_t s_pre[32], s_cnt[32];
     const int lane = lane_id();
     const int64_t E = misc[kMiscE];
     F crit, ins;
@@ -525,7 +637,7 @@ __global__ void __launch_bounds__(256) k_cascade(const int32_t* cas, int32_t* mi
                 __syncwarp();
                 if (crit.get(e)) continue;
                 const ValidT<F> ok{e, t, &crit};
-                int c = common_nbrs(adj, off, eu[e], ev[e], ok, sC, sA, sB, kCapB);
+                int c = common_nbrs_s(adj, off, eu[e], ev[e], ok, sC, sA, sB, kCapB, s_list, kListS);
                 const int32_t *C = sC, *A = sA, *B = sB;
                 if (c > kCapB) {
                     common_nbrs(adj, off, eu[e], ev[e], ok, gC, gA, gB, gcap);
@@ -533,7 +645,7 @@ __global__ void __launch_bounds__(256) k_cascade(const int32_t* cas, int32_t* mi
                     A = gA;
                     B = gB;
                 }
-                const bool dom = (c == 1) || (c >= 2 && dominated_by_one(adj, off, ok, C, c));
+                const bool dom = (c == 1) || (c >= 2 && dominated_by_one_s(adj, off, ok, C, c, s_pre, s_base, s_cnt));
                 if (dom) continue;
                 if (lane == 0) {
                     crit.set(e);

@@ -62,7 +62,7 @@ struct sspp_ctx {
     std::string err;
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
-    static constexpr int kSide = 16;
+    static constexpr int kSide = 32;
     cudaStream_t side[kSide] = {};     // heavy-tier launches overlap later light steps and each other
     std::vector<cudaEvent_t> step_ev;  // light step k done
     cudaEvent_t join_ev[kSide] = {};   // side stream joins
@@ -106,6 +106,9 @@ struct sspp_ctx {
     CollapseScratch cs;
     BuildScratch bs;               // device complex builders (the input matrix when `built`)
     bool built = false;
+    float* bvalues = nullptr;      // a built batch's column values, complex after complex
+    int64_t cap_bvalues = 0;
+    bool built_batch = false;      // the loaded matrix is a built batch (values in bvalues)
     double build_ms = 0;
     Prof prof;
     double ph_ms[PH_NUM] = {};
@@ -120,6 +123,26 @@ struct sspp_ctx {
     std::vector<int64_t> batch_bounds; // per-complex pair and essential slice starts
     bool host_ess_valid = false;
     int64_t launches = 0, light_launches = 0, heavy_launches = 0;
+    // device work queue of (complex, block) items (schedule 2)
+    int32_t* q_info = nullptr;     // 3 * k * kNumDims: active counts, min rows, max rows per complex and dimension
+    int64_t cap_q_info = 0;
+    QItem* q_items = nullptr;
+    int64_t cap_q_items = 0;
+    int* q_ctr = nullptr;          // taken, done, lin per item
+    int64_t cap_q_ctr = 0;
+    int32_t* q_cplx = nullptr;     // cur, gate, hpend, item_end, list_cap per complex + 8 scalars
+    int64_t cap_q_cplx = 0;
+    int64_t* q_loff = nullptr;     // list offsets per complex
+    int64_t cap_q_loff = 0;
+    int2* q_lists = nullptr;
+    int64_t cap_q_lists = 0;
+    int32_t* q_pool_c = nullptr;
+    int64_t cap_q_pool_c = 0;
+    int64_t* q_cstart = nullptr;   // {0, n} when the context holds one complex
+    int queue_bpsm = -1;           // queue kernel blocks per SM for q_conf's capacities and threads
+    int q_conf[3] = {-1, -1, -1};
+    std::vector<int32_t> h_qinfo;
+    std::vector<QItem> h_items;
 };
 
 namespace {
@@ -278,6 +301,7 @@ int check_params(sspp_ctx* ctx, const sspp_params* p) {
         return set_err(ctx, SSPP_ERR_BAD_INPUT, "representatives must be 0 or 1");
     if (p->representatives && p->dualize)
         return set_err(ctx, SSPP_ERR_BAD_INPUT, "representatives need dualize 0 (the dual reduces cocycles)");
+    if (p->schedule < 0 || p->schedule > 2) return set_err(ctx, SSPP_ERR_BAD_INPUT, "schedule must be 0, 1 or 2");
     return SSPP_OK;
 }
 
@@ -425,7 +449,10 @@ int run_init(sspp_ctx* ctx) {
     CK(cudaMemcpyAsync(ctx->h_err, D.err, sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     if (*ctx->h_err) return set_err(ctx, SSPP_ERR_BAD_INPUT, "dimension out of range 0..7 or malformed col_ptr");
-    ctx->launches += reorder(D, s);
+    // the reorder also does the first init pass unless an edge collapse will
+    // empty columns in between (the autotuner never changes the model)
+    const bool lows_in_reorder = !(ctx->params.model & 2);
+    ctx->launches += reorder(D, lows_in_reorder, s);
     CK(cudaMemcpyAsync(D.arena_top, D.blk + reorder_total_slot(D), sizeof(unsigned long long),
                        cudaMemcpyDeviceToDevice, s));
     if (ctx->user_params.autotune && !ctx->tune_locked) {
@@ -436,14 +463,16 @@ int run_init(sspp_ctx* ctx) {
         int rc2 = run_collapse(ctx);
         if (rc2) return rc2;
     }
-    ctx->launches += init_passes(D, s);
+    ctx->launches += init_passes(D, lows_in_reorder, s);
     if ((ctx->params.model & 1) && ctx->params.max_iteration > 0) {
         int rc2 = run_highclear(ctx);
         if (rc2) return rc2;
     }
-    ctx->launches += init_compress(D, dropped_of(ctx), ctx->params.representatives != 0, s);
-    if (ctx->params.dualize == 1) ctx->launches += dualize(D, 1, s);
-    ctx->launches += build_apparent(D, s);
+    ctx->launches += init_compress(D, dropped_of(ctx), ctx->params.representatives != 0, ctx->params.dualize != 1, s);
+    if (ctx->params.dualize == 1) {
+        ctx->launches += dualize(D, 1, s);
+        ctx->launches += build_apparent(D, s);
+    }
     ctx->launches += active_list(D, s);
     span_end(ctx, PH_INIT, ev0);
     CK(cudaGetLastError());
@@ -586,7 +615,20 @@ int run_steps(sspp_ctx* ctx, const std::vector<Step>& steps, int cap1, int cap2,
         span_end(ctx, PH_LIGHT, a);
         heavy_slice_mark(D, ctr, k + 1 < steps.size() ? ctr + 4 : nullptr, s);
         if (overlap && (!last_of_dim || gate)) {
-            cudaStream_t hs = ctx->side[k % sspp_ctx::kSide];
+            // an idle side stream if there is one: a CTA-tier launch lasts as
+            // long as its longest chain, and a launch queued behind it on the
+            // same stream would wait for that chain
+            int q = int(k % sspp_ctx::kSide);
+#ifndef SSPP_SIDE_RR
+            for (int t = 0; t < sspp_ctx::kSide; t++) {
+                const int c = int((k + t) % sspp_ctx::kSide);
+                if (cudaStreamQuery(ctx->side[c]) == cudaSuccess) {
+                    q = c;
+                    break;
+                }
+            }
+#endif
+            cudaStream_t hs = ctx->side[q];
             CK(cudaEventRecord(ctx->step_ev[k], s));
             CK(cudaStreamWaitEvent(hs, ctx->step_ev[k], 0));
             span_begin(ctx, b, hs);
@@ -610,6 +652,165 @@ int run_steps(sspp_ctx* ctx, const std::vector<Step>& steps, int cap1, int cap2,
         if (rcj) return rcj;
     }
     ctx->ss_steps = int64_t(steps.size());
+    return SSPP_OK;
+}
+
+// Spectral-sequence blocks of dimensions [dlo, dhi] (ascending or
+// descending) of every complex the context holds, as one persistent launch
+// draining a device queue of (complex, block) items (k_reduce_queue).  Each
+// complex gets the schedule ss_schedule gives its own active columns and row
+// bounds; the host reads those per-complex bounds once (one synchronisation)
+// and issues one launch.
+constexpr int kQueueChunk = 8;
+constexpr int kQueueGateLeft = 16;
+
+int run_queue(sspp_ctx* ctx, int dlo, int dhi, bool ascending, int cap1, int cap2, int threads) {
+    Device& D = ctx->D;
+    cudaStream_t s = ctx->stream;
+    const sspp_params& P = ctx->params;
+    const bool batch = ctx->batch_start.size() >= 2;
+    const int32_t k = batch ? int32_t(ctx->batch_start.size() - 1) : 1;
+    const int64_t* d_cstart = ctx->d_batch;
+    if (!batch) {
+        if (!ctx->q_cstart) CK(cudaMalloc(&ctx->q_cstart, 2 * sizeof(int64_t)));
+        const int64_t h[2] = {0, D.n};
+        CK(cudaMemcpyAsync(ctx->q_cstart, h, sizeof(h), cudaMemcpyHostToDevice, s));
+        d_cstart = ctx->q_cstart;
+    }
+    const int64_t m = int64_t(k) * kNumDims;
+    CK(grow(ctx->q_info, ctx->cap_q_info, 3 * m, s));
+    ctx->launches += queue_complex_info(D, k, d_cstart, ctx->q_info, ctx->q_info + m, ctx->q_info + 2 * m, s);
+    ctx->h_qinfo.resize(size_t(3 * m));
+    CK(cudaMemcpyAsync(ctx->h_qinfo.data(), ctx->q_info, sizeof(int32_t) * 3 * m, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    const int32_t* act = ctx->h_qinfo.data();
+    const int32_t* mnr = act + m;
+    const int32_t* mxr = act + 2 * m;
+    const DimInfo& I = ctx->hinfo;
+    // items, complex by complex; the active list holds each dimension's
+    // columns complex after complex
+    std::vector<QItem>& items = ctx->h_items;
+    items.clear();
+    const size_t nk = size_t(k);
+    std::vector<int32_t> first(nk, 0), iend(nk, 0), lcap(nk, 0);
+    std::vector<int64_t> loff(nk + 1, 0);
+    std::vector<int32_t> dim_start(kNumDims);
+    for (int d = 0; d < kNumDims; d++) dim_start[d] = I.act_begin[d];
+    std::vector<Step> st;
+    for (int32_t c = 0; c < k; c++) {
+        first[size_t(c)] = int32_t(items.size());
+        int32_t cap = 0;
+        for (int j = 0; j <= dhi - dlo; j++) {
+            const int d = ascending ? dlo + j : dhi - j;
+            const int32_t cnt = act[int64_t(c) * kNumDims + d];
+            const int32_t ab = dim_start[d], ae = ab + cnt;
+            cap = std::max(cap, cnt);
+            st.clear();
+            const int32_t mr = mnr[int64_t(c) * kNumDims + d];
+            ss_schedule(P, ab, ae, mr == INT32_MAX ? 0 : mr, mxr[int64_t(c) * kNumDims + d], st);
+            int32_t eprev = -1;
+            const size_t d0 = items.size();
+            for (const Step& x : st) {
+                QItem q{};
+                q.cplx = c;
+                q.nbeg = eprev < 0 ? x.beg : std::max(eprev, x.beg);
+                q.nend = std::max(q.nbeg, x.end);
+                eprev = std::max(eprev, x.end);
+                q.minrow = x.minrow;
+                q.flags = ((items.size() - d0) & 1) ? QF_HALF : 0;
+                items.push_back(q);
+            }
+            if (items.size() > d0) items.back().flags |= QF_LAST_OF_DIM;
+        }
+        // dimensions outside [dlo, dhi] keep their columns, but the running
+        // offsets cover every dimension
+        for (int d = 0; d < kNumDims; d++) dim_start[d] += act[int64_t(c) * kNumDims + d];
+        iend[size_t(c)] = int32_t(items.size());
+        lcap[size_t(c)] = cap + 32;
+        loff[size_t(c) + 1] = loff[size_t(c)] + 2 * int64_t(lcap[size_t(c)]);
+    }
+    const int64_t nit = int64_t(items.size());
+    ctx->ss_steps = nit;
+    if (nit == 0) return SSPP_OK;
+    if (ctx->queue_bpsm < 0 || cap1 != ctx->q_conf[0] || cap2 != ctx->q_conf[1] || threads != ctx->q_conf[2]) {
+        int b = 0;
+        CK(queue_configure(cap1, cap2, threads, &b));
+        ctx->queue_bpsm = b;
+        ctx->q_conf[0] = cap1;
+        ctx->q_conf[1] = cap2;
+        ctx->q_conf[2] = threads;
+    }
+    if (ctx->queue_bpsm < 1) return set_err(ctx, SSPP_ERR_CAPACITY, "level capacities too large for shared memory");
+    // device state
+    CK(grow(ctx->q_items, ctx->cap_q_items, nit, s));
+    CK(grow(ctx->q_ctr, ctx->cap_q_ctr, 3 * (nit + 1), s));
+    CK(grow(ctx->q_cplx, ctx->cap_q_cplx, 5 * int64_t(k) + 8, s));
+    CK(grow(ctx->q_loff, ctx->cap_q_loff, int64_t(k), s));
+    CK(grow(ctx->q_lists, ctx->cap_q_lists, std::max<int64_t>(loff[size_t(k)], 1), s));
+    const int64_t want_pool = std::max<int64_t>(ctx->pool_request, std::max<int64_t>(D.n / 4, 1 << 16));
+    if (want_pool > D.pool_cap) {
+        if (D.heavy) cudaFreeAsync(D.heavy, s);
+        D.heavy = nullptr;
+        D.pool_cap = 0;
+        CK(grow(D.heavy, D.pool_cap, want_pool, s));
+    }
+    if (D.pool_cap > ctx->cap_q_pool_c) {
+        if (ctx->q_pool_c) cudaFreeAsync(ctx->q_pool_c, s);
+        ctx->q_pool_c = nullptr;
+        ctx->cap_q_pool_c = 0;
+        CK(grow(ctx->q_pool_c, ctx->cap_q_pool_c, D.pool_cap, s));
+    }
+    std::vector<int32_t> hc(size_t(5 * int64_t(k) + 8), 0);
+    int32_t nfin = 0;
+    for (int32_t c = 0; c < k; c++) {
+        const bool none = first[size_t(c)] == iend[size_t(c)];
+        hc[size_t(c)] = none ? -1 : first[size_t(c)];   // cur
+        nfin += none ? 1 : 0;
+        hc[size_t(3 * k + c)] = iend[size_t(c)];         // item_end
+        hc[size_t(4 * k + c)] = lcap[size_t(c)];         // list_cap
+    }
+    hc[size_t(5 * k)] = nfin;  // finished; then abort, pool_head, pool_tail
+    CK(cudaMemcpyAsync(ctx->q_items, items.data(), sizeof(QItem) * size_t(nit), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(ctx->q_cplx, hc.data(), sizeof(int32_t) * hc.size(), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(ctx->q_loff, loff.data(), sizeof(int64_t) * size_t(k), cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(ctx->q_ctr, 0, sizeof(int) * 3 * size_t(nit + 1), s));
+    CK(cudaMemsetAsync(D.heavy, 0xff, sizeof(int32_t) * size_t(D.pool_cap), s));
+    QueueArgs Q{};
+    Q.items = ctx->q_items;
+    Q.nitems = int32_t(nit);
+    Q.ncplx = k;
+    Q.taken = ctx->q_ctr;
+    Q.done = ctx->q_ctr + (nit + 1);
+    Q.lin = ctx->q_ctr + 2 * (nit + 1);
+    Q.cur = ctx->q_cplx;
+    Q.gate = ctx->q_cplx + k;
+    Q.hpend = ctx->q_cplx + 2 * k;
+    Q.item_end = ctx->q_cplx + 3 * k;
+    Q.list_cap = ctx->q_cplx + 4 * k;
+    Q.finished = ctx->q_cplx + 5 * k;
+    Q.abort = ctx->q_cplx + 5 * k + 1;
+    Q.pool_head = ctx->q_cplx + 5 * k + 2;
+    Q.pool_tail = ctx->q_cplx + 5 * k + 3;
+    Q.list_off = ctx->q_loff;
+    Q.lists = ctx->q_lists;
+    Q.pool = D.heavy;
+    Q.pool_c = ctx->q_pool_c;
+    Q.pool_cap = int32_t(std::min<int64_t>(D.pool_cap, INT32_MAX));
+    Q.gate_left = kQueueGateLeft;
+    Q.chunk = kQueueChunk;
+    Q.cap1 = cap1;
+    Q.spin_limit = (long long)1 << 22;  // idle polls of about a quarter to one microsecond each
+    const int share = std::max(1, ctx->cfg.sm_share);
+    const int sms = std::max(1, ctx->num_sms / share);
+    const int grid = std::max(2, sms * ctx->queue_bpsm);
+    // a block per SM for the CTA tier (half the blocks when only one fits per SM)
+    Q.heavy_ctas = ctx->queue_bpsm >= 2 ? sms : std::max(1, grid / 2);
+    cudaEvent_t a = nullptr;
+    span_begin(ctx, a);
+    CK(reduce_queue_launch(D, cap1, cap2, threads, Q, grid, s));
+    span_end(ctx, PH_LIGHT, a);
+    ctx->launches += 1;
+    ctx->light_launches += 1;
     return SSPP_OK;
 }
 
@@ -652,9 +853,19 @@ int run_compute(sspp_ctx* ctx) {
         }
         return st;
     };
+    // schedule 1 (and 0): a host loop of per-block launches; 2: one persistent
+    // launch per phase draining the (complex, block) work queue.  The host loop
+    // is the default: its warp-tier kernel keeps four times as many warps
+    // resident as the persistent kernel, whose CTA-tier role sets the register
+    // budget of every block
+    const bool queue = P.schedule == 2;
+    auto phase = [&](int dlo, int dhi, bool ascending) {
+        return queue ? run_queue(ctx, dlo, dhi, ascending, cap1, cap2, ht)
+                     : run_steps(ctx, schedule(dlo, dhi, ascending), cap1, cap2, ht);
+    };
     int64_t nsteps = 0;
     if (P.dualize == 2) {
-        int rc = run_steps(ctx, schedule(1, 1, false), cap1, cap2, ht);
+        int rc = phase(1, 1, false);
         if (rc) return rc;
         nsteps += ctx->ss_steps;
         ctx->launches += dualize(D, 2, s);
@@ -663,12 +874,11 @@ int run_compute(sspp_ctx* ctx) {
         CK(cudaMemcpyAsync(ctx->h_info, D.diminfo, sizeof(DimInfo), cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
         ctx->hinfo = *ctx->h_info;
-        rc = run_steps(ctx, schedule(1, kMaxDim, true), cap1, cap2, ht);
+        rc = phase(1, kMaxDim, true);
         if (rc) return rc;
         nsteps += ctx->ss_steps;
     } else {
-        int rc = P.dualize ? run_steps(ctx, schedule(0, kMaxDim, true), cap1, cap2, ht)
-                           : run_steps(ctx, schedule(0, kMaxDim, false), cap1, cap2, ht);
+        int rc = P.dualize ? phase(0, kMaxDim, true) : phase(0, kMaxDim, false);
         if (rc) return rc;
         nsteps += ctx->ss_steps;
     }
@@ -699,6 +909,7 @@ int run_compute(sspp_ctx* ctx) {
 int load_common(sspp_ctx* ctx, int64_t n, int64_t nnz) {
     ctx->loaded = ctx->inited = ctx->computed = false;
     ctx->built = false;
+    ctx->built_batch = false;
     ctx->build_ms = 0;
     ctx->batch_start.clear();
     ctx->host_pairs_valid = false;
@@ -774,6 +985,36 @@ int finish_build(sspp_ctx* ctx, int rc, const Built& b, const std::string& msg,
 
 }  // namespace
 
+namespace {
+
+// A device buffer of `want` T that keeps its first `used` entries.
+template <typename T>
+cudaError_t grow_keep(T*& p, int64_t& cap, int64_t want, int64_t used, cudaStream_t s) {
+    if (want <= cap && p) return cudaSuccess;
+    const int64_t nc = std::max<int64_t>(want, cap + cap / 2);
+    T* q = nullptr;
+    cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&q), size_t(std::max<int64_t>(nc, 1)) * sizeof(T), s);
+    if (e != cudaSuccess) return e;
+    if (p && used > 0) e = cudaMemcpyAsync(q, p, size_t(used) * sizeof(T), cudaMemcpyDeviceToDevice, s);
+    if (p) cudaFreeAsync(p, s);
+    p = q;
+    cap = nc;
+    return e;
+}
+
+// own_dims and own_colptr share one capacity (cap_own_n); they keep their
+// first `used` and `used + 1` entries
+cudaError_t grow_own_cols(sspp_ctx* ctx, int64_t want, int64_t used, cudaStream_t s) {
+    if (want <= ctx->cap_own_n && ctx->own_dims && ctx->own_colptr) return cudaSuccess;
+    int64_t c1 = ctx->own_dims ? ctx->cap_own_n : 0, c2 = ctx->own_colptr ? ctx->cap_own_n : 0;
+    cudaError_t e = grow_keep(ctx->own_dims, c1, want, used, s);
+    if (e == cudaSuccess) e = grow_keep(ctx->own_colptr, c2, c1, used + 1, s);
+    ctx->cap_own_n = std::min(c1, c2);
+    return e;
+}
+
+}  // namespace
+
 extern "C" {
 
 void sspp_default_params(sspp_params* p) {
@@ -789,6 +1030,7 @@ void sspp_default_params(sspp_params* p) {
     p->level2_capacity = 8000;
     p->autotune = 0;
     p->heavy_threads = 0;
+    p->schedule = 0;
 }
 
 sspp_ctx* sspp_create(const sspp_config* cfg) {
@@ -847,6 +1089,12 @@ void sspp_destroy(sspp_ctx* ctx) {
     if (ctx->own_colptr) cudaFree(ctx->own_colptr);
     if (ctx->own_rows) cudaFree(ctx->own_rows);
     if (ctx->d_batch) cudaFree(ctx->d_batch);
+    {
+        void* q[] = {ctx->q_info, ctx->q_items, ctx->q_ctr, ctx->q_cplx, ctx->q_loff, ctx->q_lists, ctx->q_pool_c,
+                     ctx->q_cstart, ctx->bvalues};
+        for (void* p : q)
+            if (p) cudaFree(p);
+    }
     collapse_free(ctx->cs);
     build_free(ctx->bs);
     for (auto* t : ctx->hc.tup)
@@ -982,10 +1230,113 @@ int32_t sspp_input_copy(sspp_ctx* ctx, int32_t* dims, int64_t* col_ptr, int32_t*
     if (rows && D.nnz > 0)
         CK(cudaMemcpyAsync(rows, D.in_rows, sizeof(int32_t) * size_t(D.nnz), cudaMemcpyDeviceToHost, s));
     if (values && D.n > 0)
-        CK(cudaMemcpyAsync(values, ctx->bs.p[BuildScratch::VALUES], sizeof(float) * size_t(D.n),
-                           cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(values, ctx->built_batch ? ctx->bvalues : static_cast<float*>(ctx->bs.p[BuildScratch::VALUES]),
+                           sizeof(float) * size_t(D.n), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     return SSPP_OK;
+}
+
+int32_t sspp_load_built_batch(sspp_ctx* ctx, int32_t k, const sspp_build_spec* specs) {
+    if (!ctx) return SSPP_ERR_BAD_INPUT;
+    cudaSetDevice(ctx->cfg.device);
+    if (k < 0 || (k > 0 && !specs)) return set_err(ctx, SSPP_ERR_BAD_INPUT, "null build specs");
+    for (int32_t i = 0; i < k; i++) {
+        const sspp_build_spec& b = specs[i];
+        if (b.kind == SSPP_BUILD_RIPS) {
+            if (b.size[0] < 0 || (b.size[0] > 0 && !b.data) || b.size[1] < 1 || b.size[1] > 3)
+                return set_err(ctx, SSPP_ERR_BAD_INPUT, "bad point array or space dimension");
+        } else if (b.kind == SSPP_BUILD_LOWERSTAR) {
+            const int64_t gx = b.size[0], gy = b.size[1], gz = b.size[2];
+            if (gx < 1 || gy < 1 || gz < 1 || !b.data || gx > INT32_MAX || gy > INT32_MAX || gz > INT32_MAX ||
+                gx * gy > INT32_MAX || gx * gy * gz > INT32_MAX)
+                return set_err(ctx, SSPP_ERR_BAD_INPUT, "bad grid size or null values");
+        } else {
+            return set_err(ctx, SSPP_ERR_BAD_INPUT, "unknown build kind");
+        }
+    }
+    const auto t0 = std::chrono::steady_clock::now();
+    ctx->loaded = false;
+    cudaStream_t s = ctx->stream;
+    std::vector<int64_t> starts(size_t(2) * (size_t(k) + 1), 0);  // column starts, then entry starts
+    int64_t* cst = starts.data();
+    int64_t* est = cst + k + 1;
+    // each complex is built in the builder's buffers, then appended to the
+    // context's input buffers (col_ptr entries and faces still local)
+    for (int32_t i = 0; i < k; i++) {
+        const sspp_build_spec& b = specs[i];
+        const int64_t nin = b.kind == SSPP_BUILD_RIPS ? b.size[0] * b.size[1] : b.size[0] * b.size[1] * b.size[2];
+        const float* din = nullptr;
+        if (nin > 0) {
+            int rc = stage_floats(ctx, b.data, nin, &din);
+            if (rc) return rc;
+        }
+        Built out;
+        std::string msg;
+        const int rc = b.kind == SSPP_BUILD_RIPS
+                           ? build_rips(ctx->bs, din, b.size[0], int(b.size[1]), b.radius, b.maxdim, s, &out, &msg)
+                           : build_lowerstar(ctx->bs, din, b.size[0], b.size[1], b.size[2], b.maxdim, s, &out, &msg);
+        if (rc) return set_err(ctx, rc == -1 ? SSPP_ERR_BAD_INPUT : SSPP_ERR_CUDA, msg);
+        const int64_t n0 = cst[i], e0 = est[i];
+        cst[i + 1] = n0 + out.ncols;
+        est[i + 1] = e0 + out.nnz;
+        if (cst[i + 1] > INT32_MAX - 8) return set_err(ctx, SSPP_ERR_CAPACITY, "more than 2^31 columns");
+        CK(grow_own_cols(ctx, cst[i + 1] + 1, n0, s));
+        CK(grow_keep(ctx->own_rows, ctx->cap_own_nnz, std::max<int64_t>(est[i + 1], 1), e0, s));
+        CK(grow_keep(ctx->bvalues, ctx->cap_bvalues, std::max<int64_t>(cst[i + 1], 1), n0, s));
+        if (out.ncols > 0) {
+            CK(cudaMemcpyAsync(ctx->own_dims + n0, out.dims, sizeof(int32_t) * size_t(out.ncols),
+                               cudaMemcpyDeviceToDevice, s));
+            CK(cudaMemcpyAsync(ctx->own_colptr + n0 + 1, out.col_ptr + 1, sizeof(int64_t) * size_t(out.ncols),
+                               cudaMemcpyDeviceToDevice, s));
+            CK(cudaMemcpyAsync(ctx->bvalues + n0, out.values, sizeof(float) * size_t(out.ncols),
+                               cudaMemcpyDeviceToDevice, s));
+        }
+        if (out.nnz > 0)
+            CK(cudaMemcpyAsync(ctx->own_rows + e0, out.rows, sizeof(int32_t) * size_t(out.nnz),
+                               cudaMemcpyDeviceToDevice, s));
+    }
+    const int64_t n = cst[k], nnz = est[k];
+    CK(grow_own_cols(ctx, n + 1, n, s));
+    if (!ctx->own_rows) CK(grow_keep(ctx->own_rows, ctx->cap_own_nnz, 1, 0, s));
+    CK(cudaMemsetAsync(ctx->own_colptr, 0, sizeof(int64_t), s));
+    CK(grow(ctx->d_batch, ctx->cap_d_batch, 2 * int64_t(starts.size()) + 1, s));
+    CK(cudaMemcpyAsync(ctx->d_batch, starts.data(), sizeof(int64_t) * starts.size(), cudaMemcpyHostToDevice, s));
+    int* d_bad = reinterpret_cast<int*>(ctx->d_batch + starts.size());
+    CK(cudaMemsetAsync(d_bad, 0, sizeof(int), s));
+    batch_rebase(n, nnz, k, ctx->d_batch, ctx->d_batch + k + 1, ctx->own_colptr, ctx->own_rows, d_bad, s);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(s));
+    int rc = load_common(ctx, n, nnz);
+    if (rc) return rc;
+    ctx->D.in_dims = ctx->own_dims;
+    ctx->D.in_colptr = ctx->own_colptr;
+    ctx->D.in_rows = ctx->own_rows;
+    ctx->batch_start.assign(cst, cst + k + 1);
+    ctx->loaded = true;
+    ctx->built = true;
+    ctx->built_batch = true;
+    ctx->build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return SSPP_OK;
+}
+
+int64_t sspp_batch_values(sspp_ctx* ctx, int32_t i, float* out, int64_t cap) {
+    if (!ctx) return -1;
+    cudaSetDevice(ctx->cfg.device);
+    if (!ctx->loaded || !ctx->built_batch || i < 0 || i + 1 >= int32_t(ctx->batch_start.size())) {
+        set_err(ctx, SSPP_ERR_STATE, "no built batch loaded, or no complex of that index");
+        return -1;
+    }
+    const int64_t b = ctx->batch_start[size_t(i)], e = ctx->batch_start[size_t(i) + 1];
+    const int64_t m = std::min(cap, e - b);
+    if (out && m > 0) {
+        if (cudaMemcpyAsync(out, ctx->bvalues + b, sizeof(float) * size_t(m), cudaMemcpyDeviceToHost, ctx->stream) !=
+                cudaSuccess ||
+            cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+            set_err(ctx, SSPP_ERR_CUDA, "value copy failed");
+            return -1;
+        }
+    }
+    return e - b;
 }
 
 int32_t sspp_load_batch(sspp_ctx* ctx, int32_t k, const int64_t* ncols, const int32_t* const* dims,
@@ -1325,7 +1676,7 @@ int32_t sspp_export_preprocessed(sspp_ctx* ctx, const sspp_params* p, const char
         CK(cudaMemcpyAsync(ctx->h_err, D.err, sizeof(int), cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
         if (*ctx->h_err) return set_err(ctx, SSPP_ERR_BAD_INPUT, "dimension out of range 0..7 or malformed col_ptr");
-        reorder(D, s);
+        reorder(D, false, s);
         CK(cudaMemcpyAsync(D.arena_top, D.blk + reorder_total_slot(D), sizeof(unsigned long long),
                            cudaMemcpyDeviceToDevice, s));
         CK(cudaMemcpyAsync(ctx->h_err, D.err, sizeof(int), cudaMemcpyDeviceToHost, s));

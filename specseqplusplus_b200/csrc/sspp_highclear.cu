@@ -184,14 +184,36 @@ __device__ __forceinline__ bool adj_has(const int32_t* adj, const int64_t* adj_o
 
 // G lanes per top-dimension simplex (G = max_iteration rounded up to a power
 // of two, at most 32), one lane per candidate; a warp takes 32 / G simplices
-// at a time, so a small max_iteration does not leave most lanes idle.
+// at a time, so a small max_iteration does not leave most lanes idle.  The
+// candidates are read with one coalesced load per group; for each further
+// vertex of the simplex the group stages that vertex's neighbour list in
+// shared memory (coalesced; lists longer than kNbrCap are searched in global
+// memory instead) and every surviving candidate is binary-searched there.
+constexpr int kHcThreads = 256;
+constexpr int kNbrCap = 64;
+
+__device__ __forceinline__ bool sorted_has(const int32_t* a, int n, int32_t w) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (a[mid] < w) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo < n && a[lo] == w;
+}
+
 template <int G>
-__global__ void k_highclear(int32_t cb, int32_t ce, int D, int max_iter, const int32_t* tup, const int32_t* adj,
-                            const int64_t* adj_off, const int32_t* table, uint32_t mask, const uint8_t* dropped,
-                            uint8_t* cleared, long long* counters) {
+__global__ void __launch_bounds__(kHcThreads) k_highclear(int32_t cb, int32_t ce, int D, int max_iter,
+                                                          const int32_t* tup, const int32_t* adj,
+                                                          const int64_t* adj_off, const int32_t* table, uint32_t mask,
+                                                          const uint8_t* dropped, uint8_t* cleared,
+                                                          long long* counters) {
     constexpr int kPer = 32 / G;  // simplices per warp
     constexpr unsigned kGroupMask = G == 32 ? 0xffffffffu : ((1u << G) - 1);
-    const int lane = threadIdx.x & 31, grp = lane / G, gl = lane % G;
+    __shared__ int32_t s_nbr[kHcThreads / 32][kPer][kNbrCap];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, grp = lane / G, gl = lane % G;
+    const unsigned gmask = kGroupMask << (grp * G);
+    int32_t* nbuf = s_nbr[wid][grp];
     const int64_t warp = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5;
     const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
     const int k = D + 1;
@@ -201,37 +223,48 @@ __global__ void k_highclear(int32_t cb, int32_t ce, int D, int max_iter, const i
         const int32_t* s = tup + (i - cb) * k;
         const bool valid = i < ce && s[0] >= 0 && !(dropped && dropped[i]);
         const int32_t v0 = valid ? s[0] : 0;
-        const int64_t nb = valid ? adj_off[v0 + 1] - adj_off[v0] : 0;
+        const int64_t a0 = valid ? adj_off[v0] : 0;
+        const int64_t nb = valid ? adj_off[v0 + 1] - a0 : 0;
         const int64_t limit = nb < max_iter ? nb : max_iter;
         bool found = false;
         for (int64_t base = 0;; base += G) {
             const bool act = valid && !found && base < limit;
             if (!__any_sync(kFull, act)) break;
-            bool ok = false;
             const int64_t q = base + gl;
-            if (act && q < limit) {
-                const int32_t w = adj[adj_off[v0] + q];
-                ok = true;
-                for (int j = 1; j < k && ok; j++) ok = adj_has(adj, adj_off, s[j], w);
-                if (ok) {
-                    // t = s + {w}, sorted; every facet other than s must exist and precede column i
-                    int32_t t[kMaxDim + 2];
-                    int m = 0;
-                    bool placed = false;
-                    for (int j = 0; j < k; j++) {
-                        if (!placed && w < s[j]) { t[m++] = w; placed = true; }
-                        t[m++] = s[j];
-                    }
-                    if (!placed) t[m++] = w;
-                    int32_t f[kMaxDim + 1];
-                    for (int drop = 0; drop <= k && ok; drop++) {
-                        if (t[drop] == w) continue;  // that facet is s itself
-                        int mm = 0;
-                        for (int j = 0; j <= k; j++)
-                            if (j != drop) f[mm++] = t[j];
-                        int32_t c = hash_find(f, k, table, mask, tup, cb);
-                        ok = (c >= 0 && c < i);
-                    }
+            bool ok = act && q < limit;
+            const int32_t w = ok ? adj[a0 + q] : -1;
+            // w must be adjacent to every other vertex of s
+            for (int j = 1; j < k; j++) {
+                if (!__any_sync(kFull, ok)) break;
+                const bool gany = (__ballot_sync(kFull, ok) & gmask) != 0;
+                const int32_t u = gany ? s[j] : 0;
+                const int64_t b0 = gany ? adj_off[u] : 0;
+                const int len = gany ? int(adj_off[u + 1] - b0) : 0;
+                const bool staged = len <= kNbrCap;
+                if (gany && staged)
+                    for (int t = gl; t < len; t += G) nbuf[t] = adj[b0 + t];
+                __syncwarp();
+                if (ok) ok = staged ? sorted_has(nbuf, len, w) : adj_has(adj, adj_off, u, w);
+                __syncwarp();  // the next vertex's list overwrites the buffer
+            }
+            if (ok) {
+                // t = s + {w}, sorted; every facet other than s must exist and precede column i
+                int32_t t[kMaxDim + 2];
+                int m = 0;
+                bool placed = false;
+                for (int j = 0; j < k; j++) {
+                    if (!placed && w < s[j]) { t[m++] = w; placed = true; }
+                    t[m++] = s[j];
+                }
+                if (!placed) t[m++] = w;
+                int32_t f[kMaxDim + 1];
+                for (int drop = 0; drop <= k && ok; drop++) {
+                    if (t[drop] == w) continue;  // that facet is s itself
+                    int mm = 0;
+                    for (int j = 0; j <= k; j++)
+                        if (j != drop) f[mm++] = t[j];
+                    int32_t c = hash_find(f, k, table, mask, tup, cb);
+                    ok = (c >= 0 && c < i);
                 }
             }
             const unsigned bl = __ballot_sync(kFull, ok);
@@ -282,9 +315,9 @@ int highclear(Device& D, const DimInfo& info, int max_iteration, const uint8_t* 
     const int32_t cb = info.col_begin[top], ce = info.col_end[top];
     k_hash_insert<<<gridn(ce - cb, 256), 256, 0, s>>>(cb, ce, top + 1, S.tup[top], dropped, S.table, S.mask);
     const int g = max_iteration <= 4 ? 4 : max_iteration <= 8 ? 8 : max_iteration <= 16 ? 16 : 32;
-    const unsigned grid = gridn(int64_t(ce - cb) * g, 256, 148 * 64);
+    const unsigned grid = gridn(int64_t(ce - cb) * g, kHcThreads, 148 * 64);
 #define SSPP_HC(G_)                                                                                               \
-    k_highclear<G_><<<grid, 256, 0, s>>>(cb, ce, top, max_iteration, S.tup[top], S.adj, S.adj_off, S.table, S.mask, \
+    k_highclear<G_><<<grid, kHcThreads, 0, s>>>(cb, ce, top, max_iteration, S.tup[top], S.adj, S.adj_off, S.table, S.mask, \
                                          dropped, D.cleared, D.counters)
     if (g == 4) SSPP_HC(4);
     else if (g == 8) SSPP_HC(8);

@@ -231,9 +231,12 @@ __global__ void k_dim_starts(DimInfo* info) {
 }
 
 // stable rank of each column inside its dimension -> reordered index
+// Also starts the init passes' per-column state of reordered column idx: no
+// leftmost column yet, no pivot owner, not cleared, not negative.
 __global__ void __launch_bounds__(kPartThreads) k_dim_assign(const int32_t* dims, int64_t n, const int32_t* dimcnt,
                                                              const DimInfo* info, int32_t* newidx, int32_t* perm,
-                                                             int32_t* rdim) {
+                                                             int32_t* rdim, int32_t* leftmost, uint64_t* pivot,
+                                                             uint8_t* cleared, uint8_t* negative) {
     __shared__ int wcnt[kPartThreads / 32][kNumDims];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     int64_t j = int64_t(blockIdx.x) * kPartThreads + threadIdx.x;
@@ -254,51 +257,74 @@ __global__ void __launch_bounds__(kPartThreads) k_dim_assign(const int32_t* dims
         newidx[j] = idx;
         perm[idx] = int32_t(j);
         rdim[idx] = d;
+        leftmost[idx] = INT_MAX;
+        pivot[idx] = kNoOwner;
+        cleared[idx] = 0;
+        negative[idx] = 0;
     }
 }
 
 // Copies input column perm[i] into its padded arena slot with rows remapped to
-// reordered indices; validates face dimension, range and strict order.
-__global__ void k_scatter_cols(int64_t n, const int64_t* colptr, const int32_t* rows, const int32_t* dims,
-                               const int32_t* perm, const int32_t* newidx, const int64_t* off, int32_t* arena,
-                               uint64_t* desc, int32_t* leftmost, int* err) {
+// reordered indices; validates range, strict order and face dimension (a face
+// of a dimension-d column must land in the reordered range of dimension d-1).
+// With `lows` it also does the first init pass (include/kernel.h:444-457):
+// the column's lowest row, and each row's leftmost column by atomicMin (the
+// stable reorder keeps a column's rows ascending).
+__global__ void k_scatter_cols(int64_t n, const int64_t* colptr, const int32_t* rows, const int32_t* rdim,
+                               const int32_t* perm, const int32_t* newidx, const int64_t* off, const DimInfo* info,
+                               int32_t* arena, uint64_t* desc, int32_t* low, int32_t* leftmost, bool lows, int* err) {
+    __shared__ int32_t s_beg[kNumDims], s_end[kNumDims];
+    if (threadIdx.x < kNumDims) {
+        s_beg[threadIdx.x] = info->col_begin[threadIdx.x];
+        s_end[threadIdx.x] = info->col_end[threadIdx.x];
+    }
+    __syncthreads();
     for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
         const int32_t j = perm[i];
         const int64_t b = colptr[j], e = colptr[j + 1];
         const int64_t len = e - b;
         const int64_t o = off[i];
-        const int dj = dims[j];
+        const int dj = rdim[i];
+        const int32_t fb = dj > 0 ? s_beg[dj - 1] : 0, fe = dj > 0 ? s_end[dj - 1] : 0;
         bool bad = len < 0 || len > kMaxColLen;
-        int32_t prev = -1;
+        int32_t prev = -1, last = -1;
         int32_t* data = arena + o + kHdr;
         for (int64_t k = 0; k < len && !bad; k++) {
-            int32_t r = rows[b + k];
-            if (r < 0 || r >= n || r <= prev || dims[r] != dj - 1) { bad = true; break; }
+            const int32_t r = rows[b + k];
+            if (r < 0 || r >= n || r <= prev) { bad = true; break; }
+            const int32_t x = newidx[r];
+            if (x < fb || x >= fe) { bad = true; break; }
             prev = r;
-            data[k] = newidx[r];
+            data[k] = x;
+            last = x;
         }
         if (bad) {
             atomicOr(err, ERRB_BAD_INPUT);
             desc[i] = pack_desc(uint64_t(o), 0);
             *reinterpret_cast<int4*>(arena + o) = make_int4(0, int32_t(i), 0, 0);
+            if (lows) low[i] = -1;
         } else {
             for (int64_t k = len; k < pad4(len); k++) data[k] = INT_MAX;
             desc[i] = pack_desc(uint64_t(o), uint32_t(len));
             *reinterpret_cast<int4*>(arena + o) = make_int4(int32_t(len), int32_t(i), 0, 0);
+            if (lows) {
+                low[i] = len ? last : -1;
+                for (int64_t k = 0; k < len; k++) atomicMin(&leftmost[data[k]], int32_t(i));
+            }
         }
-        leftmost[i] = INT_MAX;
     }
 }
 
 int64_t reorder_total_slot(const Device& D) { return scan_blocks(D.n); }
 
-int reorder(Device& D, cudaStream_t s) {
+int reorder(Device& D, bool lows, cudaStream_t s) {
     const int64_t n = D.n;
     const int64_t nb = (n + kPartThreads - 1) / kPartThreads;
     k_dim_count<<<unsigned(nb), kPartThreads, 0, s>>>(D.in_dims, n, D.dimcnt, D.err);
     k_dim_offsets<<<kNumDims, 1024, 0, s>>>(D.dimcnt, nb, D.diminfo);
     k_dim_starts<<<1, 32, 0, s>>>(D.diminfo);
-    k_dim_assign<<<unsigned(nb), kPartThreads, 0, s>>>(D.in_dims, n, D.dimcnt, D.diminfo, D.newidx, D.perm, D.dim);
+    k_dim_assign<<<unsigned(nb), kPartThreads, 0, s>>>(D.in_dims, n, D.dimcnt, D.diminfo, D.newidx, D.perm, D.dim,
+                                                       D.leftmost, D.pivot, D.cleared, D.negative);
     // padded column offsets in reordered order
     const int64_t* colptr = D.in_colptr;
     const int32_t* perm = D.perm;
@@ -306,22 +332,21 @@ int reorder(Device& D, cudaStream_t s) {
     scan([=] __device__(int64_t i) -> int64_t { int32_t j = perm[i]; return slot_ints(colptr[j + 1] - colptr[j]); },
          [=] __device__(int64_t i, int64_t pre, int64_t) { off[i] = pre; }, n, D.blk, s);
     k_scatter_cols<<<grid_for(n, 256) > 65536 ? 65536 : grid_for(n, 256), 256, 0, s>>>(
-        n, D.in_colptr, D.in_rows, D.in_dims, D.perm, D.newidx, off, D.arena, D.desc, D.leftmost, D.err);
+        n, D.in_colptr, D.in_rows, D.dim, D.perm, D.newidx, off, D.diminfo, D.arena, D.desc, D.low, D.leftmost, lows,
+        D.err);
     return 8;
 }
 
 // ------------------------------------------------------------- init passes
-__global__ void k_init_low(int64_t n, const int32_t* arena, const uint64_t* desc, int32_t* low, int32_t* leftmost,
-                           uint64_t* pivot, uint8_t* cleared, uint8_t* negative) {
+// lowest row and leftmost columns when the reorder did not compute them (an
+// edge collapse emptied columns in between); leftmost starts at INT_MAX
+__global__ void k_init_low(int64_t n, const int32_t* arena, const uint64_t* desc, int32_t* low, int32_t* leftmost) {
     for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
         uint64_t d = desc[i];
         const int32_t* c = arena + desc_off(d) + kHdr;
         uint32_t len = desc_len(d);
         low[i] = len ? c[len - 1] : -1;
         for (uint32_t k = 0; k < len; k++) atomicMin(&leftmost[c[k]], int32_t(i));
-        pivot[i] = kNoOwner;
-        cleared[i] = 0;
-        negative[i] = 0;
     }
 }
 
@@ -347,12 +372,16 @@ __global__ void k_init_apparent(int64_t n, const int32_t* arena, const uint64_t*
     if ((threadIdx.x & 31) == 0 && app) cnt_add(&counters[CNT_APPARENT], app);
 }
 
-// Clears positive columns and removes negative rows in place.
+// Clears positive columns and removes negative rows in place.  With `app` it
+// also writes the inline apparent columns (Device::app): a column that owns its
+// lowest row l by an apparent pair writes app[l]; a row without an owner
+// writes its own entry (each row's entry has exactly one writer).
 __global__ void k_init_compress(int64_t n, int32_t* arena, uint64_t* desc, int32_t* low, const uint64_t* pivot,
                                 const uint8_t* cleared, const uint8_t* negative, uint8_t* state,
-                                const uint8_t* dropped, bool keep_rows, long long* counters, int* err) {
+                                const uint8_t* dropped, bool keep_rows, int4* app, long long* counters, int* err) {
     long long ncl = 0, nact = 0;
     for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+        if (app && pivot[i] == kNoOwner) app[i] = make_int4(-1, INT_MAX, INT_MAX, INT_MAX);
         uint64_t d = desc[i];
         int32_t* hdr = arena + desc_off(d);
         int32_t* c = hdr + kHdr;
@@ -389,6 +418,16 @@ __global__ void k_init_compress(int64_t n, int32_t* arena, uint64_t* desc, int32
         low[i] = l;
         uint8_t st = (m == 0) ? ST_ZERO : (pv_col(pivot[l]) == int32_t(i) ? ST_OWNER : ST_ACTIVE);
         state[i] = st;
+        if (app && st == ST_OWNER) {
+            int4 v = make_int4(-1, INT_MAX, INT_MAX, INT_MAX);
+            if (m <= 4) {
+                v.x = int(m) - 1;
+                if (m > 1) v.y = c[0];
+                if (m > 2) v.z = c[1];
+                if (m > 3) v.w = c[2];
+            }
+            app[l] = v;
+        }
         nact += (st == ST_ACTIVE);
     }
     ncl = warp_sum(ncl);
@@ -426,20 +465,20 @@ __global__ void k_diminfo_reset(DimInfo* info) {
     if (d < kNumDims) { info->min_row[d] = INT_MAX; info->max_row[d] = -1; }
 }
 
-int init_passes(Device& D, cudaStream_t s) {
+int init_passes(Device& D, bool lows_done, cudaStream_t s) {
     const int64_t n = D.n;
     const unsigned g = grid_for(n, 256) > 65536 ? 65536 : grid_for(n, 256);
-    k_init_low<<<g, 256, 0, s>>>(n, D.arena, D.desc, D.low, D.leftmost, D.pivot, D.cleared, D.negative);
+    if (!lows_done) k_init_low<<<g, 256, 0, s>>>(n, D.arena, D.desc, D.low, D.leftmost);
     k_init_apparent<<<g, 256, 0, s>>>(n, D.arena, D.desc, D.low, D.leftmost, D.pivot, D.cleared, D.negative,
                                       D.counters);
-    return 2;
+    return lows_done ? 1 : 2;
 }
 
-int init_compress(Device& D, const uint8_t* dropped, bool keep_rows, cudaStream_t s) {
+int init_compress(Device& D, const uint8_t* dropped, bool keep_rows, bool with_app, cudaStream_t s) {
     const int64_t n = D.n;
     const unsigned g = grid_for(n, 256) > 65536 ? 65536 : grid_for(n, 256);
     k_init_compress<<<g, 256, 0, s>>>(n, D.arena, D.desc, D.low, D.pivot, D.cleared, D.negative, D.state, dropped,
-                                      keep_rows, D.counters, D.err);
+                                      keep_rows, with_app ? D.app : nullptr, D.counters, D.err);
     return 1;
 }
 

@@ -72,6 +72,16 @@ struct ReduceArgs {
     const int4* app;      // inline short apparent columns by row (Device::app)
 };
 
+// Where one reduction of a column stops: the band's lowest row (a column whose
+// low drops below it parks), and the counter of the work it came from, so that
+// a long chain in the warp tier moves to the CTA tier once that work is fully
+// handed out (drain_ctr >= drain_total).
+struct Band {
+    int32_t minrow;
+    const int* drain_ctr;
+    int32_t drain_total;
+};
+
 constexpr int kMaxMergesPerColumn = 1 << 24;
 
 __device__ __forceinline__ uint64_t ld_acquire_u64(const uint64_t* p) {
@@ -597,6 +607,12 @@ __device__ int fold_delta(int32_t* a, int nb, int dv, int d, int32_t* tmp, int* 
 // toggles the addends' other entries into the delta; no dependent load waits
 // between its additions.
 constexpr int kCacheRefill = 16;  // cache lanes used before the cache is filled again
+#ifndef SSPP_FAST_PREFETCH
+#define SSPP_FAST_PREFETCH 1
+#endif
+#ifndef SSPP_FAST_TOGGLE3
+#define SSPP_FAST_TOGGLE3 0
+#endif
 
 // largest entry of an inline apparent column below its top (-1 if none)
 __device__ __forceinline__ int app_max_below(int4 q) {
@@ -604,8 +620,9 @@ __device__ __forceinline__ int app_max_below(int4 q) {
 }
 
 template <int T>
-__device__ int fast_adds(const BlockG<T>& g, const ReduceArgs& A, int col, Work& w, int& L, uint64_t& e,
-                         int32_t* tmp, int32_t* sb, long long& adds, long long& add_ints, int iters_left) {
+__device__ int fast_adds(const BlockG<T>& g, const ReduceArgs& A, int32_t minrow, int col, Work& w, int& L,
+                         uint64_t& e, int32_t* tmp, int32_t* sb, long long& adds, long long& add_ints,
+                         int iters_left) {
     __shared__ FastState fs;
     (void)sb;
     if (threadIdx.x < 32) {
@@ -623,6 +640,10 @@ __device__ int fast_adds(const BlockG<T>& g, const ReduceArgs& A, int col, Work&
         int cb = -1;
         int cr = -1;
         int4 ca = make_int4(-1, 0, 0, 0);
+        // inline apparent columns of the last addend's largest entries,
+        // loaded while that addition runs: one of them is usually the next low
+        int pf_row = -1;
+        int4 pf_ap = make_int4(-1, 0, 0, 0);
         bool have_e = true;  // ec is the pivot entry of Lc
         // toggles x in the delta (a fold into the bulk when the delta is full
         // invalidates the bulk cache)
@@ -647,7 +668,56 @@ __device__ int fast_adds(const BlockG<T>& g, const ReduceArgs& A, int col, Work&
                 d++;
             }
         };
-        while (done < iters_left && nb + d > 0 && Lc >= A.minrow) {
+        // toggles up to three ascending entries x0 < x1 < x2 at once: entries
+        // found in the delta are removed, the others inserted; every output
+        // lane finds its source with bit counts and one shuffle gathers it
+        auto toggle3 = [&](int q, int x0, int x1, int x2) {
+            if (d + q > 32) {  // the bulk absorbs the delta first
+                nb = fold_delta(a, nb, dv, d, tmp, A.err);
+                d = 0;
+                dv = INT_MAX;
+                cb = -1;
+            }
+            const unsigned below_d = d >= 32 ? kFull : ((1u << d) - 1);
+            unsigned del = 0;
+            int e0 = 64, e1 = 64, e2 = 64;  // output slots of the inserted entries (64: not inserted)
+            int ninsb = 0;                  // entries inserted so far (all smaller than the next one)
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                if (j >= q) break;
+                const int x = j == 0 ? x0 : (j == 1 ? x1 : x2);
+                const unsigned eq = __ballot_sync(kFull, dv == x) & below_d;
+                if (eq) {
+                    del |= eq;
+                } else {
+                    const unsigned lt = __ballot_sync(kFull, dv < x) & below_d;
+                    const int e = __popc(lt) - __popc(del & lt) + ninsb;
+                    if (j == 0) e0 = e;
+                    else if (j == 1) e1 = e;
+                    else e2 = e;
+                    ninsb++;
+                }
+            }
+            // output lane t: an inserted entry, or the (t - inserted before t)-th kept entry
+            const int kt = (e0 < lane) + (e1 < lane) + (e2 < lane);
+            int src = lane - kt;
+            unsigned dm = del;
+            while (dm) {
+                const int pdel = __ffs(dm) - 1;
+                if (pdel > src) break;
+                src++;
+                dm &= dm - 1;
+            }
+            const int g = __shfl_sync(kFull, dv, src & 31);
+            const int nd = d - __popc(del) + ninsb;
+            int v = src < d ? g : INT_MAX;
+            if (lane == e0) v = x0;
+            else if (lane == e1) v = x1;
+            else if (lane == e2) v = x2;
+            dv = lane < nd ? v : INT_MAX;
+            d = nd;
+        };
+        while (done < iters_left && nb + d > 0 && Lc >= minrow) {
             // the inline apparent column of the current low: from the bulk
             // cache when the low is the bulk top, else one load
             int4 ap;
@@ -669,12 +739,17 @@ __device__ int fast_adds(const BlockG<T>& g, const ReduceArgs& A, int col, Work&
                     break;
                 }
             } else {
-                ap = make_int4(-1, 0, 0, 0);
-                if (lane == 31 && Lc >= 0 && Lc < A.ncols) ap = __ldg(A.app + Lc);
-                ap.x = __shfl_sync(kFull, ap.x, 31);
-                ap.y = __shfl_sync(kFull, ap.y, 31);
-                ap.z = __shfl_sync(kFull, ap.z, 31);
-                ap.w = __shfl_sync(kFull, ap.w, 31);
+                const unsigned pm = __ballot_sync(kFull, pf_row == Lc);
+                const int src = pm ? __ffs(pm) - 1 : 31;
+                ap = pf_ap;
+                if (!pm) {
+                    ap = make_int4(-1, 0, 0, 0);
+                    if (lane == 31 && Lc >= 0 && Lc < A.ncols) ap = __ldg(A.app + Lc);
+                }
+                ap.x = __shfl_sync(kFull, ap.x, src);
+                ap.y = __shfl_sync(kFull, ap.y, src);
+                ap.z = __shfl_sync(kFull, ap.z, src);
+                ap.w = __shfl_sync(kFull, ap.w, src);
             }
             if (top_in_bulk && ap.x >= 0) {
                 // a run from cache lane h: lane l (> h) joins while lanes h..l-1
@@ -715,13 +790,18 @@ __device__ int fast_adds(const BlockG<T>& g, const ReduceArgs& A, int col, Work&
                         const int qy = __shfl_sync(kFull, ca.y, i);
                         const int qz = __shfl_sync(kFull, ca.z, i);
                         const int qw = __shfl_sync(kFull, ca.w, i);
-                        if (qx > 0) toggle(qy);
-                        if (qx > 1) toggle(qz);
-                        if (qx > 2) toggle(qw);
+                        if (SSPP_FAST_TOGGLE3) {
+                            if (qx > 0) toggle3(qx, qy, qz, qw);
+                        } else {
+                            if (qx > 0) toggle(qy);
+                            if (qx > 1) toggle(qz);
+                            if (qx > 2) toggle(qw);
+                        }
                         ai += 2 * (nb + d) + qx + 2;
                     }
                     done += P;
                     n_inline += P;
+                    pf_row = -1;
                     // the next lowest row: the larger top; equal tops cancel
                     int nl = -1;
                     while (true) {
@@ -769,6 +849,13 @@ __device__ int fast_adds(const BlockG<T>& g, const ReduceArgs& A, int col, Work&
             }
             const int m = plen - 1;  // addend entries below the common top
             if (nb + d + m > A.cap) break;  // the folded column might not fit
+            // the addend's three largest other entries: their inline apparent
+            // columns load while this addition runs
+            pf_row = -1;
+            if (SSPP_FAST_PREFETCH && lane < m && lane >= m - 3 && bj >= 0 && bj < A.ncols) {
+                pf_row = bj;
+                pf_ap = __ldg(A.app + bj);
+            }
             if (top_in_bulk) {  // the tops cancel
                 nb--;
             } else {
@@ -776,7 +863,11 @@ __device__ int fast_adds(const BlockG<T>& g, const ReduceArgs& A, int col, Work&
                 if (lane == d) dv = INT_MAX;
             }
             // toggle the addend's other entries in the delta
-            for (int j = 0; j < m; j++) toggle(__shfl_sync(kFull, bj, j));
+            if (SSPP_FAST_TOGGLE3 && ap.x >= 0) {
+                if (m > 0) toggle3(m, ap.y, ap.z, ap.w);
+            } else {
+                for (int j = 0; j < m; j++) toggle(__shfl_sync(kFull, bj, j));
+            }
             // the next lowest row: the larger top; equal tops cancel
             int nl = -1;
             while (true) {
@@ -840,8 +931,9 @@ __device__ int fast_adds(const BlockG<T>& g, const ReduceArgs& A, int col, Work&
 // in arena buffers.  *displaced receives the owner this column displaced (-1
 // if none).  sp holds kHdr + cap ints (staged addend with its header).
 template <class G>
-__device__ Outcome reduce_column(const G& g, const ReduceArgs& A, int col, int32_t* sw0, int32_t* sw1, int32_t* sp,
-                                 bool defer, int* displaced) {
+__device__ Outcome reduce_column(const G& g, const ReduceArgs& A, const Band& band, int col, int32_t* sw0,
+                                 int32_t* sw1, int32_t* sp, bool defer, int* displaced) {
+    const int32_t minrow = band.minrow;
     *displaced = -1;
     uint64_t d = 0;
     if (g.leader()) d = ld_cg_u64(A.desc + col);
@@ -882,9 +974,9 @@ __device__ Outcome reduce_column(const G& g, const ReduceArgs& A, int col, int32
         return OUT_FAIL;
     }
     // inline apparent column of row r (every thread loads it: one transaction per warp)
-    auto app_of = [&](int r) { return (r >= 0 && r >= A.minrow) ? __ldg(A.app + r) : make_int4(-1, 0, 0, 0); };
+    auto app_of = [&](int r) { return (r >= 0 && r >= minrow) ? __ldg(A.app + r) : make_int4(-1, 0, 0, 0); };
     int4 apc = app_of(L);
-    if (L >= A.minrow) {
+    if (L >= minrow) {
         if (g.leader()) e = ld_acquire_u64(A.pivot + L);
         e = g.bcast64(e);
     }
@@ -921,7 +1013,7 @@ __device__ Outcome reduce_column(const G& g, const ReduceArgs& A, int col, int32
             if (g.leader()) atomicOr(A.err, ERRB_TIMEOUT);
             break;
         }
-        if (L < A.minrow) {
+        if (L < minrow) {
             if (w.dirty && !publish(g, A, col, w)) break;
             if (g.leader()) A.low[col] = L;
             res = OUT_PARKED;
@@ -955,12 +1047,12 @@ __device__ Outcome reduce_column(const G& g, const ReduceArgs& A, int col, int32
             e = old;  // someone else changed the owner; look again
             continue;
         }
-        if (defer && A.light_chain > 0 && iter >= A.light_chain && (iter & 7) == 0) {
+        if (defer && band.drain_ctr && A.light_chain > 0 && iter >= A.light_chain && (iter & 7) == 0) {
             // once the step's window is handed out, a long chain in the warp tier
             // only holds up the step's tail: the CTA tier continues it on a side
             // stream while the next step runs
             int drained = 0;
-            if (g.leader()) drained = __ldcg(A.ctr) >= A.end - A.beg;
+            if (g.leader()) drained = __ldcg(band.drain_ctr) >= band.drain_total;
             if (g.bcast(drained)) {
                 if (w.dirty && !publish(g, A, col, w)) break;
                 res = OUT_DEFERRED;
@@ -969,7 +1061,7 @@ __device__ Outcome reduce_column(const G& g, const ReduceArgs& A, int col, int32
         }
         if constexpr (G::kSize > 32) {  // CTA tier: short addends by one warp
             if (!w.global) {
-                const int done = fast_adds(g, A, col, w, L, e, w.buf == sw0 ? sw1 : sw0, sp, adds, add_ints,
+                const int done = fast_adds(g, A, minrow, col, w, L, e, w.buf == sw0 ? sw1 : sw0, sp, adds, add_ints,
                                            min(kClearCheck, kMaxMergesPerColumn - iter));
                 if (done < 0) break;
                 if (done > 0) {
@@ -1037,7 +1129,7 @@ __device__ Outcome reduce_column(const G& g, const ReduceArgs& A, int col, int32
         // the group's last thread takes the entry: in short merges it holds no
         // element, so its acquire load completes while the others merge
         uint64_t pref = kNoOwner;
-        if (g.rank() == G::kSize - 1 && L2 >= A.minrow && L2 >= 0) pref = ld_acquire_u64(A.pivot + L2);
+        if (g.rank() == G::kSize - 1 && L2 >= minrow && L2 >= 0) pref = ld_acquire_u64(A.pivot + L2);
         const int4 apn = app_of(L2);
         int out_len;
         const int bound = w.len + plen - 2;
@@ -1143,6 +1235,7 @@ __global__ void __launch_bounds__(128) k_reduce_light(ReduceArgs A) {
     int32_t* sp = sw1 + A.cap;
     const int count = A.end - A.beg;
     const int chunk = A.chunk;
+    const Band band{A.minrow, A.ctr, count};
     while (true) {
         int base = 0;
         if (lane == 0) base = atomicAdd(A.ctr, chunk);
@@ -1163,7 +1256,7 @@ __global__ void __launch_bounds__(128) k_reduce_light(ReduceArgs A) {
             int col = __shfl_sync(kFull, c, src);
             while (col >= 0) {  // the column, then any owner it displaced
                 int next = -1;
-                Outcome o = reduce_column(g, A, col, sw0, sw1, sp, true, &next);
+                Outcome o = reduce_column(g, A, band, col, sw0, sw1, sp, true, &next);
                 if (!settle(g, A, col, o)) return;
                 col = next;
             }
@@ -1187,6 +1280,7 @@ __global__ void __launch_bounds__(T, 1) k_reduce_heavy(ReduceArgs A) {
     int32_t* sw1 = sw0 + A.cap;
     int32_t* sp = sw1 + A.cap;
     const int hb = __ldcg(A.ctr + 1), he = __ldcg(A.ctr + 2);
+    const Band band{INT32_MIN, nullptr, 0};
     while (true) {
         int k = 0;
         if (g.leader()) k = hb + atomicAdd(A.ctr + 3, 1);
@@ -1195,7 +1289,7 @@ __global__ void __launch_bounds__(T, 1) k_reduce_heavy(ReduceArgs A) {
         int col = __ldcg(A.heavy + k);
         while (col >= 0) {
             int next = -1;
-            Outcome o = reduce_column(g, A, col, sw0, sw1, sp, false, &next);
+            Outcome o = reduce_column(g, A, band, col, sw0, sw1, sp, false, &next);
             if (!settle(g, A, col, o)) return;
             col = next;
         }
@@ -1204,6 +1298,334 @@ __global__ void __launch_bounds__(T, 1) k_reduce_heavy(ReduceArgs A) {
             if (A.gate_host) st_relaxed_sys(A.gate_host, v);
         }
     }
+}
+
+// ------------------------------------------------------------- work queue
+// One persistent, cooperative launch drains the (complex, block) items of a
+// whole schedule: every spectral-sequence block of every complex of a batch
+// (one complex when not batched), in each complex's own block order, with
+// each complex's own dimension gate.  The host loop it replaces issues, per
+// block, a warp-tier launch and a CTA-tier launch and synchronises at every
+// dimension (the reference: include/specseq.h:616-661, three launches and a
+// host synchronisation per block).
+//
+// Blocks [0, heavy_ctas) reduce the columns the warp tier defers, taken from a
+// pool in order; the other blocks run independent warps over the open items.
+// An item opens when its predecessor of the same complex has finished; the
+// first item of a complex's next dimension opens once at most gate_left of the
+// complex's CTA-tier columns are left (none for its last item, after which the
+// complex is finished).  An item's entries are the columns its predecessors
+// parked (their lowest row below the band; kept with that row, so a later
+// block looks at a parked column without loading it) followed by the columns
+// its block adds to the window; a warp takes `chunk` of them at a time.
+// Columns of different complexes never share rows, so the items of different
+// complexes run concurrently.  All blocks are resident (cooperative launch),
+// so a block may poll for work that another block produces; every poll is
+// bounded by spin_limit, after which the launch sets ERRB_TIMEOUT and leaves.
+
+__device__ __forceinline__ int ld_acq(const int* p) { return ld_acquire(p); }
+__device__ __forceinline__ void st_rel(int* p, int v) {
+    asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ void queue_fail(const ReduceArgs& A, const QueueArgs& Q, int bits) {
+    atomicOr(A.err, bits);
+    st_rel(Q.abort, 1);
+}
+
+// Opens complex c's next item once its CTA-tier columns allow (c waits at a
+// gate, its current item ci finished); any lane may call it.
+__device__ void queue_try_gate(const QueueArgs& Q, int c, int ci) {
+    const bool last = ci + 1 >= Q.item_end[c];
+    if (ld_acq(Q.hpend + c) > (last ? 0 : Q.gate_left)) return;
+    if (atomicCAS(Q.gate + c, 1, 0) != 1) return;
+    if (last) {
+        st_rel(Q.cur + c, -1);
+        __threadfence();
+        atomicAdd(Q.finished, 1);
+    } else {
+        st_rel(Q.cur + c, ci + 1);
+    }
+}
+
+// Item `it` of complex c has finished: the next item opens, or, after the
+// last block of a dimension, the complex waits at its gate.
+__device__ __forceinline__ void queue_finish_item(const QueueArgs& Q, int c, int it, int flags) {
+    __threadfence();
+    if (flags & QF_LAST_OF_DIM) st_rel(Q.gate + c, 1);
+    else st_rel(Q.cur + c, it + 1);
+}
+
+// Final state of a warp-tier column taken from the queue (settle's rules;
+// deferred columns go to the pool, parked ones to the next item's list).
+__device__ bool settle_q(const ReduceArgs& A, const QueueArgs& Q, int cc, int col, Outcome o, int it, int2* lout,
+                         int32_t lcap) {
+    bool ok = true;
+    if ((threadIdx.x & 31) == 0) {
+        switch (o) {
+            case OUT_OWNER: break;
+            case OUT_ZERO: A.state[col] = ST_ZERO; break;
+            case OUT_DEFERRED: {
+                A.state[col] = ST_HEAVY;
+                atomicAdd(Q.hpend + cc, 1);
+                const int i = atomicAdd(Q.pool_tail, 1);
+                if (i < Q.pool_cap) {
+                    Q.pool_c[i] = cc;
+                    __threadfence();
+                    st_rel(Q.pool + i, col);
+                } else {
+                    queue_fail(A, Q, ERRB_CAPACITY);  // the run is repeated with a larger pool
+                }
+                break;
+            }
+            case OUT_PARKED: {
+                const int low = A.low[col];
+                __threadfence();
+                st_release_u8(A.state + col, ST_ACTIVE);
+                const int j = atomicAdd(Q.lin + it + 1, 1);
+                if (j < lcap) lout[j] = make_int2(col, low);
+                else queue_fail(A, Q, ERRB_CAPACITY);
+                break;
+            }
+            default:
+                __threadfence();
+                st_release_u8(A.state + col, ST_ACTIVE);
+                queue_fail(A, Q, ERRB_CHECK);
+                ok = false;
+                break;
+        }
+    }
+    __syncwarp();
+    return __shfl_sync(kFull, ok ? 1 : 0, 0) != 0;
+}
+
+__device__ void queue_light(const ReduceArgs& A, const QueueArgs& Q, int32_t* sw0, int32_t* sw1, int32_t* sp,
+                            int warps_per_block) {
+    WarpG g;
+    const int lane = g.rank();
+    const int wl = (blockIdx.x - Q.heavy_ctas) * warps_per_block + (threadIdx.x >> 5);
+    int start = Q.ncplx > 0 ? wl % Q.ncplx : 0;
+    long long idle = 0;
+    while (true) {
+        int stop = 0;
+        if (lane == 0) stop = ld_acq(Q.abort) || ld_acq(Q.finished) >= Q.ncplx;
+        if (__shfl_sync(kFull, stop, 0)) break;
+        // an open item with entries left: the lanes look at 32 complexes at a time
+        int it = -1, cc = -1;
+        for (int base = 0; base < Q.ncplx && it < 0; base += 32) {
+            int myit = -1, c = -1;
+            if (base + lane < Q.ncplx) {
+                c = (start + base + lane) % Q.ncplx;
+                const int ci = ld_acq(Q.cur + c);
+                if (ci >= 0) {
+                    if (ld_acq(Q.gate + c)) {
+                        queue_try_gate(Q, c, ci);
+                    } else {
+                        const QItem& I = Q.items[ci];
+                        const int total = ld_acq(Q.lin + ci) + (I.nend - I.nbeg);
+                        if (total == 0) {  // nothing to do: whoever sees it first finishes it
+                            if (atomicCAS(Q.taken + ci, 0, 1) == 0) queue_finish_item(Q, c, ci, I.flags);
+                        } else if (__ldcg(Q.taken + ci) < total) {
+                            myit = ci;
+                        }
+                    }
+                }
+            }
+            const unsigned m = __ballot_sync(kFull, myit >= 0);
+            if (m) {
+                const int src = __ffs(m) - 1;
+                it = __shfl_sync(kFull, myit, src);
+                cc = __shfl_sync(kFull, c, src);
+            }
+        }
+        if (it < 0) {
+            if (++idle > Q.spin_limit) {
+                if (lane == 0) queue_fail(A, Q, ERRB_TIMEOUT);
+                break;
+            }
+            __nanosleep(256);
+            continue;
+        }
+        idle = 0;
+        start = cc;
+        const QItem I = Q.items[it];
+        const int nl = ld_acq(Q.lin + it);
+        const int total = nl + (I.nend - I.nbeg);
+        int base = 0;
+        if (lane == 0) base = atomicAdd(Q.taken + it, Q.chunk);
+        base = __shfl_sync(kFull, base, 0);
+        if (base >= total) continue;
+        const int cnt = min(Q.chunk, total - base);
+        const int32_t lcap = Q.list_cap[cc];
+        const int2* lin_list = Q.lists + Q.list_off[cc] + ((I.flags & QF_HALF) ? lcap : 0);
+        int2* lout = Q.lists + Q.list_off[cc] + ((I.flags & QF_HALF) ? 0 : lcap);
+        int col = -1, lowc = 0;
+        bool run = false, park = false;
+        if (lane < cnt) {
+            const int e = base + lane;
+            if (e < nl) {
+                const int2 v = lin_list[e];
+                col = v.x;
+                lowc = v.y;
+            } else {
+                col = A.active[I.nbeg + (e - nl)];
+                lowc = __ldcg(A.low + col);
+            }
+            if (col < 0 || col >= A.ncols) {  // self-check: a list or active entry in range
+                queue_fail(A, Q, ERRB_CHECK);
+                col = -1;
+            } else {
+                const bool act = ld_acquire_u8(A.state + col) == ST_ACTIVE && !ld_acquire_u8(A.cleared + col);
+                run = act && lowc >= I.minrow;
+                park = act && lowc < I.minrow;
+            }
+        }
+        // still below the band: on to the next item's list as they are
+        const unsigned pm = __ballot_sync(kFull, park);
+        if (pm) {
+            int pb = 0;
+            if (lane == 0) pb = atomicAdd(Q.lin + it + 1, __popc(pm));
+            pb = __shfl_sync(kFull, pb, 0);
+            if (park) {
+                const int j = pb + __popc(pm & lanemask_lt());
+                if (j < lcap) lout[j] = make_int2(col, lowc);
+                else queue_fail(A, Q, ERRB_CAPACITY);
+            }
+        }
+        const Band band{I.minrow, Q.taken + it, total};
+        unsigned m = __ballot_sync(kFull, run);
+        bool failed = false;
+        while (m && !failed) {
+            const int src = __ffs(m) - 1;
+            m &= m - 1;
+            int c2 = __shfl_sync(kFull, col, src);
+            while (c2 >= 0) {  // the column, then any owner it displaced
+                int next = -1;
+                const Outcome o = reduce_column(g, A, band, c2, sw0, sw1, sp, true, &next);
+                if (!settle_q(A, Q, cc, c2, o, it, lout, lcap)) {
+                    failed = true;
+                    break;
+                }
+                c2 = next;
+            }
+        }
+        if (failed) break;
+        // the chunk is finished; the warp finishing the item opens the next one
+        int fin = 0;
+        if (lane == 0) {
+            __threadfence();
+            fin = atomicAdd(Q.done + it, cnt) + cnt == total;
+            if (fin) queue_finish_item(Q, cc, it, I.flags);
+        }
+        __syncwarp();
+    }
+}
+
+template <int T>
+__device__ void queue_heavy(const ReduceArgs& A, const QueueArgs& Q, const BlockG<T>& g, int32_t* sw0, int32_t* sw1,
+                            int32_t* sp) {
+    const Band band{INT32_MIN, nullptr, 0};
+    long long idle = 0;
+    while (true) {
+        unsigned long long pk = 0;  // bit 63: stop; else (complex << 32) | column, or all ones for none
+        if (g.leader()) {
+            if (ld_acq(Q.abort) || ld_acq(Q.finished) >= Q.ncplx) {
+                pk = 1ull << 63;
+            } else {
+                pk = ~0ull >> 1;
+                const int h = ld_acq(Q.pool_head);
+                if (h < Q.pool_cap) {
+                    const int v = ld_acq(Q.pool + h);
+                    if (v >= 0 && atomicCAS(Q.pool_head, h, h + 1) == h)
+                        pk = (uint64_t(uint32_t(Q.pool_c[h])) << 32) | uint32_t(v);
+                }
+            }
+        }
+        pk = g.bcast64(pk);
+        if (pk >> 63) break;
+        if (pk == (~0ull >> 1)) {
+            if (++idle > Q.spin_limit) {
+                if (g.leader()) queue_fail(A, Q, ERRB_TIMEOUT);
+                break;
+            }
+            if (g.leader()) __nanosleep(512);
+            continue;
+        }
+        idle = 0;
+        const int cc = int(pk >> 32);
+        int col = int(uint32_t(pk));
+        while (col >= 0) {
+            int next = -1;
+            const Outcome o = reduce_column(g, A, band, col, sw0, sw1, sp, false, &next);
+            if (!settle(g, A, col, o)) {
+                if (g.leader()) queue_fail(A, Q, ERRB_CHECK);
+                return;
+            }
+            col = next;
+        }
+        if (g.leader()) {
+            __threadfence();
+            atomicSub(Q.hpend + cc, 1);
+        }
+    }
+}
+
+// Al: warp-tier arguments (cap = level-1 capacity), Ah: CTA tier (level 2).
+template <int T>
+__global__ void __launch_bounds__(T, 1) k_reduce_queue(ReduceArgs Al, ReduceArgs Ah, QueueArgs Q) {
+    extern __shared__ __align__(16) int32_t smem[];
+    __shared__ int gsm[2 * (T / 32 + 2)];
+    __shared__ unsigned long long gsb[2];
+    if (int(blockIdx.x) < Q.heavy_ctas) {
+        BlockG<T> g;
+        g.sm = gsm;
+        g.sb = gsb;
+        queue_heavy<T>(Ah, Q, g, smem, smem + Ah.cap, smem + 2 * Ah.cap);
+    } else {
+        int32_t* sw0 = smem + size_t(threadIdx.x >> 5) * (3 * Al.cap + kHdr);
+        queue_light(Al, Q, sw0, sw0 + Al.cap, sw0 + 2 * Al.cap, T / 32);
+    }
+}
+
+// per complex and dimension: active columns, min first row over non-empty
+// columns and max low + 1 over active columns (the quantities ColumnShrink
+// computes for the whole matrix, include/specseq.h:374-398)
+__global__ void k_queue_info(int64_t n, int32_t k, const int64_t* cstart, const int32_t* perm, const int32_t* rdim,
+                             const int32_t* arena, const uint64_t* desc, const int32_t* low, const uint8_t* state,
+                             int32_t* act_cnt, int32_t* min_row, int32_t* max_row) {
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+        const uint64_t d = desc[i];
+        const uint32_t len = desc_len(d);
+        if (!len) continue;
+        const int64_t x = perm[i];
+        int32_t a = 0, b = k;  // largest a with cstart[a] <= x
+        while (b - a > 1) {
+            const int32_t mid = (a + b) >> 1;
+            if (cstart[mid] <= x) a = mid;
+            else b = mid;
+        }
+        const int dm = rdim[i];
+        const int64_t slot = int64_t(a) * kNumDims + dm;
+        atomicMin(min_row + slot, arena[desc_off(d) + kHdr]);
+        if (state[i] == ST_ACTIVE) {
+            atomicAdd(act_cnt + slot, 1);
+            atomicMax(max_row + slot, low[i] + 1);
+        }
+    }
+}
+
+int queue_complex_info(const Device& D, int32_t k, const int64_t* d_cstart, int32_t* act_cnt, int32_t* min_row,
+                       int32_t* max_row, cudaStream_t s) {
+    const int64_t m = int64_t(k) * kNumDims;
+    cudaMemsetAsync(act_cnt, 0, sizeof(int32_t) * m, s);
+    fill_i32(min_row, INT32_MAX, m, s);
+    fill_i32(max_row, -1, m, s);
+    if (D.n == 0) return 0;
+    int64_t g = (D.n + 255) / 256;
+    if (g > 65536) g = 65536;
+    k_queue_info<<<unsigned(g), 256, 0, s>>>(D.n, k, d_cstart, D.perm, D.dim, D.arena, D.desc, D.low, D.state, act_cnt,
+                                             min_row, max_row);
+    return 3;
 }
 
 int light_smem_bytes(int cap) { return 4 * (3 * cap + kHdr) * 4; }
@@ -1278,7 +1700,7 @@ void reduce_heavy_launch(const Device& D, int cap, int threads, int* ctr, int gr
 // that no launch finds it lowered below its own request.
 static cudaError_t raise_smem_limit(const void* fn, int slot, int bytes) {
     static std::mutex mu;
-    static int limit[64][3] = {};
+    static int limit[64][5] = {};
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
@@ -1288,6 +1710,40 @@ static cudaError_t raise_smem_limit(const void* fn, int slot, int bytes) {
     e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e == cudaSuccess) cur = bytes;
     return e;
+}
+
+static int queue_smem_bytes(int cap1, int cap2, int threads) {
+    const int light = (threads / 32) * (3 * cap1 + kHdr) * 4;
+    const int heavy = (3 * cap2 + kHdr) * 4;
+    return light > heavy ? light : heavy;
+}
+
+cudaError_t queue_configure(int cap1, int cap2, int threads, int* blocks_per_sm) {
+    const int smem = queue_smem_bytes(cap1, cap2, threads);
+    *blocks_per_sm = 0;
+    cudaError_t e;
+    if (threads == 256) {
+        e = raise_smem_limit(reinterpret_cast<const void*>(k_reduce_queue<256>), 3, smem);
+        if (e != cudaSuccess) return e;
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_reduce_queue<256>, 256, smem);
+    }
+    e = raise_smem_limit(reinterpret_cast<const void*>(k_reduce_queue<128>), 4, smem);
+    if (e != cudaSuccess) return e;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_reduce_queue<128>, 128, smem);
+}
+
+cudaError_t reduce_queue_launch(const Device& D, int cap1, int cap2, int threads, const QueueArgs& Q, int grid,
+                                cudaStream_t s) {
+    ReduceArgs Al = make_args(D, D.active, 0, 0, INT32_MIN, cap1, 1, nullptr);
+    ReduceArgs Ah = make_args(D, nullptr, 0, 0, INT32_MIN, cap2, 1, nullptr);
+    Al.gate_host = Ah.gate_host = nullptr;
+    Al.heavy_done = Ah.heavy_done = nullptr;
+    QueueArgs q = Q;
+    void* args[] = {&Al, &Ah, &q};
+    const int smem = queue_smem_bytes(cap1, cap2, threads);
+    if (threads == 256)
+        return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(k_reduce_queue<256>), grid, 256, args, smem, s);
+    return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(k_reduce_queue<128>), grid, 128, args, smem, s);
 }
 
 cudaError_t reduce_configure(int cap1, int cap2, int heavy_threads, int* light_blocks_per_sm,

@@ -193,11 +193,72 @@ int32_t try_built(sspp_ctx* ctx, const sspp_params& params, Request* r, Phases& 
     return rc;
 }
 
+// Several point-cloud and field requests built on the device one after
+// another and reduced as one block-diagonal batch; pairs are indices of each
+// built matrix.
+int32_t try_built_batch(sspp_ctx* ctx, const sspp_params& params, const std::vector<Request*>& b, Phases& ph) {
+    if (!ctx) {
+        for (Request* r : b) set_result(r, SSPP_ERR_CUDA, "no usable CUDA device");
+        return SSPP_ERR_CUDA;
+    }
+    std::vector<sspp_build_spec> specs(b.size());
+    for (size_t i = 0; i < b.size(); i++) {
+        const Request* r = b[i];
+        sspp_build_spec& sp = specs[i];
+        std::memset(&sp, 0, sizeof(sp));
+        sp.kind = r->kind == KIND_RIPS ? SSPP_BUILD_RIPS : SSPP_BUILD_LOWERSTAR;
+        sp.maxdim = r->maxdim;
+        sp.size[0] = r->g[0];
+        sp.size[1] = r->g[1];
+        sp.size[2] = r->kind == KIND_RIPS ? 0 : r->g[2];
+        sp.data = r->fin;
+        sp.radius = r->radius;
+    }
+    const Clock::time_point t0 = Clock::now();
+    int32_t rc = sspp_load_built_batch(ctx, int32_t(b.size()), specs.data());
+    const Clock::time_point t1 = Clock::now();
+    if (rc == SSPP_OK) rc = sspp_reduce(ctx, &params, nullptr);
+    const Clock::time_point t2 = Clock::now();
+    ph.load += ms_between(t0, t1) / 1000.0;
+    ph.reduce += ms_between(t1, t2) / 1000.0;
+    if (rc != SSPP_OK) {
+        for (Request* r : b) set_result(r, rc, sspp_last_error(ctx));
+        return rc;
+    }
+    std::vector<int64_t> np(b.size()), ne(b.size());
+    rc = sspp_batch_counts(ctx, np.data(), ne.data());
+    std::vector<int64_t*> po(b.size()), eo(b.size());
+    for (size_t i = 0; rc == SSPP_OK && i < b.size(); i++) {
+        Request* r = b[i];
+        r->npairs = np[i];
+        r->ness = ne[i];
+        r->pairs.reset(new int64_t[size_t(std::max<int64_t>(2 * np[i], 1))]);
+        r->ess.reset(new int64_t[size_t(std::max<int64_t>(ne[i], 1))]);
+        po[i] = r->pairs.get();
+        eo[i] = r->ess.get();
+        const int64_t nc = sspp_batch_values(ctx, int32_t(i), nullptr, 0);
+        if (nc < 0) {
+            rc = SSPP_ERR_CUDA;
+            break;
+        }
+        r->ncols = nc;
+        if (r->want_values) {
+            r->values.reset(new float[size_t(std::max<int64_t>(nc, 1))]);
+            if (sspp_batch_values(ctx, int32_t(i), r->values.get(), nc) != nc) rc = SSPP_ERR_CUDA;
+        }
+    }
+    if (rc == SSPP_OK) rc = sspp_batch_copy(ctx, po.data(), eo.data());
+    ph.results += ms_between(t2, Clock::now()) / 1000.0;
+    for (Request* r : b) set_result(r, rc, rc == SSPP_OK ? nullptr : sspp_last_error(ctx));
+    return rc;
+}
+
 void worker_main(sspp_server* S, int host_threads) {
     sspp_config c;
     std::memset(&c, 0, sizeof(c));
     c.device = S->cfg.device;
     c.host_threads = host_threads;
+    c.sm_share = S->cfg.workers;  // the workers' persistent reductions run side by side
     sspp_ctx* ctx = sspp_create(&c);
     const size_t max_req = S->cfg.max_batch_requests > 0 ? size_t(S->cfg.max_batch_requests) : SIZE_MAX;
     const int64_t max_cols = S->cfg.max_batch_cols > 0 ? S->cfg.max_batch_cols : INT64_MAX;
@@ -220,8 +281,8 @@ void worker_main(sspp_server* S, int host_threads) {
             int64_t cols = 0;
             while (!S->queue.empty()) {
                 Request* r = S->queue.front();
-                // built requests run alone
-                if (!batch.empty() && (r->kind != KIND_MATRIX || batch[0]->kind != KIND_MATRIX ||
+                // matrices batch with matrices, built requests with built ones
+                if (!batch.empty() && ((r->kind == KIND_MATRIX) != (batch[0]->kind == KIND_MATRIX) ||
                                        est + r->est > S->share || cols + r->ncols > max_cols ||
                                        batch.size() >= max_req || cols >= fair))
                     break;
@@ -235,7 +296,13 @@ void worker_main(sspp_server* S, int host_threads) {
         }
         Phases ph;
         if (batch[0]->kind != KIND_MATRIX) {
-            try_built(ctx, S->params, batch[0], ph);
+            if (batch.size() == 1) {
+                try_built(ctx, S->params, batch[0], ph);
+            } else {
+                int32_t rc = try_built_batch(ctx, S->params, batch, ph);
+                if (rc != SSPP_OK)  // isolate the request that failed
+                    for (Request* r : batch) try_built(ctx, S->params, r, ph);
+            }
         } else {
             int32_t rc = try_batch(ctx, S->params, batch, ph);
             if (rc != SSPP_OK && batch.size() > 1)  // isolate the request that failed

@@ -31,14 +31,20 @@ class SsppError(RuntimeError):
 
 class _Config(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("arena_bytes", ctypes.c_int64), ("verbose", ctypes.c_int32),
-                ("profile", ctypes.c_int32), ("host_threads", ctypes.c_int32)]
+                ("profile", ctypes.c_int32), ("host_threads", ctypes.c_int32), ("sm_share", ctypes.c_int32)]
 
 
 class _Params(ctypes.Structure):
     _fields_ = [("dualize", ctypes.c_int32), ("model", ctypes.c_int32), ("max_iteration", ctypes.c_int32),
                 ("ss_block_size", ctypes.c_int32), ("growth", ctypes.c_float), ("queue_size", ctypes.c_int32),
                 ("level1_capacity", ctypes.c_int32), ("level2_capacity", ctypes.c_int32),
-                ("autotune", ctypes.c_int32), ("heavy_threads", ctypes.c_int32), ("representatives", ctypes.c_int32)]
+                ("autotune", ctypes.c_int32), ("heavy_threads", ctypes.c_int32), ("representatives", ctypes.c_int32),
+                ("schedule", ctypes.c_int32)]
+
+
+class _BuildSpec(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("maxdim", ctypes.c_int32), ("size", ctypes.c_int64 * 3),
+                ("data", ctypes.c_void_p), ("radius", ctypes.c_float)]
 
 
 class _Stats(ctypes.Structure):
@@ -79,6 +85,7 @@ class Params:
     autotune: int = 0
     heavy_threads: int = 0
     representatives: int = 0
+    schedule: int = 0  # 1 (= 0) host loop of per-block launches, 2 one persistent device work-queue launch
 
     def _c(self) -> _Params:
         return _Params(*(getattr(self, f.name) for f in fields(self)))
@@ -124,6 +131,8 @@ def load_library():
         "sspp_reduce_noalloc": (i32, [i64, i64, vp, vp, vp, vp, vp, vp, ctypes.c_char_p, i32]),
         "sspp_load_batch": (i32, [vp, i32, vp, vp, vp, vp]),
         "sspp_load_batch_device": (i32, [vp, i32, vp, vp, vp, vp]),
+        "sspp_load_built_batch": (i32, [vp, i32, vp]),
+        "sspp_batch_values": (i64, [vp, i32, vp, i64]),
         "sspp_batch_num_pairs": (i64, [vp, i32]),
         "sspp_batch_pairs": (i64, [vp, i32, vp, i64]),
         "sspp_get_params": (i32, [vp, ctypes.POINTER(_Params)]),
@@ -165,7 +174,8 @@ def load_library():
 EXPORTED = ("sspp_create", "sspp_destroy", "sspp_last_error", "sspp_default_params", "sspp_load_phat",
             "sspp_load_csc", "sspp_load_csc_device", "sspp_init", "sspp_compute", "sspp_reduce", "sspp_num_pairs",
             "sspp_pairs", "sspp_num_essential", "sspp_essentials", "sspp_write_pairs", "sspp_get_stats",
-            "sspp_reduce_noalloc", "sspp_load_batch", "sspp_load_batch_device", "sspp_batch_num_pairs",
+            "sspp_reduce_noalloc", "sspp_load_batch", "sspp_load_batch_device", "sspp_load_built_batch",
+            "sspp_batch_values", "sspp_batch_num_pairs",
             "sspp_batch_pairs", "sspp_get_params", "sspp_batch_num_essential", "sspp_batch_essentials",
             "sspp_batch_counts", "sspp_batch_copy",
             "sspp_server_create", "sspp_server_destroy", "sspp_server_last_error", "sspp_server_submit",
@@ -285,6 +295,42 @@ class Engine:
         arr = lambda i: (ctypes.c_void_p * max(k, 1))(*[t[i].ctypes.data for t in keep])
         self._check(self._lib.sspp_load_batch(self._h, k, ncols.ctypes.data, arr(0), arr(1), arr(2)))
         self._batch_k = k
+
+    def load_built_batch(self, requests) -> None:
+        """Builds several complexes on the device and loads them as one batch: each request is
+        ("rips", points [npts, D], radius, maxdim) or ("lowerstar", field [gz, gy, gx], maxdim), as
+        load_rips / load_lowerstar take them; results come back per complex (batch_pairs ...)."""
+        reqs = list(requests)
+        specs = (_BuildSpec * max(len(reqs), 1))()
+        keep = []
+        for i, r in enumerate(reqs):
+            if r[0] == "rips":
+                ptr, shape, k_ = self._float_buffer(r[1], 2)
+                specs[i].kind = 0
+                specs[i].size[0], specs[i].size[1], specs[i].size[2] = shape[0], shape[1], 0
+                specs[i].radius = float(r[2])
+                specs[i].maxdim = int(r[3])
+            elif r[0] == "lowerstar":
+                ptr, shape, k_ = self._float_buffer(r[1], 3)
+                specs[i].kind = 1
+                specs[i].size[0], specs[i].size[1], specs[i].size[2] = shape[2], shape[1], shape[0]
+                specs[i].maxdim = int(r[2])
+            else:
+                raise ValueError(f"unknown request kind {r[0]!r}")
+            specs[i].data = ptr
+            keep.append(k_)
+        self._check(self._lib.sspp_load_built_batch(self._h, len(reqs), specs))
+        del keep
+        self._batch_k = len(reqs)
+
+    def batch_values(self, i: int) -> np.ndarray:
+        """Column filtration values of complex i of a built batch."""
+        n = self._lib.sspp_batch_values(self._h, i, None, 0)
+        if n < 0:
+            self._check(ERR_STATE)
+        out = np.empty(max(n, 1), dtype=np.float32)
+        self._lib.sspp_batch_values(self._h, i, out.ctypes.data, n)
+        return out[:n]
 
     def load_batch_device(self, ncols, d_dims: int, d_col_ptr: int, d_rows: int) -> None:
         nc = np.ascontiguousarray(ncols, dtype=np.int64)

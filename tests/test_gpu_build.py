@@ -204,3 +204,36 @@ def test_server_builds_point_cloud_and_field_requests():
     with Server(Params(), workers=1, memory_budget=1 << 20) as small:
         with pytest.raises(SsppError):
             small.submit_lowerstar(gen.field(40, 1.0, 1))  # larger than the budget: refused at submit
+
+
+def test_built_batch_matches_separate_builds():
+    # several point clouds and fields built one after another into one
+    # block-diagonal batch: each complex's matrix values, pairs and essentials
+    # equal those of building and reducing it alone
+    reqs = [("rips", gen.points(900, 2, 1), 0.06, 2), ("lowerstar", gen.field(11, 1.5, 5), 3),
+            ("rips", gen.points(1500, 3, 2), 0.09, 3), ("rips", gen.points(3, 3, 4), 0.01, 3),
+            ("lowerstar", np.random.default_rng(3).normal(size=(6, 8, 5)).astype(np.float32), 2),
+            ("rips", gen.points(600, 3, 8), gen.rips_radius_for_degree(600, 3, 30), 3)]
+    want = []
+    with Engine(0) as e:
+        for r in reqs:
+            if r[0] == "rips":
+                e.load_rips(r[1], r[2], r[3])
+            else:
+                e.load_lowerstar(r[1], r[2])
+            vals = e.input_matrix(values=True).values
+            e.reduce(Params())
+            want.append((e.pairs(), e.essentials(), vals))
+        for p in (Params(), Params(autotune=2), Params(schedule=1)):
+            e.load_built_batch(reqs)
+            e.reduce(p)
+            for i, (pw, ew, vw) in enumerate(want):
+                assert np.array_equal(e.batch_pairs(i), pw), (p, i)
+                assert np.array_equal(e.batch_essentials(i), ew), (p, i)
+                assert np.array_equal(e.batch_values(i).view(np.uint32), vw.view(np.uint32)), (p, i)
+        bad = gen.field(6, 1.0, 9)
+        bad[1, 2, 3] = np.nan
+        with pytest.raises(SsppError):
+            e.load_built_batch([reqs[0], ("lowerstar", bad, 3)])
+        e.load_built_batch([])
+        e.reduce(Params())
