@@ -178,11 +178,12 @@ __device__ bool dominated_by_one(const uint64_t* adj, const int64_t* off, const 
 // form), and dominated_by_one_s spreads the (w in C, neighbour of w) pairs over
 // the lanes, so every lane loads independent entries instead of walking one
 // list (C of at most 32 vertices; larger ones take the global form).
+// er: the edge's neighbour-list bounds {off[u], off[u+1], off[v], off[v+1]}
 template <class V>
-__device__ int common_nbrs_s(const uint64_t* adj, const int64_t* off, int32_t u, int32_t v, const V& ok, int32_t* C,
-                             int32_t* ea, int32_t* eb, int64_t cap, uint64_t* sl, int slcap) {
+__device__ int common_nbrs_s(const uint64_t* adj, const int64_t* off, int32_t u, int32_t v, int4 er, const V& ok,
+                             int32_t* C, int32_t* ea, int32_t* eb, int64_t cap, uint64_t* sl, int slcap) {
     const int lane = lane_id();
-    int64_t a0 = off[u], a1 = off[u + 1], b0 = off[v], b1 = off[v + 1];
+    int64_t a0 = er.x, a1 = er.y, b0 = er.z, b1 = er.w;
     if (a1 - a0 > b1 - b0) {  // walk the shorter list
         int64_t x = a0; a0 = b0; b0 = x;
         x = a1; a1 = b1; b1 = x;
@@ -235,14 +236,14 @@ __device__ int common_nbrs_s(const uint64_t* adj, const int64_t* off, int32_t u,
 }
 
 template <class V>
-__device__ bool dominated_by_one_s(const uint64_t* adj, const int64_t* off, const V& ok, const int32_t* C, int c,
-                                   int32_t* spre, int64_t* sbase, int32_t* scnt) {
+__device__ bool dominated_by_one_s(const uint64_t* adj, const int64_t* off, const int2* vrec, const V& ok,
+                                   const int32_t* C, int c, int32_t* spre, int64_t* sbase, int32_t* scnt) {
     if (c > 32) return dominated_by_one(adj, off, ok, C, c);
     const int lane = lane_id();
     int deg = 0;
     if (lane < c) {
-        const int32_t w = C[lane];
-        const int64_t s0 = off[w], s1 = off[w + 1];
+        const int2 b = vrec[C[lane]];
+        const int64_t s0 = b.x, s1 = b.y;
         deg = s1 - s0 >= c - 1 ? int(s1 - s0) : 0;  // fewer neighbours than c - 1: cannot dominate
         sbase[lane] = s0;
         scnt[lane] = 0;
@@ -278,6 +279,19 @@ __device__ bool dominated_by_one_s(const uint64_t* adj, const int64_t* off, cons
     const bool any = __any_sync(kFull, dom);
     __syncwarp();  // the scratch is rewritten by the next call
     return any;
+}
+
+// per edge and per vertex: neighbour-list bounds (int32: 2E < 2^31)
+__global__ void k_cbounds(const int32_t* misc, int64_t nv, const int32_t* eu, const int32_t* ev, const int64_t* off,
+                          int4* erec, int2* vrec) {
+    const int64_t E = misc[kMiscE];
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < E; e += stride) {
+        const int32_t u = eu[e], v = ev[e];
+        erec[e] = make_int4(int32_t(off[u]), int32_t(off[u + 1]), int32_t(off[v]), int32_t(off[v + 1]));
+    }
+    for (int64_t w = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; w < nv; w += stride)
+        vrec[w] = make_int2(int32_t(off[w]), int32_t(off[w + 1]));
 }
 
 __global__ void k_cdeg(const int32_t* misc, const int32_t* eu, const int32_t* ev, int32_t* deg) {
@@ -535,8 +549,9 @@ template <class F>
 __global__ void __launch_bounds__(256) k_cascade(const int32_t* cas, int32_t* misc, const int32_t* eu,
                                                   const int32_t* ev, const uint64_t* adj, const int64_t* off,
                                                   uint8_t* crit_g, uint8_t* ins_g, int32_t* heap, const int32_t* open,
-                                                  const int8_t* nopen, int32_t* gC, int32_t* gA, int32_t* gB,
-                                                  int64_t gcap, long long max_steps, int* err) {
+                                                  const int8_t* nopen, const int4* erec, const int2* vrec, int32_t* gC,
+                                                  int32_t* gA, int32_t* gB, int64_t gcap, long long max_steps,
+                                                  int* err) {
     extern __shared__ uint32_t sbits[];
     __shared__ int32_t sC[kCapB], sA[kCapB], sB[kCapB];
     __shared__ int32_t sheap[kHeapS];
@@ -631,13 +646,16 @@ __global__ void __launch_bounds__(256) k_cascade(const int32_t* cas, int32_t* mi
                 if (lane == 0) {
                     e = heap_pop(P.h, P.size);
                     ins.clr(e);
+                    // the next pop is usually the current top: start fetching its bounds
+                    if (P.size > 0) asm volatile("prefetch.global.L1 [%0];" ::"l"(erec + P.h[0]));
                 }
                 e = __shfl_sync(kFull, e, 0);
                 size = __shfl_sync(kFull, P.size, 0);
                 __syncwarp();
                 if (crit.get(e)) continue;
                 const ValidT<F> ok{e, t, &crit};
-                int c = common_nbrs_s(adj, off, eu[e], ev[e], ok, sC, sA, sB, kCapB, s_list, kListS);
+                const int4 er = erec[e];  // both endpoints' list bounds in one load
+                int c = common_nbrs_s(adj, off, eu[e], ev[e], er, ok, sC, sA, sB, kCapB, s_list, kListS);
                 const int32_t *C = sC, *A = sA, *B = sB;
                 if (c > kCapB) {
                     common_nbrs(adj, off, eu[e], ev[e], ok, gC, gA, gB, gcap);
@@ -645,7 +663,7 @@ __global__ void __launch_bounds__(256) k_cascade(const int32_t* cas, int32_t* mi
                     A = gA;
                     B = gB;
                 }
-                const bool dom = (c == 1) || (c >= 2 && dominated_by_one_s(adj, off, ok, C, c, s_pre, s_base, s_cnt));
+                const bool dom = (c == 1) || (c >= 2 && dominated_by_one_s(adj, off, vrec, ok, C, c, s_pre, s_base, s_cnt));
                 if (dom) continue;
                 if (lane == 0) {
                     crit.set(e);
@@ -735,7 +753,7 @@ cudaError_t grow_buf(T*& p, int64_t want, cudaStream_t s) {
 
 void collapse_free(CollapseScratch& S) {
     void* ptrs[] = {S.eu, S.ev, S.ecol, S.deg, S.adj_off, S.adj, S.arr, S.crit, S.ins, S.heap, S.cas, S.open, S.nopen,
-                    S.cbuf, S.misc};
+                    S.cbuf, S.misc, S.erec, S.vrec};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     S = CollapseScratch();
@@ -754,12 +772,13 @@ int collapse(Device& D, const DimInfo& info, uint8_t* dropped, CollapseScratch& 
     if (ne > S.cap_e) {
         if (grow_buf(S.eu, ne, s) || grow_buf(S.ev, ne, s) || grow_buf(S.ecol, ne, s) || grow_buf(S.adj, 2 * ne, s) ||
             grow_buf(S.arr, ne, s) || grow_buf(S.crit, ne, s) || grow_buf(S.ins, ne, s) || grow_buf(S.heap, ne, s) ||
-            grow_buf(S.cas, ne, s) || grow_buf(S.open, ne * kOpen, s) || grow_buf(S.nopen, ne, s))
+            grow_buf(S.cas, ne, s) || grow_buf(S.open, ne * kOpen, s) || grow_buf(S.nopen, ne, s) ||
+            grow_buf(S.erec, ne, s))
             return -1;
         S.cap_e = ne;
     }
     if (nv + 1 > S.cap_v) {
-        if (grow_buf(S.deg, nv + 1, s) || grow_buf(S.adj_off, nv + 1, s)) return -1;
+        if (grow_buf(S.deg, nv + 1, s) || grow_buf(S.adj_off, nv + 1, s) || grow_buf(S.vrec, nv + 1, s)) return -1;
         S.cap_v = nv + 1;
     }
     if (!S.misc && grow_buf(S.misc, 8, s)) return -1;
@@ -792,6 +811,10 @@ int collapse(Device& D, const DimInfo& info, uint8_t* dropped, CollapseScratch& 
         return -1;
     }
     if (E == 0) return launches;
+    if (2 * E >= int64_t(INT32_MAX)) {  // neighbour-list offsets are kept as int32
+        *err_msg = "edge collapse: more than 2^30 edges";
+        return -1;
+    }
     // adjacency: (neighbour, edge id), ascending per vertex
     cudaMemsetAsync(S.deg, 0, sizeof(int32_t) * (nv + 1), s);
     k_cdeg<<<grid_of(E, 256), 256, 0, s>>>(S.misc, S.eu, S.ev, S.deg);
@@ -804,7 +827,8 @@ int collapse(Device& D, const DimInfo& info, uint8_t* dropped, CollapseScratch& 
     cudaMemsetAsync(S.deg, 0, sizeof(int32_t) * (nv + 1), s);
     k_cfill<<<grid_of(E, 256), 256, 0, s>>>(S.misc, S.eu, S.ev, S.adj_off, S.deg, S.adj);
     k_csort<<<grid_of(nv, 128), 128, 0, s>>>(nv, S.adj_off, S.adj, S.misc);
-    launches += 6;
+    k_cbounds<<<grid_of(std::max<int64_t>(E, nv), 256), 256, 0, s>>>(S.misc, nv, S.eu, S.ev, S.adj_off, S.erec, S.vrec);
+    launches += 7;
     int32_t maxdeg = 0;
     cudaMemcpyAsync(&maxdeg, S.misc + kMiscMaxDeg, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
     if (cudaStreamSynchronize(s) != cudaSuccess) {
@@ -847,13 +871,13 @@ int collapse(Device& D, const DimInfo& info, uint8_t* dropped, CollapseScratch& 
     const size_t bits_bytes = size_t(2) * size_t((E + 31) >> 5) * sizeof(uint32_t);
     if (bits_bytes <= cascade_shared_limit()) {
         k_cascade<FlagsS><<<1, 256, bits_bytes, s>>>(S.cas, S.misc, S.eu, S.ev, S.adj, S.adj_off, S.crit, S.ins,
-                                                      S.heap, S.open, S.nopen, S.cbuf, S.cbuf + gcap,
+                                                      S.heap, S.open, S.nopen, S.erec, S.vrec, S.cbuf, S.cbuf + gcap,
                                                       S.cbuf + 2 * gcap, gcap, max_steps, D.err);
     } else {
         cudaMemsetAsync(S.ins, 0, size_t(E), s);
         k_cascade<FlagsG><<<1, 32, 0, s>>>(S.cas, S.misc, S.eu, S.ev, S.adj, S.adj_off, S.crit, S.ins, S.heap,
-                                           S.open, S.nopen, S.cbuf, S.cbuf + gcap, S.cbuf + 2 * gcap, gcap,
-                                           max_steps, D.err);
+                                           S.open, S.nopen, S.erec, S.vrec, S.cbuf, S.cbuf + gcap, S.cbuf + 2 * gcap,
+                                           gcap, max_steps, D.err);
     }
     k_drop_edges<<<grid_of(E, 256), 256, 0, s>>>(S.misc, S.crit, S.ecol, dropped);
     launches += 7;

@@ -22,6 +22,8 @@ struct CollapseScratch {
     int8_t* nopen = nullptr;     // [E] how many (-1: more than kOpen, or not listed)
     int32_t* cbuf = nullptr;     // overflow buffers of the common neighbourhoods
     int32_t* misc = nullptr;     // [8] device scalars
+    int4* erec = nullptr;        // [E] neighbour-list bounds of both endpoints {off[u], off[u+1], off[v], off[v+1]}
+    int2* vrec = nullptr;        // [nv] neighbour-list bounds {off[w], off[w+1]}
     int64_t cap_e = 0, cap_v = 0, cap_cbuf = 0;
 };
 

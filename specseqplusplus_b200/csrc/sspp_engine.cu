@@ -62,7 +62,12 @@ struct sspp_ctx {
     std::string err;
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
-    static constexpr int kSide = 32;
+#ifndef SSPP_SIDE_STREAMS
+#define SSPP_SIDE_STREAMS 64
+#endif
+    // CTA-tier launches in flight at once: each holds its stream until its
+    // longest chain ends, so a later launch needs a stream of its own
+    static constexpr int kSide = SSPP_SIDE_STREAMS;
     cudaStream_t side[kSide] = {};     // heavy-tier launches overlap later light steps and each other
     std::vector<cudaEvent_t> step_ev;  // light step k done
     cudaEvent_t join_ev[kSide] = {};   // side stream joins
@@ -89,6 +94,7 @@ struct sspp_ctx {
     int* d_gate = nullptr;         // its device address
     int* h_tail = nullptr;         // pinned: the pool tail after a dimension's sweep
     cudaEvent_t gate_ev = nullptr;
+    cudaEvent_t hc_fork = nullptr, hc_join = nullptr;  // guided clearing beside the apparent-pair pass
     long long* h_counters = nullptr;
     DimInfo* h_info = nullptr;
     unsigned long long* h_top = nullptr;
@@ -370,11 +376,12 @@ int run_collapse(sspp_ctx* ctx) {
 
 // Sizes the guided-clearing scratch from the per-dimension column ranges and
 // runs it (needs one host read of the ranges).
-int run_highclear(sspp_ctx* ctx) {
+// The branch runs on stream `s`; the sizes are read through the context's
+// stream, whose work so far (the reorder) they come from.
+int run_highclear(sspp_ctx* ctx, cudaStream_t s) {
     Device& D = ctx->D;
-    cudaStream_t s = ctx->stream;
-    CK(cudaMemcpyAsync(ctx->h_info, D.diminfo, sizeof(DimInfo), cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
+    CK(cudaMemcpyAsync(ctx->h_info, D.diminfo, sizeof(DimInfo), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
     const DimInfo info = *ctx->h_info;
     HighclearScratch& S = ctx->hc;
     int top = -1;
@@ -463,17 +470,29 @@ int run_init(sspp_ctx* ctx) {
         int rc2 = run_collapse(ctx);
         if (rc2) return rc2;
     }
-    ctx->launches += init_passes(D, lows_in_reorder, s);
-    if ((ctx->params.model & 1) && ctx->params.max_iteration > 0) {
-        int rc2 = run_highclear(ctx);
-        if (rc2) return rc2;
+    // guided clearing reads only the reordered matrix and marks top-dimension
+    // columns, the apparent-pair pass marks youngest facets (never of the top
+    // dimension): the two run side by side, the compression waits for both
+    const bool guided = (ctx->params.model & 1) && ctx->params.max_iteration > 0;
+    if (guided) {
+        cudaStream_t hs = ctx->side[0];
+        CK(cudaEventRecord(ctx->hc_fork, s));
+        CK(cudaStreamWaitEvent(hs, ctx->hc_fork, 0));
+        int rc2 = run_highclear(ctx, hs);
+        CK(cudaEventRecord(ctx->hc_join, hs));
+        if (rc2) {
+            CK(cudaStreamWaitEvent(s, ctx->hc_join, 0));
+            return rc2;
+        }
     }
+    ctx->launches += init_passes(D, lows_in_reorder, s);
+    if (guided) CK(cudaStreamWaitEvent(s, ctx->hc_join, 0));
     ctx->launches += init_compress(D, dropped_of(ctx), ctx->params.representatives != 0, ctx->params.dualize != 1, s);
     if (ctx->params.dualize == 1) {
         ctx->launches += dualize(D, 1, s);
         ctx->launches += build_apparent(D, s);
     }
-    ctx->launches += active_list(D, s);
+    ctx->launches += active_list(D, ctx->params.dualize != 1, s);
     span_end(ctx, PH_INIT, ev0);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(ctx->h_info, D.diminfo, sizeof(DimInfo), cudaMemcpyDeviceToHost, s));
@@ -870,7 +889,7 @@ int run_compute(sspp_ctx* ctx) {
         nsteps += ctx->ss_steps;
         ctx->launches += dualize(D, 2, s);
         ctx->launches += build_apparent(D, s);
-        ctx->launches += active_list(D, s);
+        ctx->launches += active_list(D, false, s);
         CK(cudaMemcpyAsync(ctx->h_info, D.diminfo, sizeof(DimInfo), cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
         ctx->hinfo = *ctx->h_info;
@@ -1047,6 +1066,11 @@ sspp_ctx* sspp_create(const sspp_config* cfg) {
             return nullptr;
         }
     }
+    if (cudaEventCreateWithFlags(&ctx->hc_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->hc_join, cudaEventDisableTiming) != cudaSuccess) {
+        delete ctx;
+        return nullptr;
+    }
     ctx->stream = ctx->own_stream;
     cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->cfg.device);
     {  // keep freed stream-ordered allocations in the pool (no release at synchronisations)
@@ -1116,6 +1140,8 @@ void sspp_destroy(sspp_ctx* ctx) {
     if (ctx->h_gate) cudaFreeHost(ctx->h_gate);
     if (ctx->h_tail) cudaFreeHost(ctx->h_tail);
     if (ctx->gate_ev) cudaEventDestroy(ctx->gate_ev);
+    if (ctx->hc_fork) cudaEventDestroy(ctx->hc_fork);
+    if (ctx->hc_join) cudaEventDestroy(ctx->hc_join);
     if (ctx->h_counters) cudaFreeHost(ctx->h_counters);
     if (ctx->h_info) cudaFreeHost(ctx->h_info);
     if (ctx->h_top) cudaFreeHost(ctx->h_top);
@@ -1688,7 +1714,7 @@ int32_t sspp_export_preprocessed(sspp_ctx* ctx, const sspp_params* p, const char
         }
         CK(cudaMemsetAsync(D.cleared, 0, size_t(n), s));
         if ((p->model & 1) && p->max_iteration > 0) {
-            rc = run_highclear(ctx);
+            rc = run_highclear(ctx, ctx->stream);
             if (rc) return rc;
         }
         std::vector<int32_t> perm(static_cast<size_t>(n));

@@ -232,10 +232,13 @@ __global__ void k_dim_starts(DimInfo* info) {
 
 // stable rank of each column inside its dimension -> reordered index
 // Also starts the init passes' per-column state of reordered column idx: no
-// leftmost column yet, no pivot owner, not cleared, not negative.
-__global__ void __launch_bounds__(kPartThreads) k_dim_assign(const int32_t* dims, int64_t n, const int32_t* dimcnt,
-                                                             const DimInfo* info, int32_t* newidx, int32_t* perm,
-                                                             int32_t* rdim, int32_t* leftmost, uint64_t* pivot,
+// leftmost column yet, no pivot owner, not cleared, not negative; and records
+// its length (rlen, read in this kernel's coalesced pass over col_ptr, so the
+// slot scan that follows reads it in reordered order without gathers).
+__global__ void __launch_bounds__(kPartThreads) k_dim_assign(const int32_t* dims, const int64_t* colptr, int64_t n,
+                                                             const int32_t* dimcnt, const DimInfo* info,
+                                                             int32_t* newidx, int32_t* perm, int32_t* rdim,
+                                                             int32_t* rlen, int32_t* leftmost, uint64_t* pivot,
                                                              uint8_t* cleared, uint8_t* negative) {
     __shared__ int wcnt[kPartThreads / 32][kNumDims];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -257,6 +260,8 @@ __global__ void __launch_bounds__(kPartThreads) k_dim_assign(const int32_t* dims
         newidx[j] = idx;
         perm[idx] = int32_t(j);
         rdim[idx] = d;
+        const int64_t len = colptr[j + 1] - colptr[j];  // validated: 0 <= len <= kMaxColLen
+        rlen[idx] = int32_t(len < 0 ? 0 : (len > kMaxColLen ? kMaxColLen : len));
         leftmost[idx] = INT_MAX;
         pivot[idx] = kNoOwner;
         cleared[idx] = 0;
@@ -264,27 +269,29 @@ __global__ void __launch_bounds__(kPartThreads) k_dim_assign(const int32_t* dims
     }
 }
 
-// Copies input column perm[i] into its padded arena slot with rows remapped to
-// reordered indices; validates range, strict order and face dimension (a face
-// of a dimension-d column must land in the reordered range of dimension d-1).
+// Copies input column j into the padded arena slot of its reordered index
+// i = newidx[j] with rows remapped to reordered indices; validates range,
+// strict order and face dimension (a face of a dimension-d column must land in
+// the reordered range of dimension d-1).  Threads walk the input columns, so
+// col_ptr and the faces are read in order and each slot is written whole.
 // With `lows` it also does the first init pass (include/kernel.h:444-457):
 // the column's lowest row, and each row's leftmost column by atomicMin (the
 // stable reorder keeps a column's rows ascending).
-__global__ void k_scatter_cols(int64_t n, const int64_t* colptr, const int32_t* rows, const int32_t* rdim,
-                               const int32_t* perm, const int32_t* newidx, const int64_t* off, const DimInfo* info,
-                               int32_t* arena, uint64_t* desc, int32_t* low, int32_t* leftmost, bool lows, int* err) {
+__global__ void k_scatter_cols(int64_t n, const int64_t* colptr, const int32_t* rows, const int32_t* dims,
+                               const int32_t* newidx, const int64_t* off, const DimInfo* info, int32_t* arena,
+                               uint64_t* desc, int32_t* low, int32_t* leftmost, bool lows, int* err) {
     __shared__ int32_t s_beg[kNumDims], s_end[kNumDims];
     if (threadIdx.x < kNumDims) {
         s_beg[threadIdx.x] = info->col_begin[threadIdx.x];
         s_end[threadIdx.x] = info->col_end[threadIdx.x];
     }
     __syncthreads();
-    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
-        const int32_t j = perm[i];
+    for (int64_t j = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; j < n; j += int64_t(gridDim.x) * blockDim.x) {
         const int64_t b = colptr[j], e = colptr[j + 1];
         const int64_t len = e - b;
+        const int32_t i = newidx[j];
         const int64_t o = off[i];
-        const int dj = rdim[i];
+        const int dj = dims[j];
         const int32_t fb = dj > 0 ? s_beg[dj - 1] : 0, fe = dj > 0 ? s_end[dj - 1] : 0;
         bool bad = len < 0 || len > kMaxColLen;
         int32_t prev = -1, last = -1;
@@ -323,16 +330,17 @@ int reorder(Device& D, bool lows, cudaStream_t s) {
     k_dim_count<<<unsigned(nb), kPartThreads, 0, s>>>(D.in_dims, n, D.dimcnt, D.err);
     k_dim_offsets<<<kNumDims, 1024, 0, s>>>(D.dimcnt, nb, D.diminfo);
     k_dim_starts<<<1, 32, 0, s>>>(D.diminfo);
-    k_dim_assign<<<unsigned(nb), kPartThreads, 0, s>>>(D.in_dims, n, D.dimcnt, D.diminfo, D.newidx, D.perm, D.dim,
-                                                       D.leftmost, D.pivot, D.cleared, D.negative);
+    // the active list is built later: until then its buffer holds the reordered lengths
+    int32_t* rlen = D.active;
+    k_dim_assign<<<unsigned(nb), kPartThreads, 0, s>>>(D.in_dims, D.in_colptr, n, D.dimcnt, D.diminfo, D.newidx,
+                                                       D.perm, D.dim, rlen, D.leftmost, D.pivot, D.cleared,
+                                                       D.negative);
     // padded column offsets in reordered order
-    const int64_t* colptr = D.in_colptr;
-    const int32_t* perm = D.perm;
     int64_t* off = D.scratch64;
-    scan([=] __device__(int64_t i) -> int64_t { int32_t j = perm[i]; return slot_ints(colptr[j + 1] - colptr[j]); },
+    scan([=] __device__(int64_t i) -> int64_t { return slot_ints(rlen[i]); },
          [=] __device__(int64_t i, int64_t pre, int64_t) { off[i] = pre; }, n, D.blk, s);
     k_scatter_cols<<<grid_for(n, 256) > 65536 ? 65536 : grid_for(n, 256), 256, 0, s>>>(
-        n, D.in_colptr, D.in_rows, D.dim, D.perm, D.newidx, off, D.diminfo, D.arena, D.desc, D.low, D.leftmost, lows,
+        n, D.in_colptr, D.in_rows, D.in_dims, D.newidx, off, D.diminfo, D.arena, D.desc, D.low, D.leftmost, lows,
         D.err);
     return 8;
 }
@@ -375,10 +383,21 @@ __global__ void k_init_apparent(int64_t n, const int32_t* arena, const uint64_t*
 // Clears positive columns and removes negative rows in place.  With `app` it
 // also writes the inline apparent columns (Device::app): a column that owns its
 // lowest row l by an apparent pair writes app[l]; a row without an owner
-// writes its own entry (each row's entry has exactly one writer).
+// writes its own entry (each row's entry has exactly one writer).  With
+// `rinfo` (non-null: the reordered dimensions) it also gathers the per-
+// dimension row bounds of the schedule (min first row over non-empty columns,
+// max lowest row + 1 over active ones; ColumnShrink, include/specseq.h:374-398)
+// into info, whose bounds must start at INT_MAX / -1.
 __global__ void k_init_compress(int64_t n, int32_t* arena, uint64_t* desc, int32_t* low, const uint64_t* pivot,
                                 const uint8_t* cleared, const uint8_t* negative, uint8_t* state,
-                                const uint8_t* dropped, bool keep_rows, int4* app, long long* counters, int* err) {
+                                const uint8_t* dropped, bool keep_rows, int4* app, const int32_t* rinfo,
+                                DimInfo* info, long long* counters, int* err) {
+    __shared__ int smin[kNumDims], smax[kNumDims];
+    if (threadIdx.x < kNumDims) {
+        smin[threadIdx.x] = INT_MAX;
+        smax[threadIdx.x] = -1;
+    }
+    __syncthreads();
     long long ncl = 0, nact = 0;
     for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
         if (app && pivot[i] == kNoOwner) app[i] = make_int4(-1, INT_MAX, INT_MAX, INT_MAX);
@@ -418,6 +437,11 @@ __global__ void k_init_compress(int64_t n, int32_t* arena, uint64_t* desc, int32
         low[i] = l;
         uint8_t st = (m == 0) ? ST_ZERO : (pv_col(pivot[l]) == int32_t(i) ? ST_OWNER : ST_ACTIVE);
         state[i] = st;
+        if (rinfo && m > 0) {
+            const int dm = rinfo[i];
+            atomicMin(&smin[dm], c[0]);
+            if (st == ST_ACTIVE) atomicMax(&smax[dm], l + 1);
+        }
         if (app && st == ST_OWNER) {
             int4 v = make_int4(-1, INT_MAX, INT_MAX, INT_MAX);
             if (m <= 4) {
@@ -435,6 +459,13 @@ __global__ void k_init_compress(int64_t n, int32_t* arena, uint64_t* desc, int32
     if ((threadIdx.x & 31) == 0) {
         if (ncl) cnt_add(&counters[CNT_CLEARED], ncl);
         if (nact) cnt_add(&counters[CNT_ACTIVE], nact);
+    }
+    if (rinfo) {
+        __syncthreads();
+        if (threadIdx.x < kNumDims) {
+            if (smin[threadIdx.x] != INT_MAX) atomicMin(&info->min_row[threadIdx.x], smin[threadIdx.x]);
+            if (smax[threadIdx.x] >= 0) atomicMax(&info->max_row[threadIdx.x], smax[threadIdx.x]);
+        }
     }
 }
 
@@ -474,12 +505,15 @@ int init_passes(Device& D, bool lows_done, cudaStream_t s) {
     return lows_done ? 1 : 2;
 }
 
-int init_compress(Device& D, const uint8_t* dropped, bool keep_rows, bool with_app, cudaStream_t s) {
+int init_compress(Device& D, const uint8_t* dropped, bool keep_rows, bool final, cudaStream_t s) {
     const int64_t n = D.n;
-    const unsigned g = grid_for(n, 256) > 65536 ? 65536 : grid_for(n, 256);
+    // the row bounds go to the DimInfo through a few atomics per block: few blocks
+    const unsigned g = grid_for(n, 256) > 4096 ? 4096 : grid_for(n, 256);
+    if (final) k_diminfo_reset<<<1, 32, 0, s>>>(D.diminfo);
     k_init_compress<<<g, 256, 0, s>>>(n, D.arena, D.desc, D.low, D.pivot, D.cleared, D.negative, D.state, dropped,
-                                      keep_rows, with_app ? D.app : nullptr, D.counters, D.err);
-    return 1;
+                                      keep_rows, final ? D.app : nullptr, final ? D.dim : nullptr, D.diminfo,
+                                      D.counters, D.err);
+    return final ? 2 : 1;
 }
 
 // Inline copies of the short apparent columns, by row (see Device::app).
@@ -519,7 +553,7 @@ __global__ void k_act_segments(const int64_t* actpos, int64_t n, DimInfo* info) 
     }
 }
 
-int active_list(Device& D, cudaStream_t s) {
+int active_list(Device& D, bool rows_done, cudaStream_t s) {
     const int64_t n = D.n;
     const uint8_t* state = D.state;
     int32_t* act = D.active;
@@ -533,6 +567,7 @@ int active_list(Device& D, cudaStream_t s) {
     // pos[n] = total
     cudaMemcpyAsync(pos + n, D.blk + scan_blocks(n), sizeof(int64_t), cudaMemcpyDeviceToDevice, s);
     k_act_segments<<<1, 32, 0, s>>>(pos, n, D.diminfo);
+    if (rows_done) return 4;
     k_diminfo_reset<<<1, 32, 0, s>>>(D.diminfo);
     const unsigned g = grid_for(n, 256) > 4096 ? 4096 : grid_for(n, 256);
     k_dim_rows<<<g, 256, 0, s>>>(n, D.dim, D.arena, D.desc, D.low, D.state, D.diminfo);

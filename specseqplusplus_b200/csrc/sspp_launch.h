@@ -34,9 +34,11 @@ int batch_localize(int64_t npairs, int64_t ness, int32_t k, const int64_t* d_cst
 int init_passes(Device& D, bool lows_done, cudaStream_t s);
 // keep_rows: leave negative rows in the columns (whole reduced columns, for
 // representative cycles); otherwise they are removed.
-// with_app: also the inline apparent columns (as build_apparent)
-int init_compress(Device& D, const uint8_t* dropped, bool keep_rows, bool with_app, cudaStream_t s);
-int active_list(Device& D, cudaStream_t s);
+// final (no dualization follows): also the inline apparent columns (as
+// build_apparent) and the per-dimension row bounds (as active_list)
+int init_compress(Device& D, const uint8_t* dropped, bool keep_rows, bool final, cudaStream_t s);
+// rows_done: init_compress already gathered the row bounds
+int active_list(Device& D, bool rows_done, cudaStream_t s);
 // D.app from the pivot table as it stands (apparent pairs only)
 int build_apparent(Device& D, cudaStream_t s);
 // anti-transpose of the compressed matrix behind the primal columns in the

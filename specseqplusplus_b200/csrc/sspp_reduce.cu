@@ -84,6 +84,14 @@ struct Band {
 
 constexpr int kMaxMergesPerColumn = 1 << 24;
 
+// A pivot entry read early, before it is known whether it is needed: relaxed,
+// so a fence (acquire) must come before the owner's slot is read through it.
+__device__ __forceinline__ uint64_t ld_relaxed_u64(const uint64_t* p) {
+    uint64_t v;
+    asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
 __device__ __forceinline__ uint64_t ld_acquire_u64(const uint64_t* p) {
     uint64_t v;
     asm volatile("ld.acquire.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
@@ -613,6 +621,9 @@ constexpr int kCacheRefill = 16;  // cache lanes used before the cache is filled
 #ifndef SSPP_FAST_TOGGLE3
 #define SSPP_FAST_TOGGLE3 0
 #endif
+#ifndef SSPP_FAST_PVPF
+#define SSPP_FAST_PVPF 0
+#endif
 
 // largest entry of an inline apparent column below its top (-1 if none)
 __device__ __forceinline__ int app_max_below(int4 q) {
@@ -644,6 +655,10 @@ __device__ int fast_adds(const BlockG<T>& g, const ReduceArgs& A, int32_t minrow
         // loaded while that addition runs: one of them is usually the next low
         int pf_row = -1;
         int4 pf_ap = make_int4(-1, 0, 0, 0);
+        uint64_t pf_pv = kNoOwner;  // ... and their pivot entries (relaxed), for owners that are not inline
+        bool have_pf_pv = false;    // ec_pf below holds the current low's prefetched entry
+        uint64_t ec_pf = kNoOwner;
+        int next_clear = kClearCheck;  // additions before the next look at the cleared flag
         bool have_e = true;  // ec is the pivot entry of Lc
         // toggles x in the delta (a fold into the bulk when the delta is full
         // invalidates the bulk cache)
@@ -718,8 +733,15 @@ __device__ int fast_adds(const BlockG<T>& g, const ReduceArgs& A, int32_t minrow
             d = nd;
         };
         while (done < iters_left && nb + d > 0 && Lc >= minrow) {
+            if (done >= next_clear) {  // cleared meanwhile: the general path stops the column
+                next_clear = done + kClearCheck;
+                unsigned c = 0;
+                if (lane == 0) c = ld_acquire_u8(A.cleared + col);
+                if (__shfl_sync(kFull, c, 0)) break;
+            }
             // the inline apparent column of the current low: from the bulk
             // cache when the low is the bulk top, else one load
+            have_pf_pv = false;  // set below only when the prefetch holds this low's entry
             int4 ap;
             int h = -1;
             if (top_in_bulk) {
@@ -750,6 +772,8 @@ __device__ int fast_adds(const BlockG<T>& g, const ReduceArgs& A, int32_t minrow
                 ap.y = __shfl_sync(kFull, ap.y, src);
                 ap.z = __shfl_sync(kFull, ap.z, src);
                 ap.w = __shfl_sync(kFull, ap.w, src);
+                have_pf_pv = pm != 0 && ap.x < 0 && SSPP_FAST_PREFETCH && SSPP_FAST_PVPF;
+                if (have_pf_pv) ec_pf = __shfl_sync(kFull, (unsigned long long)pf_pv, src);
             }
             if (top_in_bulk && ap.x >= 0) {
                 // a run from cache lane h: lane l (> h) joins while lanes h..l-1
@@ -833,9 +857,17 @@ __device__ int fast_adds(const BlockG<T>& g, const ReduceArgs& A, int32_t minrow
                 bj = lane == 0 ? ap.y : (lane == 1 ? ap.z : ap.w);
             } else {
                 if (!have_e) {
-                    uint64_t t = 0;
-                    if (lane == 0) t = ld_acquire_u64(A.pivot + Lc);
-                    ec = __shfl_sync(kFull, (unsigned long long)t, 0);
+                    if (have_pf_pv) {
+                        // read early (relaxed): an older entry still names an earlier
+                        // column with this low, whose published versions never change;
+                        // the fence orders the slot reads after it
+                        ec = ec_pf;
+                        __threadfence();
+                    } else {
+                        uint64_t t = 0;
+                        if (lane == 0) t = ld_acquire_u64(A.pivot + Lc);
+                        ec = __shfl_sync(kFull, (unsigned long long)t, 0);
+                    }
                     have_e = true;
                 }
                 if (pv_col(ec) >= col) break;                         // claim: the general path
@@ -855,6 +887,7 @@ __device__ int fast_adds(const BlockG<T>& g, const ReduceArgs& A, int32_t minrow
             if (SSPP_FAST_PREFETCH && lane < m && lane >= m - 3 && bj >= 0 && bj < A.ncols) {
                 pf_row = bj;
                 pf_ap = __ldg(A.app + bj);
+                if (SSPP_FAST_PVPF) pf_pv = ld_relaxed_u64(A.pivot + bj);
             }
             if (top_in_bulk) {  // the tops cancel
                 nb--;
@@ -921,6 +954,96 @@ __device__ int fast_adds(const BlockG<T>& g, const ReduceArgs& A, int32_t minrow
         add_ints += fs.add_ints;
     }
     __syncthreads();  // fs is rewritten by the next call
+    return done;
+}
+
+// Warp tier, inline apparent addends.  A working column of at most 32 entries
+// is held in registers, one entry per lane, ascending; while the owner of its
+// lowest row is an inline apparent column (Device::app), an addition removes
+// the top and toggles the addend's other entries in place (a ballot and a
+// shuffle each), with no staging and no shared-memory merge, and the inline
+// columns of the addend's entries load during the addition (one of them is
+// usually the next low).  Stops at a row without such an owner, below the
+// band, or when the column would outgrow 32 entries or the buffer; the column
+// goes back to w.buf.  Returns the additions done, or -1 after a failed
+// self-check.
+#ifndef SSPP_WARP_REG
+#define SSPP_WARP_REG 1
+#endif
+__device__ int warp_adds(const ReduceArgs& A, int32_t minrow, Work& w, int& L, uint64_t& e, int4 ap, long long& adds,
+                         long long& add_ints, int iters_left) {
+    const int lane = threadIdx.x & 31;
+    int len = w.len;
+    int ev = lane < len ? lds(w.buf + lane) : INT_MAX;
+    int Lc = L, done = 0;
+    bool bad = false;
+    long long ai = 0;
+    int pf_row = -1;
+    int4 pf_ap = make_int4(-1, 0, 0, 0);
+    while (done < iters_left && ap.x >= 0) {
+        const int m = ap.x;
+        if (len - 1 + m > 32 || len - 1 + m > A.cap) break;
+        const int bj = lane == 0 ? ap.y : (lane == 1 ? ap.z : ap.w);
+        pf_row = -1;
+        if (lane < m && bj >= 0 && bj < A.ncols) {
+            pf_row = bj;
+            pf_ap = __ldg(A.app + bj);
+        }
+        len--;  // the tops cancel
+        if (lane == len) ev = INT_MAX;
+        for (int j = 0; j < m; j++) {
+            const int x = j == 0 ? ap.y : (j == 1 ? ap.z : ap.w);
+            const unsigned eq = __ballot_sync(kFull, lane < len && ev == x);
+            if (eq) {
+                const int q = __ffs(eq) - 1;
+                const int nx = __shfl_down_sync(kFull, ev, 1);
+                if (lane >= q) ev = lane + 1 < len ? nx : INT_MAX;
+                len--;
+            } else {
+                const int q = __popc(__ballot_sync(kFull, lane < len && ev < x));
+                const int pv = __shfl_up_sync(kFull, ev, 1);
+                if (lane > q && lane <= len) ev = pv;
+                if (lane == q) ev = x;
+                len++;
+            }
+        }
+        ai += 2 * len + m + 2;
+        done++;
+        const int nl = len > 0 ? __shfl_sync(kFull, ev, (len - 1) & 31) : -1;
+        if (nl >= Lc) {  // self-check: the lowest row only moves down
+            bad = true;
+            break;
+        }
+        Lc = nl;
+        if (Lc < 0 || Lc < minrow) break;
+        const unsigned pm = __ballot_sync(kFull, pf_row == Lc);
+        const int src = pm ? __ffs(pm) - 1 : 31;
+        int4 q4 = pf_ap;
+        if (!pm) {
+            q4 = make_int4(-1, 0, 0, 0);
+            if (lane == 31 && Lc < A.ncols) q4 = __ldg(A.app + Lc);
+        }
+        ap.x = __shfl_sync(kFull, q4.x, src);
+        ap.y = __shfl_sync(kFull, q4.y, src);
+        ap.z = __shfl_sync(kFull, q4.z, src);
+        ap.w = __shfl_sync(kFull, q4.w, src);
+    }
+    if (bad) {
+        if (lane == 0) atomicOr(A.err, ERRB_CHECK);
+        return -1;
+    }
+    if (done > 0) {
+        if (lane < pad4(len)) w.buf[lane] = lane < len ? ev : INT_MAX;
+        __syncwarp();
+        w.len = len;
+        w.dirty = true;
+        L = Lc;
+        uint64_t t = kNoOwner;
+        if (lane == 0 && Lc >= 0 && Lc >= minrow) t = ld_acquire_u64(A.pivot + Lc);
+        e = __shfl_sync(kFull, (unsigned long long)t, 0);
+        adds += done;
+        add_ints += ai;
+    }
     return done;
 }
 
@@ -1062,6 +1185,17 @@ __device__ Outcome reduce_column(const G& g, const ReduceArgs& A, const Band& ba
         if constexpr (G::kSize > 32) {  // CTA tier: short addends by one warp
             if (!w.global) {
                 const int done = fast_adds(g, A, minrow, col, w, L, e, w.buf == sw0 ? sw1 : sw0, sp, adds, add_ints,
+                                           kMaxMergesPerColumn - iter);
+                if (done < 0) break;
+                if (done > 0) {
+                    iter += done;
+                    apc = app_of(L);
+                    continue;
+                }
+            }
+        } else if (SSPP_WARP_REG) {  // warp tier: the column in registers
+            if (!w.global && apc.x >= 0 && w.len <= 32) {
+                const int done = warp_adds(A, minrow, w, L, e, apc, adds, add_ints,
                                            min(kClearCheck, kMaxMergesPerColumn - iter));
                 if (done < 0) break;
                 if (done > 0) {

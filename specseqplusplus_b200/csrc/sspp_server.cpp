@@ -274,9 +274,11 @@ void worker_main(sspp_server* S, int host_threads) {
                                     [&] { return S->stop || S->queue.size() >= max_req; });
                 if (S->queue.empty()) continue;  // another worker took them
             }
-            // a fair share of the queued columns, so that the other workers'
-            // batches (and their copies) overlap with this one
-            const int64_t fair = (S->queued_cols + S->cfg.workers - 1) / S->cfg.workers;
+            // half a fair share of the queued columns, so that every worker
+            // gets two or more batches and their copies, builds and
+            // reductions overlap on the device
+            const int64_t share_of = 2 * int64_t(S->cfg.workers);
+            const int64_t fair = (S->queued_cols + share_of - 1) / share_of;
             double est = 0;
             int64_t cols = 0;
             while (!S->queue.empty()) {
@@ -445,9 +447,10 @@ int64_t sspp_server_submit_rips(sspp_server* S, int64_t npts, int32_t space_dim,
     r->maxdim = maxdim;
     r->want_values = (flags & SSPP_SUBMIT_VALUES) != 0;
     take_floats(r.get(), points, npts * space_dim, flags);
-    // the size is known once built; the queue counts 16 columns per point
-    r->ncols = 16 * npts;
-    r->nnz = 40 * npts;
+    // the size is known once built; for batching the queue counts the
+    // columns of a complex of mean degree 24 (1 + 12 + 48 + 96 per point in 3-D)
+    r->ncols = (space_dim == 3 ? 157 : 61) * npts;
+    r->nnz = 4 * r->ncols;
     r->est = 0;
     return enqueue(S, std::move(r));
 }
