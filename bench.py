@@ -45,6 +45,7 @@ import subprocess
 import sys
 import tempfile
 import time
+import threading
 
 import numpy as np
 
@@ -70,9 +71,55 @@ def dist_info():
 
 
 class Clocks:
-    """nvidia-smi clock/throttle sampling during the timed region."""
+    """SM clock and throttle-reason sampling during the timed region.
+
+    NVML is read every 5 ms from a thread (a timed region of ~100 ms gets ~20
+    samples); without NVML, nvidia-smi is polled every 200 ms instead.  Only
+    reads: no clock or other GPU setting is touched.
+    """
+
+    _NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, device):
+        self.sm, self.mx, self.reasons = [], 0.0, set()
+        self.p = self.thread = None
+        self.done = threading.Event()
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            try:
+                import torch
+
+                uuid = str(torch.cuda.get_device_properties(device).uuid)
+                h = pynvml.nvmlDeviceGetHandleByUUID("GPU-" + uuid if not uuid.startswith("GPU-") else uuid)
+            except Exception:
+                h = pynvml.nvmlDeviceGetHandleByIndex(device)
+            self.mx = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+            bits = dict(zip(self._NAMES, (pynvml.nvmlClocksEventReasonHwSlowdown,
+                                          pynvml.nvmlClocksEventReasonHwThermalSlowdown,
+                                          pynvml.nvmlClocksEventReasonSwThermalSlowdown,
+                                          pynvml.nvmlClocksEventReasonSwPowerCap)))
+            first = threading.Event()
+
+            def run():
+                while True:
+                    try:
+                        self.sm.append(float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)))
+                        r = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                        self.reasons.update(n for n, b in bits.items() if r & b)
+                    except Exception:
+                        pass
+                    first.set()
+                    if self.done.wait(0.005):
+                        return
+
+            self.thread = threading.Thread(target=run, daemon=True)
+            self.thread.start()
+            first.wait(2.0)
+            return
+        except Exception:
+            self.thread = None
         self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -84,6 +131,10 @@ class Clocks:
             self.p = None
 
     def stop(self):
+        if self.thread is not None:
+            self.done.set()
+            self.thread.join(timeout=5)
+            return self._summary("nvml")
         if self.p is None:
             return None
         self.p.terminate()
@@ -93,24 +144,26 @@ class Clocks:
             self.p.kill()
         self.f.flush()
         self.f.seek(0)
-        sm, mx, reasons = [], 0.0, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in self.f.read().splitlines():
             parts = [x.strip() for x in line.split(",")]
             if len(parts) < 9:
                 continue
             try:
-                sm.append(float(parts[1]))
-                mx = max(mx, float(parts[2]))
+                self.sm.append(float(parts[1]))
+                self.mx = max(self.mx, float(parts[2]))
             except ValueError:
                 continue
-            for nm, v in zip(names, parts[5:9]):
+            for nm, v in zip(self._NAMES, parts[5:9]):
                 if v.lower() == "active":
-                    reasons.add(nm)
+                    self.reasons.add(nm)
         os.unlink(self.f.name)
-        if not sm:
+        return self._summary("nvidia-smi")
+
+    def _summary(self, source):
+        if not self.sm:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": statistics.median(self.sm), "sm_max_mhz": self.mx, "reasons": sorted(self.reasons),
+                "samples": len(self.sm), "source": source}
 
 
 def load_peaks():

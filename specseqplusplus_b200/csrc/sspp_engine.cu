@@ -564,17 +564,19 @@ int dimension_gate(sspp_ctx* ctx) {
     return SSPP_OK;
 }
 
+constexpr int kStepCtr = 8;  // counters per spectral-sequence step (see ReduceArgs::ctr)
+
 int run_steps(sspp_ctx* ctx, const std::vector<Step>& steps, int cap1, int cap2, int ht) {
     Device& D = ctx->D;
     cudaStream_t s = ctx->stream;
     const sspp_params& P = ctx->params;
-    if (4 * int64_t(steps.size()) > D.cap_steps) {
+    if (kStepCtr * int64_t(steps.size()) > D.cap_steps) {
         if (D.step_ctr) cudaFreeAsync(D.step_ctr, s);
         D.step_ctr = nullptr;
         D.cap_steps = 0;
-        CK(grow(D.step_ctr, D.cap_steps, 4 * int64_t(steps.size()) + 64, s));
+        CK(grow(D.step_ctr, D.cap_steps, kStepCtr * int64_t(steps.size()) + 64, s));
     }
-    if (!steps.empty()) CK(cudaMemsetAsync(D.step_ctr, 0, sizeof(int) * 4 * steps.size(), s));
+    if (!steps.empty()) CK(cudaMemsetAsync(D.step_ctr, 0, sizeof(int) * kStepCtr * steps.size(), s));
     // heavy pool: deferrals are rare (heavy columns and displaced owners); a
     // full pool sets the capacity bit and the run is repeated with a larger one
     const int64_t want_pool = std::max<int64_t>(ctx->pool_request, std::max<int64_t>(D.n / 4, 1 << 16));
@@ -627,12 +629,12 @@ int run_steps(sspp_ctx* ctx, const std::vector<Step>& steps, int cap1, int cap2,
         int64_t chunks = (int64_t(st.end - st.beg) + chunk - 1) / chunk;
         int grid = int(std::min<int64_t>(std::min<int64_t>((chunks + 3) / 4, light_max), q_blocks));
         grid = std::max(grid, 1);
-        int* ctr = D.step_ctr + 4 * k;
+        int* ctr = D.step_ctr + kStepCtr * k;
         cudaEvent_t a = nullptr, b = nullptr;
         span_begin(ctx, a);
-        reduce_light_launch(D, D.active, st.beg, st.end, st.minrow, cap1, chunk, ctr, grid, s);
+        reduce_light_launch(D, D.active, st.beg, st.end, st.minrow, cap1, chunk, ctr,
+                            k + 1 < steps.size() ? ctr + kStepCtr : nullptr, grid, s);
         span_end(ctx, PH_LIGHT, a);
-        heavy_slice_mark(D, ctr, k + 1 < steps.size() ? ctr + 4 : nullptr, s);
         if (overlap && (!last_of_dim || gate)) {
             // an idle side stream if there is one: a CTA-tier launch lasts as
             // long as its longest chain, and a launch queued behind it on the
@@ -660,7 +662,7 @@ int run_steps(sspp_ctx* ctx, const std::vector<Step>& steps, int cap1, int cap2,
         }
         ctx->light_launches++;
         ctx->heavy_launches++;
-        ctx->launches += 3;
+        ctx->launches += 2;
         if (gate && last_of_dim && k + 1 < steps.size()) {
             int rcg = dimension_gate(ctx);
             if (rcg) return rcg;

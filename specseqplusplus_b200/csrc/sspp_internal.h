@@ -120,7 +120,7 @@ struct Device {
     DimInfo* diminfo = nullptr;
     int* err = nullptr;
     long long* counters = nullptr;
-    int* step_ctr = nullptr;     // per-step work counters (4 ints per step)
+    int* step_ctr = nullptr;     // per-step work counters (8 ints per step)
     int32_t* heavy = nullptr;    // pool of columns handed to the CTA tier, appended step after step
     int64_t pool_cap = 0;
     int* pool_tail = nullptr;

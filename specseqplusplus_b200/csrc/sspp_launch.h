@@ -103,9 +103,10 @@ cudaError_t reduce_queue_launch(const Device& D, int cap1, int cap2, int threads
 
 cudaError_t reduce_configure(int cap1, int cap2, int heavy_threads, int* light_blocks_per_sm,
                              int* heavy_blocks_per_sm);
+// ctr: the step's 8 counters; the launch's last block also marks the step's
+// CTA-tier pool slice (ctr[2], and ctr_next[1] of the next step when given)
 void reduce_light_launch(const Device& D, const int32_t* active, int32_t beg, int32_t end, int32_t minrow, int cap,
-                         int chunk, int* ctr, int grid, cudaStream_t s);
-void heavy_slice_mark(const Device& D, int* ctr_k, int* ctr_next, cudaStream_t s);
+                         int chunk, int* ctr, int* ctr_next, int grid, cudaStream_t s);
 void reduce_heavy_launch(const Device& D, int cap, int threads, int* ctr, int grid, cudaStream_t s);
 
 }  // namespace sspp

@@ -60,7 +60,9 @@ struct ReduceArgs {
     uint64_t* pivot;
     uint8_t* state;
     uint8_t* cleared;
-    int* ctr;             // per step: [0] chunk counter, [1] [2] heavy pool range, [3] heavy pull counter
+    int* ctr;             // per step: [0] chunk counter, [1] [2] heavy pool range, [3] heavy pull counter,
+                          // [4] warp-tier blocks finished
+    int* ctr_next;        // the next step's counters (its pool range starts where this step's ends), or null
     int32_t* heavy;       // heavy pool (columns handed to the CTA tier, appended in step order)
     int* pool_tail;
     int* heavy_done;      // pool columns finished by the CTA tier
@@ -1358,6 +1360,22 @@ __device__ __forceinline__ bool settle(const G& g, const ReduceArgs& A, int col,
     return o != OUT_FAIL;
 }
 
+// The last warp-tier block of a step to finish marks the step's slice of the
+// CTA-tier pool: it ends at the pool tail, where the next step's slice starts
+// (every deferral of the step is appended before its block finishes).
+__device__ void light_block_done(const ReduceArgs& A) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(A.ctr + 4, 1) == int(gridDim.x) - 1) {
+            __threadfence();
+            const int t = ld_acquire(A.pool_tail);
+            A.ctr[2] = t;
+            if (A.ctr_next) A.ctr_next[1] = t;
+        }
+    }
+}
+
 // Light tier: warps take `chunk` window entries at a time and reduce the
 // runnable ones (active, not cleared, lowest row inside the band).
 __global__ void __launch_bounds__(128) k_reduce_light(ReduceArgs A) {
@@ -1370,7 +1388,8 @@ __global__ void __launch_bounds__(128) k_reduce_light(ReduceArgs A) {
     const int count = A.end - A.beg;
     const int chunk = A.chunk;
     const Band band{A.minrow, A.ctr, count};
-    while (true) {
+    bool stop = false;  // warp-uniform: a failure ends this warp's work
+    while (!stop) {
         int base = 0;
         if (lane == 0) base = atomicAdd(A.ctr, chunk);
         base = g.bcast(base);
@@ -1384,18 +1403,22 @@ __global__ void __launch_bounds__(128) k_reduce_light(ReduceArgs A) {
                   __ldcg(A.low + c) >= A.minrow;
         }
         unsigned m = __ballot_sync(kFull, run);
-        while (m) {
+        while (m && !stop) {
             const int src = __ffs(m) - 1;
             m &= m - 1;
             int col = __shfl_sync(kFull, c, src);
             while (col >= 0) {  // the column, then any owner it displaced
                 int next = -1;
                 Outcome o = reduce_column(g, A, band, col, sw0, sw1, sp, true, &next);
-                if (!settle(g, A, col, o)) return;
+                if (!settle(g, A, col, o)) {
+                    stop = true;
+                    break;
+                }
                 col = next;
             }
         }
     }
+    light_block_done(A);
 }
 
 // Heavy tier: one CTA per deferred column, buffers of the level-2 capacity.
@@ -1794,6 +1817,7 @@ static ReduceArgs make_args(const Device& D, const int32_t* active, int32_t beg,
     A.state = D.state;
     A.cleared = D.cleared;
     A.ctr = ctr;
+    A.ctr_next = nullptr;
     A.heavy = D.heavy;
     A.pool_tail = D.pool_tail;
     A.heavy_done = D.heavy_done;
@@ -1807,19 +1831,10 @@ static ReduceArgs make_args(const Device& D, const int32_t* active, int32_t beg,
 }
 
 void reduce_light_launch(const Device& D, const int32_t* active, int32_t beg, int32_t end, int32_t minrow, int cap,
-                         int chunk, int* ctr, int grid, cudaStream_t s) {
-    k_reduce_light<<<grid, 128, light_smem_bytes(cap), s>>>(make_args(D, active, beg, end, minrow, cap, chunk, ctr));
-}
-
-// step k's slice of the heavy pool ends where the pool tail is now; the next step's slice starts there
-__global__ void k_pool_mark(const int* pool_tail, int* ctr_k, int* ctr_next) {
-    int t = *pool_tail;
-    ctr_k[2] = t;
-    if (ctr_next) ctr_next[1] = t;
-}
-
-void heavy_slice_mark(const Device& D, int* ctr_k, int* ctr_next, cudaStream_t s) {
-    k_pool_mark<<<1, 1, 0, s>>>(D.pool_tail, ctr_k, ctr_next);
+                         int chunk, int* ctr, int* ctr_next, int grid, cudaStream_t s) {
+    ReduceArgs A = make_args(D, active, beg, end, minrow, cap, chunk, ctr);
+    A.ctr_next = ctr_next;
+    k_reduce_light<<<grid, 128, light_smem_bytes(cap), s>>>(A);
 }
 
 void reduce_heavy_launch(const Device& D, int cap, int threads, int* ctr, int grid, cudaStream_t s) {
