@@ -50,6 +50,8 @@ import threading
 import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
+# 32 hardware work queues for the engine's side streams, before any CUDA context
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 sys.path.insert(0, ROOT)
 
 GRID, SIGMA, SEED = 64, 2.0, 2
@@ -63,7 +65,8 @@ def workload_config(n, nnz):
             "ncols": n, "nnz": nnz, "grid": GRID, "sigma": SIGMA, "seed": SEED, "model": MODEL,
             "max_iteration": MAX_ITER, "ss_block_size": SS, "growth": GROWTH, "queue_size": QUEUE,
             "level1_capacity": L1, "level2_capacity": L2, "dualize": 0, "index": "int32", "values": "float32",
-            "l2": "flushed between steps (256 MiB write); inputs (149 MB) also exceed L2"}
+            "l2": "flushed between steps (256 MiB write); inputs (149 MB) also exceed L2",
+            "hw_queues": os.environ.get("CUDA_DEVICE_MAX_CONNECTIONS")}
 
 
 def dist_info():

@@ -31,6 +31,17 @@
 
 using namespace sspp;
 
+// CTA-tier launches of successive spectral-sequence steps run on separate side
+// streams.  The driver maps streams onto CUDA_DEVICE_MAX_CONNECTIONS hardware
+// work queues (8 by default), and launches on streams that share a queue wait
+// for each other: a short launch queued behind a long chain of another step.
+// When the library is loaded, ask for the maximum (32) unless the variable is
+// set; it applies to a CUDA context created afterwards (for a program linked
+// against the library, every context).
+__attribute__((constructor)) static void sspp_request_hw_queues() {
+    setenv("CUDA_DEVICE_MAX_CONNECTIONS", "32", 0);
+}
+
 namespace {
 enum Phase { PH_INIT = 0, PH_LIGHT, PH_HEAVY, PH_PAIRS, PH_NUM };
 
@@ -185,7 +196,7 @@ void free_device(Device& D) {
     void* ptrs[] = {D.dim, D.perm, D.newidx, D.scratch64, D.arena, D.arena_top,
                     D.desc, D.low, D.pivot, D.state, D.cleared, D.negative, D.leftmost, D.active, D.blk, D.dimcnt,
                     D.diminfo, D.err, D.counters, D.step_ctr, D.heavy, D.pool_tail, D.heavy_done, D.death_of, D.pairs,
-                    D.ess, D.misc, D.app};
+                    D.ess, D.misc, D.app, D.runlist};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     D = Device();
@@ -215,6 +226,7 @@ int ensure_columns(sspp_ctx* ctx, int64_t n, int64_t nnz) {
         CK(g(D.negative, 1));
         CK(g(D.leftmost, 1));
         CK(g(D.active, 1));
+        CK(g(D.runlist, 1));
         CK(g(D.death_of, 1));
         CK(g(D.pairs, 2));
         CK(g(D.ess, 1));
@@ -593,7 +605,18 @@ int run_steps(sspp_ctx* ctx, const std::vector<Step>& steps, int cap1, int cap2,
 #ifndef SSPP_LIGHT_CHUNK
 #define SSPP_LIGHT_CHUNK 8
 #endif
-    const int chunk = SSPP_LIGHT_CHUNK;  // window entries a warp takes per fetch
+#ifndef SSPP_LIGHT_FILTER
+#define SSPP_LIGHT_FILTER 1
+#endif
+#ifndef SSPP_FILTER_CHUNK
+#define SSPP_FILTER_CHUNK 1
+#endif
+    // Each step first lists its runnable columns (k_light_filter, one thread
+    // per window entry), then warps take them SSPP_FILTER_CHUNK at a time;
+    // without the filter, warps walk the window SSPP_LIGHT_CHUNK entries at a
+    // time through one shared counter.
+    const bool filtered = SSPP_LIGHT_FILTER != 0;
+    const int chunk = filtered ? SSPP_FILTER_CHUNK : SSPP_LIGHT_CHUNK;
     // Heavy launches go to side streams (round robin) after their light step:
     // they overlap the following light steps and each other, so long chains of
     // different steps run concurrently.  Each dimension's completion sweep, and
@@ -632,8 +655,15 @@ int run_steps(sspp_ctx* ctx, const std::vector<Step>& steps, int cap1, int cap2,
         int* ctr = D.step_ctr + kStepCtr * k;
         cudaEvent_t a = nullptr, b = nullptr;
         span_begin(ctx, a);
-        reduce_light_launch(D, D.active, st.beg, st.end, st.minrow, cap1, chunk, ctr,
-                            k + 1 < steps.size() ? ctr + kStepCtr : nullptr, grid, s);
+        int* ctr_next = k + 1 < steps.size() ? ctr + kStepCtr : nullptr;
+        if (filtered) {
+            const int fgrid = int(std::max<int64_t>(
+                1, std::min<int64_t>((int64_t(st.end - st.beg) + 255) / 256, int64_t(ctx->num_sms) * 8)));
+            reduce_light_filtered_launch(D, st.beg, st.end, st.minrow, cap1, chunk, ctr, ctr_next, fgrid, grid, s);
+            ctx->launches++;
+        } else {
+            reduce_light_launch(D, D.active, st.beg, st.end, st.minrow, cap1, chunk, ctr, ctr_next, grid, s);
+        }
         span_end(ctx, PH_LIGHT, a);
         if (overlap && (!last_of_dim || gate)) {
             // an idle side stream if there is one: a CTA-tier launch lasts as

@@ -112,6 +112,7 @@ struct Device {
     uint8_t* negative = nullptr;
     int32_t* leftmost = nullptr;
     int32_t* active = nullptr;
+    int32_t* runlist = nullptr;  // [n] a step's runnable columns (warp tier input)
     // block-scan scratch
     int64_t* blk = nullptr;      // block sums
     int64_t cap_blk = 0;

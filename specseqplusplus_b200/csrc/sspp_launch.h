@@ -107,6 +107,11 @@ cudaError_t reduce_configure(int cap1, int cap2, int heavy_threads, int* light_b
 // CTA-tier pool slice (ctr[2], and ctr_next[1] of the next step when given)
 void reduce_light_launch(const Device& D, const int32_t* active, int32_t beg, int32_t end, int32_t minrow, int cap,
                          int chunk, int* ctr, int* ctr_next, int grid, cudaStream_t s);
+// The same step in two launches: k_light_filter lists the window's runnable
+// columns (active[beg, end)) in D.runlist, then the warp tier takes them
+// `chunk` at a time.
+void reduce_light_filtered_launch(const Device& D, int32_t beg, int32_t end, int32_t minrow, int cap, int chunk,
+                                  int* ctr, int* ctr_next, int filter_grid, int grid, cudaStream_t s);
 void reduce_heavy_launch(const Device& D, int cap, int threads, int* ctr, int grid, cudaStream_t s);
 
 }  // namespace sspp

@@ -61,7 +61,8 @@ struct ReduceArgs {
     uint8_t* state;
     uint8_t* cleared;
     int* ctr;             // per step: [0] chunk counter, [1] [2] heavy pool range, [3] heavy pull counter,
-                          // [4] warp-tier blocks finished
+                          // [4] warp-tier blocks finished, [5] runnable columns listed by k_light_filter
+    const int* count;     // when set, the work is active[beg, beg + *count) (a filtered list)
     int* ctr_next;        // the next step's counters (its pool range starts where this step's ends), or null
     int32_t* heavy;       // heavy pool (columns handed to the CTA tier, appended in step order)
     int* pool_tail;
@@ -1360,6 +1361,48 @@ __device__ __forceinline__ bool settle(const G& g, const ReduceArgs& A, int col,
     return o != OUT_FAIL;
 }
 
+// The runnable columns of a step: window entries that are active, not cleared
+// and whose lowest row lies in the band (low >= minrow), listed in window
+// order within each block (one atomic per block pass) and counted in ctr[5].
+// One thread per entry reads the flags with independent loads, so the warp
+// tier then takes runnable columns one at a time instead of walking the whole
+// window with a shared counter.  A flag set concurrently (a cleared flag from
+// the previous dimension's CTA tier) is read again by the warp tier.
+constexpr int kFilterThreads = 256;
+
+__global__ void __launch_bounds__(kFilterThreads) k_light_filter(const int32_t* active, int32_t beg, int32_t end,
+                                                                 int32_t minrow, const uint8_t* state,
+                                                                 const uint8_t* cleared, const int32_t* low,
+                                                                 int32_t* out, int* ctr) {
+    __shared__ int s_warp[kFilterThreads / 32];
+    __shared__ int s_base;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int64_t b0 = beg + int64_t(blockIdx.x) * kFilterThreads; b0 < end; b0 += int64_t(gridDim.x) * kFilterThreads) {
+        const int64_t i = b0 + threadIdx.x;
+        int32_t c = -1;
+        bool r = false;
+        if (i < end) {
+            c = __ldcs(active + i);
+            r = __ldcg(state + c) == ST_ACTIVE && !__ldcg(cleared + c) && __ldcg(low + c) >= minrow;
+        }
+        const unsigned m = __ballot_sync(kFull, r);
+        if (lane == 0) s_warp[wid] = __popc(m);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int t = 0;
+            for (int w = 0; w < kFilterThreads / 32; w++) {
+                const int x = s_warp[w];
+                s_warp[w] = t;
+                t += x;
+            }
+            s_base = t ? atomicAdd(ctr + 5, t) : 0;
+        }
+        __syncthreads();
+        if (r) out[s_base + s_warp[wid] + __popc(m & ((1u << lane) - 1))] = c;
+        __syncthreads();  // s_warp and s_base are rewritten by the next pass
+    }
+}
+
 // The last warp-tier block of a step to finish marks the step's slice of the
 // CTA-tier pool: it ends at the pool tail, where the next step's slice starts
 // (every deferral of the step is appended before its block finishes).
@@ -1385,7 +1428,8 @@ __global__ void __launch_bounds__(128) k_reduce_light(ReduceArgs A) {
     int32_t* sw0 = smem + size_t(threadIdx.x >> 5) * (3 * A.cap + kHdr);
     int32_t* sw1 = sw0 + A.cap;
     int32_t* sp = sw1 + A.cap;
-    const int count = A.end - A.beg;
+    const int count = A.count ? __ldcg(A.count) : A.end - A.beg;
+    const int end = A.beg + count;
     const int chunk = A.chunk;
     const Band band{A.minrow, A.ctr, count};
     bool stop = false;  // warp-uniform: a failure ends this warp's work
@@ -1397,7 +1441,7 @@ __global__ void __launch_bounds__(128) k_reduce_light(ReduceArgs A) {
         const int idx = A.beg + base + lane;
         int c = -1;
         bool run = false;
-        if (lane < chunk && idx < A.end) {
+        if (lane < chunk && idx < end) {
             c = A.active[idx];
             run = ld_acquire_u8(A.state + c) == ST_ACTIVE && !ld_acquire_u8(A.cleared + c) &&
                   __ldcg(A.low + c) >= A.minrow;
@@ -1818,6 +1862,7 @@ static ReduceArgs make_args(const Device& D, const int32_t* active, int32_t beg,
     A.cleared = D.cleared;
     A.ctr = ctr;
     A.ctr_next = nullptr;
+    A.count = nullptr;
     A.heavy = D.heavy;
     A.pool_tail = D.pool_tail;
     A.heavy_done = D.heavy_done;
@@ -1834,6 +1879,16 @@ void reduce_light_launch(const Device& D, const int32_t* active, int32_t beg, in
                          int chunk, int* ctr, int* ctr_next, int grid, cudaStream_t s) {
     ReduceArgs A = make_args(D, active, beg, end, minrow, cap, chunk, ctr);
     A.ctr_next = ctr_next;
+    k_reduce_light<<<grid, 128, light_smem_bytes(cap), s>>>(A);
+}
+
+void reduce_light_filtered_launch(const Device& D, int32_t beg, int32_t end, int32_t minrow, int cap, int chunk,
+                                  int* ctr, int* ctr_next, int filter_grid, int grid, cudaStream_t s) {
+    k_light_filter<<<filter_grid, kFilterThreads, 0, s>>>(D.active, beg, end, minrow, D.state, D.cleared, D.low,
+                                                          D.runlist, ctr);
+    ReduceArgs A = make_args(D, D.runlist, 0, 0, minrow, cap, chunk, ctr);
+    A.ctr_next = ctr_next;
+    A.count = ctr + 5;
     k_reduce_light<<<grid, 128, light_smem_bytes(cap), s>>>(A);
 }
 
