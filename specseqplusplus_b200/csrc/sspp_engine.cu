@@ -107,6 +107,7 @@ struct sspp_ctx {
     cudaEvent_t gate_ev = nullptr;
     cudaEvent_t hc_fork = nullptr, hc_join = nullptr;  // guided clearing beside the apparent-pair pass
     long long* h_counters = nullptr;
+    unsigned long long* h_dimtot = nullptr;  // pinned: columns per dimension (validation pass)
     DimInfo* h_info = nullptr;
     unsigned long long* h_top = nullptr;
     uint8_t* dropped = nullptr;    // primal reordered numbering (model bit 2)
@@ -196,7 +197,7 @@ void free_device(Device& D) {
     void* ptrs[] = {D.dim, D.perm, D.newidx, D.scratch64, D.arena, D.arena_top,
                     D.desc, D.low, D.pivot, D.state, D.cleared, D.negative, D.leftmost, D.active, D.blk, D.dimcnt,
                     D.diminfo, D.err, D.counters, D.step_ctr, D.heavy, D.pool_tail, D.heavy_done, D.death_of, D.pairs,
-                    D.ess, D.misc, D.app, D.runlist};
+                    D.ess, D.misc, D.app, D.runlist, D.dimtot};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     D = Device();
@@ -245,6 +246,7 @@ int ensure_columns(sspp_ctx* ctx, int64_t n, int64_t nnz) {
         CK(cudaMalloc(&D.pool_tail, sizeof(int)));
         CK(cudaMalloc(&D.heavy_done, sizeof(int)));
         CK(cudaMalloc(&D.misc, sizeof(int64_t) * 8));
+        CK(cudaMalloc(&D.dimtot, sizeof(unsigned long long) * kNumDims));
     }
     return SSPP_OK;
 }
@@ -386,15 +388,33 @@ int run_collapse(sspp_ctx* ctx) {
     return SSPP_OK;
 }
 
+// Reordered column ranges of the dimensions from the validation pass's counts
+// (the reorder groups columns by ascending dimension, stably).
+DimInfo ranges_of_counts(const unsigned long long* cnt) {
+    DimInfo r{};
+    int64_t s = 0;
+    for (int d = 0; d < kNumDims; d++) {
+        r.col_begin[d] = int32_t(s);
+        s += int64_t(cnt[d]);
+        r.col_end[d] = int32_t(s);
+    }
+    return r;
+}
+
 // Sizes the guided-clearing scratch from the per-dimension column ranges and
-// runs it (needs one host read of the ranges).
-// The branch runs on stream `s`; the sizes are read through the context's
-// stream, whose work so far (the reorder) they come from.
-int run_highclear(sspp_ctx* ctx, cudaStream_t s) {
+// runs it on stream `s`.  `ranges` gives the ranges; without it they are read
+// back through the context's stream, whose work so far (the reorder) they
+// come from.
+int run_highclear(sspp_ctx* ctx, cudaStream_t s, const DimInfo* ranges = nullptr) {
     Device& D = ctx->D;
-    CK(cudaMemcpyAsync(ctx->h_info, D.diminfo, sizeof(DimInfo), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
-    const DimInfo info = *ctx->h_info;
+    DimInfo info;
+    if (ranges) {
+        info = *ranges;
+    } else {
+        CK(cudaMemcpyAsync(ctx->h_info, D.diminfo, sizeof(DimInfo), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        info = *ctx->h_info;
+    }
     HighclearScratch& S = ctx->hc;
     int top = -1;
     for (int d = kMaxDim; d >= 1; d--)
@@ -407,6 +427,10 @@ int run_highclear(sspp_ctx* ctx, cudaStream_t s) {
     CK(grow(S.deg, S.cap_deg, nv + 2, s));
     CK(grow(S.adj_off, S.cap_adj_off, nv + 2, s));
     CK(grow(S.adj, S.cap_adj, 2 * ne + 1, s));
+    if (ctx->params.max_iteration <= kMaskCandidates) {
+        CK(grow(S.adj_src, S.cap_src, 2 * ne + 1, s));
+        CK(grow(S.nmask, S.cap_nmask, 2 * ne + 1, s));
+    }
     const int64_t ntop = info.col_end[top] - info.col_begin[top];
     int64_t slots = 1024;
     while (slots < 2 * ntop) slots *= 2;
@@ -466,8 +490,10 @@ int run_init(sspp_ctx* ctx) {
     span_begin(ctx, ev0);
     ctx->launches += validate(D, s);
     CK(cudaMemcpyAsync(ctx->h_err, D.err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(ctx->h_dimtot, D.dimtot, sizeof(unsigned long long) * kNumDims, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     if (*ctx->h_err) return set_err(ctx, SSPP_ERR_BAD_INPUT, "dimension out of range 0..7 or malformed col_ptr");
+    const DimInfo ranges = ranges_of_counts(ctx->h_dimtot);
     // the reorder also does the first init pass unless an edge collapse will
     // empty columns in between (the autotuner never changes the model)
     const bool lows_in_reorder = !(ctx->params.model & 2);
@@ -490,7 +516,7 @@ int run_init(sspp_ctx* ctx) {
         cudaStream_t hs = ctx->side[0];
         CK(cudaEventRecord(ctx->hc_fork, s));
         CK(cudaStreamWaitEvent(hs, ctx->hc_fork, 0));
-        int rc2 = run_highclear(ctx, hs);
+        int rc2 = run_highclear(ctx, hs, &ranges);
         CK(cudaEventRecord(ctx->hc_join, hs));
         if (rc2) {
             CK(cudaStreamWaitEvent(s, ctx->hc_join, 0));
@@ -1127,6 +1153,7 @@ sspp_ctx* sspp_create(const sspp_config* cfg) {
     if (cudaMallocHost(&ctx->h_err, sizeof(int)) != cudaSuccess ||
         cudaMallocHost(&ctx->h_counters, sizeof(long long) * CNT_NUM) != cudaSuccess ||
         cudaMallocHost(&ctx->h_info, sizeof(DimInfo)) != cudaSuccess ||
+        cudaMallocHost(&ctx->h_dimtot, sizeof(unsigned long long) * kNumDims) != cudaSuccess ||
         cudaMallocHost(&ctx->h_top, sizeof(unsigned long long)) != cudaSuccess) {
         delete ctx;
         return nullptr;
@@ -1158,6 +1185,8 @@ void sspp_destroy(sspp_ctx* ctx) {
     if (ctx->hc.deg) cudaFree(ctx->hc.deg);
     if (ctx->hc.adj_off) cudaFree(ctx->hc.adj_off);
     if (ctx->hc.adj) cudaFree(ctx->hc.adj);
+    if (ctx->hc.adj_src) cudaFree(ctx->hc.adj_src);
+    if (ctx->hc.nmask) cudaFree(ctx->hc.nmask);
     if (ctx->hc.table) cudaFree(ctx->hc.table);
     ctx->prof.release();
     for (int q = 0; q < sspp_ctx::kSide; q++)
@@ -1176,6 +1205,7 @@ void sspp_destroy(sspp_ctx* ctx) {
     if (ctx->hc_join) cudaEventDestroy(ctx->hc_join);
     if (ctx->h_counters) cudaFreeHost(ctx->h_counters);
     if (ctx->h_info) cudaFreeHost(ctx->h_info);
+    if (ctx->h_dimtot) cudaFreeHost(ctx->h_dimtot);
     if (ctx->h_top) cudaFreeHost(ctx->h_top);
     delete ctx;
 }

@@ -126,14 +126,19 @@ __global__ void k_degree(int32_t eb, int32_t ee, const int32_t* arena, const uin
 }
 
 __global__ void k_adj_fill(int32_t eb, int32_t ee, const int32_t* arena, const uint64_t* desc, const uint8_t* dropped,
-                           const int64_t* adj_off, int32_t* fill, int32_t* adj) {
+                           const int64_t* adj_off, int32_t* fill, int32_t* adj, int32_t* src) {
     for (int64_t i = eb + blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < ee; i += int64_t(gridDim.x) * blockDim.x) {
         uint64_t ds = desc[i];
         if (desc_len(ds) != 2 || (dropped && dropped[i])) continue;
         const int32_t* c = arena + desc_off(ds) + kHdr;
         int32_t u = c[0], v = c[1];
-        adj[adj_off[u] + atomicAdd(fill + u, 1)] = v;
-        adj[adj_off[v] + atomicAdd(fill + v, 1)] = u;
+        const int64_t pu = adj_off[u] + atomicAdd(fill + u, 1), pv = adj_off[v] + atomicAdd(fill + v, 1);
+        adj[pu] = v;
+        adj[pv] = u;
+        if (src) {
+            src[pu] = u;
+            src[pv] = v;
+        }
     }
 }
 
@@ -155,20 +160,43 @@ __device__ void heap_sort(int32_t* a, int64_t n) {
     }
 }
 
+// a short list (n <= K) sorted in registers: all K loads in flight together,
+// then a bitonic sorting network (every index a compile-time constant), with
+// INT32_MAX padding that sorts to the end
+template <int K>
+__device__ __forceinline__ void sort_short(int32_t* p, int n) {
+    int32_t a[K];
+#pragma unroll
+    for (int i = 0; i < K; i++) a[i] = i < n ? p[i] : INT32_MAX;
+#pragma unroll
+    for (int k = 2; k <= K; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+#pragma unroll
+            for (int i = 0; i < K; i++) {
+                const int l = i ^ j;
+                if (l > i) {
+                    const int32_t x = a[i], y = a[l];
+                    const bool swap = ((i & k) == 0) ? (x > y) : (x < y);
+                    a[i] = swap ? y : x;
+                    a[l] = swap ? x : y;
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < K; i++)
+        if (i < n) p[i] = a[i];
+}
+
 __global__ void k_adj_sort(int64_t nv, const int64_t* adj_off, int32_t* adj) {
     for (int64_t v = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; v < nv; v += int64_t(gridDim.x) * blockDim.x) {
         int32_t* a = adj + adj_off[v];
-        int64_t n = adj_off[v + 1] - adj_off[v];
-        if (n <= 32) {
-            for (int64_t i = 1; i < n; i++) {
-                int32_t x = a[i];
-                int64_t j = i - 1;
-                while (j >= 0 && a[j] > x) { a[j + 1] = a[j]; j--; }
-                a[j + 1] = x;
-            }
-        } else {
-            heap_sort(a, n);
-        }
+        const int64_t n = adj_off[v + 1] - adj_off[v];
+        if (n <= 1) continue;
+        if (n <= 16) sort_short<16>(a, int(n));
+        else if (n <= 32) sort_short<32>(a, int(n));
+        else heap_sort(a, n);
     }
 }
 
@@ -180,6 +208,101 @@ __device__ __forceinline__ bool adj_has(const int32_t* adj, const int64_t* adj_o
         else hi = mid;
     }
     return lo < adj_off[u + 1] && adj[lo] == w;
+}
+
+// Candidate masks.  The candidates of a simplex are the first L(a) =
+// min(max_iteration, deg a) neighbours of its smallest vertex a, so whether a
+// candidate is adjacent to another vertex b of the simplex depends on the edge
+// (a, b) alone: entry (a, b) of the lists gets the bit mask of a's candidates
+// that are neighbours of b (a merge of a's first L(a) neighbours with b's
+// sorted list).  One thread per list entry; src gives the entry's vertex.
+__global__ void k_adj_masks(int64_t nv, const int32_t* src, const int32_t* adj, const int64_t* adj_off, int max_iter,
+                            uint64_t* nmask) {
+    const int64_t entries = adj_off[nv];  // the lists hold the surviving edges only
+    for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < entries; e += int64_t(gridDim.x) * blockDim.x) {
+        const int32_t a = src[e], b = adj[e];
+        const int64_t a0 = adj_off[a], b0 = adj_off[b];
+        const int64_t na = adj_off[a + 1] - a0, nb = adj_off[b + 1] - b0;
+        const int L = int(na < max_iter ? na : max_iter);
+        uint64_t m = 0;
+        int q = 0;
+        int64_t t = 0;
+        while (q < L && t < nb) {
+            const int32_t x = adj[a0 + q], y = adj[b0 + t];
+            if (x == y) m |= 1ull << q;
+            q += x <= y;
+            t += y <= x;
+        }
+        nmask[e] = m;
+    }
+}
+
+// One thread per top-dimension simplex s = (v0 < ... < vD): the candidates
+// adjacent to every vertex are the AND of the masks of the entries (v0, vj),
+// found by binary search in v0's list (every edge of a surviving simplex
+// survives); each such candidate w then needs every other facet of s + {w}
+// to exist and precede s.
+__global__ void __launch_bounds__(256) k_highclear_masks(int32_t cb, int32_t ce, int D, const int32_t* tup,
+                                                         const int32_t* adj, const int64_t* adj_off,
+                                                         const uint64_t* nmask, const int32_t* table, uint32_t mask,
+                                                         const uint8_t* dropped, uint8_t* cleared,
+                                                         long long* counters) {
+    const int k = D + 1;
+    long long found_total = 0;
+    for (int64_t i = cb + blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < ce; i += int64_t(gridDim.x) * blockDim.x) {
+        const int32_t* s = tup + (i - cb) * k;
+        int32_t sv[kMaxDim + 1];
+#pragma unroll
+        for (int j = 0; j <= kMaxDim; j++) sv[j] = j < k ? s[j] : 0;
+        if (sv[0] < 0 || (dropped && dropped[i])) continue;
+        const int64_t a0 = adj_off[sv[0]];
+        const int n0 = int(adj_off[sv[0] + 1] - a0);
+        uint64_t m = ~0ull;
+#pragma unroll
+        for (int j = 1; j <= kMaxDim; j++) {
+            if (j < k) {
+                int lo = 0, hi = n0;
+                while (lo < hi) {
+                    const int mid = (lo + hi) >> 1;
+                    if (adj[a0 + mid] < sv[j]) lo = mid + 1;
+                    else hi = mid;
+                }
+                m = (lo < n0 && adj[a0 + lo] == sv[j]) ? m & nmask[a0 + lo] : 0;
+            }
+        }
+        bool found = false;
+        while (m && !found) {
+            const int q = __ffsll(static_cast<long long>(m)) - 1;
+            m &= m - 1;
+            const int32_t w = adj[a0 + q];
+            // t = s + {w}, sorted; every facet other than s must exist and precede column i
+            int32_t t[kMaxDim + 2];
+            int c = 0;
+            bool placed = false;
+            for (int j = 0; j < k; j++) {
+                if (!placed && w < sv[j]) { t[c++] = w; placed = true; }
+                t[c++] = sv[j];
+            }
+            if (!placed) t[c++] = w;
+            bool ok = true;
+            int32_t f[kMaxDim + 1];
+            for (int drop = 0; drop <= k && ok; drop++) {
+                if (t[drop] == w) continue;  // that facet is s itself
+                int mm = 0;
+                for (int j = 0; j <= k; j++)
+                    if (j != drop) f[mm++] = t[j];
+                const int32_t col = hash_find(f, k, table, mask, tup, cb);
+                ok = col >= 0 && col < i;
+            }
+            found = ok;
+        }
+        if (found) {
+            cleared[i] = 1;
+            found_total++;
+        }
+    }
+    found_total = warp_sum(found_total);
+    if ((threadIdx.x & 31) == 0 && found_total) cnt_add(&counters[CNT_HIGHCLEAR], found_total);
 }
 
 // G lanes per top-dimension simplex (G = max_iteration rounded up to a power
@@ -306,14 +429,26 @@ int highclear(Device& D, const DimInfo& info, int max_iteration, const uint8_t* 
     scan([=] __device__(int64_t v) -> int64_t { return v < nv ? deg[v] : 0; },
          [=] __device__(int64_t v, int64_t pre, int64_t) { adj_off[v] = pre; }, nv + 1, D.blk, s);
     cudaMemsetAsync(S.deg, 0, sizeof(int32_t) * (nv + 1), s);
+    const bool masks = max_iteration <= kMaskCandidates;
     k_adj_fill<<<gridn(info.col_end[1] - info.col_begin[1], 256), 256, 0, s>>>(
-        info.col_begin[1], info.col_end[1], D.arena, D.desc, dropped, S.adj_off, S.deg, S.adj);
+        info.col_begin[1], info.col_end[1], D.arena, D.desc, dropped, S.adj_off, S.deg, S.adj,
+        masks ? S.adj_src : nullptr);
     k_adj_sort<<<gridn(nv, 128), 128, 0, s>>>(nv, S.adj_off, S.adj);
     launches += 6;
+    const int64_t ne2 = 2 * int64_t(info.col_end[1] - info.col_begin[1]);  // list entries, at most
+    if (masks) {
+        k_adj_masks<<<gridn(ne2, 256), 256, 0, s>>>(nv, S.adj_src, S.adj, S.adj_off, max_iteration, S.nmask);
+        launches++;
+    }
     // hash of the top-dimension tuples
     cudaMemsetAsync(S.table, 0xff, sizeof(int32_t) * (size_t(S.mask) + 1), s);
     const int32_t cb = info.col_begin[top], ce = info.col_end[top];
     k_hash_insert<<<gridn(ce - cb, 256), 256, 0, s>>>(cb, ce, top + 1, S.tup[top], dropped, S.table, S.mask);
+    if (masks) {
+        k_highclear_masks<<<gridn(ce - cb, 256), 256, 0, s>>>(cb, ce, top, S.tup[top], S.adj, S.adj_off, S.nmask,
+                                                             S.table, S.mask, dropped, D.cleared, D.counters);
+        return launches + 2;
+    }
     const int g = max_iteration <= 4 ? 4 : max_iteration <= 8 ? 8 : max_iteration <= 16 ? 16 : 32;
     const unsigned grid = gridn(int64_t(ce - cb) * g, kHcThreads, 148 * 64);
 #define SSPP_HC(G_)                                                                                               \

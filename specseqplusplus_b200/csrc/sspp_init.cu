@@ -67,18 +67,40 @@ void fill_i64(int64_t* p, int64_t v, int64_t n, cudaStream_t s) {
 }
 
 // Input validation before any index is used: dimensions in range and col_ptr
-// non-decreasing from 0 (device-resident inputs are only checked here).
-__global__ void k_validate(const int32_t* dims, const int64_t* colptr, int64_t n, int* err) {
-    for (int64_t j = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; j < n; j += int64_t(gridDim.x) * blockDim.x) {
-        int d = dims[j];
-        int64_t a = colptr[j], b = colptr[j + 1];
-        if (d < 0 || d > kMaxDim || b < a || b - a > kMaxColLen || (j == 0 && a != 0)) atomicOr(err, ERRB_BAD_INPUT);
+// non-decreasing from 0 (device-resident inputs are only checked here).  Also
+// counts the columns of each dimension (dimtot, zeroed before), which give
+// the host the reordered dimension ranges with the same read as the error word.
+__global__ void __launch_bounds__(256) k_validate(const int32_t* dims, const int64_t* colptr, int64_t n, int* err,
+                                                  unsigned long long* dimtot) {
+    __shared__ unsigned s_cnt[kNumDims];
+    if (threadIdx.x < kNumDims) s_cnt[threadIdx.x] = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    for (int64_t b0 = blockIdx.x * int64_t(blockDim.x); b0 < n; b0 += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t j = b0 + threadIdx.x;
+        int d = -1;
+        if (j < n) {
+            d = dims[j];
+            const int64_t a = colptr[j], b = colptr[j + 1];
+            if (d < 0 || d > kMaxDim || b < a || b - a > kMaxColLen || (j == 0 && a != 0))
+                atomicOr(err, ERRB_BAD_INPUT);
+        }
+#pragma unroll
+        for (int q = 0; q < kNumDims; q++) {
+            const unsigned m = __ballot_sync(kFull, d == q);
+            if (lane == 0 && m) atomicAdd(&s_cnt[q], unsigned(__popc(m)));
+        }
     }
+    __syncthreads();
+    if (threadIdx.x < kNumDims && s_cnt[threadIdx.x])
+        atomicAdd(dimtot + threadIdx.x, (unsigned long long)s_cnt[threadIdx.x]);
 }
 
 int validate(Device& D, cudaStream_t s) {
     if (D.n <= 0) return 0;
-    k_validate<<<grid_for(D.n, 256) > 4096 ? 4096 : grid_for(D.n, 256), 256, 0, s>>>(D.in_dims, D.in_colptr, D.n, D.err);
+    cudaMemsetAsync(D.dimtot, 0, sizeof(unsigned long long) * kNumDims, s);
+    k_validate<<<grid_for(D.n, 256) > 4096 ? 4096 : grid_for(D.n, 256), 256, 0, s>>>(D.in_dims, D.in_colptr, D.n, D.err,
+                                                                                     D.dimtot);
     return 1;
 }
 

@@ -119,6 +119,7 @@ struct Device {
     int32_t* dimcnt = nullptr;   // [nblocks * kNumDims]
     int64_t cap_dimcnt = 0;
     DimInfo* diminfo = nullptr;
+    unsigned long long* dimtot = nullptr;  // [kNumDims] input columns per dimension (validation pass)
     int* err = nullptr;
     long long* counters = nullptr;
     int* step_ctr = nullptr;     // per-step work counters (8 ints per step)

@@ -191,9 +191,10 @@ def test_bad_params_and_call_order():
 
 
 @pytest.mark.parametrize("seed,npts,r,maxiter", [(0, 300, 0.25, 50), (1, 600, 0.2, 10), (2, 2000, 0.08, 100),
-                                                  (3, 400, 0.3, 3)])
+                                                  (3, 400, 0.3, 3), (4, 500, 0.28, 64), (5, 500, 0.28, 65)])
 def test_highclear_matches_oracle(seed, npts, r, maxiter):
     # model 1: the cleared set size and the pairs match the oracle's restatement
+    # (max_iteration <= 64 runs on candidate masks, above on neighbour-list search)
     m = gen.rips(npts, 3, seed, r, 3)
     ref = oracle.reduce(m, model=1, max_iteration=maxiter)
     pairs, ess, st = run(m, Params(model=1, max_iteration=maxiter))
