@@ -405,7 +405,7 @@ DimInfo ranges_of_counts(const unsigned long long* cnt) {
 // runs it on stream `s`.  `ranges` gives the ranges; without it they are read
 // back through the context's stream, whose work so far (the reorder) they
 // come from.
-int run_highclear(sspp_ctx* ctx, cudaStream_t s, const DimInfo* ranges = nullptr) {
+int run_highclear(sspp_ctx* ctx, cudaStream_t s, const DimInfo* ranges = nullptr, bool from_input = false) {
     Device& D = ctx->D;
     DimInfo info;
     if (ranges) {
@@ -436,7 +436,7 @@ int run_highclear(sspp_ctx* ctx, cudaStream_t s, const DimInfo* ranges = nullptr
     while (slots < 2 * ntop) slots *= 2;
     CK(grow(S.table, S.cap_table, slots, s));
     S.mask = uint32_t(slots - 1);
-    ctx->launches += highclear(D, info, ctx->params.max_iteration, dropped_of(ctx), S, s);
+    ctx->launches += highclear(D, info, ctx->params.max_iteration, dropped_of(ctx), S, s, from_input);
     return SSPP_OK;
 }
 
@@ -497,7 +497,14 @@ int run_init(sspp_ctx* ctx) {
     // the reorder also does the first init pass unless an edge collapse will
     // empty columns in between (the autotuner never changes the model)
     const bool lows_in_reorder = !(ctx->params.model & 2);
-    ctx->launches += reorder(D, lows_in_reorder, s);
+    // guided clearing reads only the matrix and marks top-dimension columns,
+    // the apparent-pair pass marks youngest facets (never of the top
+    // dimension): the two run side by side and the compression waits for both.
+    // Without an edge collapse guided clearing starts as soon as the reorder
+    // has assigned the new indices (its tuples come from the input columns).
+    const bool guided = (ctx->params.model & 1) && ctx->params.max_iteration > 0;
+    const bool early = guided && !(ctx->params.model & 2);
+    ctx->launches += reorder(D, lows_in_reorder, s, early ? ctx->hc_fork : nullptr);
     CK(cudaMemcpyAsync(D.arena_top, D.blk + reorder_total_slot(D), sizeof(unsigned long long),
                        cudaMemcpyDeviceToDevice, s));
     if (ctx->user_params.autotune && !ctx->tune_locked) {
@@ -508,15 +515,11 @@ int run_init(sspp_ctx* ctx) {
         int rc2 = run_collapse(ctx);
         if (rc2) return rc2;
     }
-    // guided clearing reads only the reordered matrix and marks top-dimension
-    // columns, the apparent-pair pass marks youngest facets (never of the top
-    // dimension): the two run side by side, the compression waits for both
-    const bool guided = (ctx->params.model & 1) && ctx->params.max_iteration > 0;
     if (guided) {
         cudaStream_t hs = ctx->side[0];
-        CK(cudaEventRecord(ctx->hc_fork, s));
+        if (!early) CK(cudaEventRecord(ctx->hc_fork, s));  // after the collapse
         CK(cudaStreamWaitEvent(hs, ctx->hc_fork, 0));
-        int rc2 = run_highclear(ctx, hs, &ranges);
+        int rc2 = run_highclear(ctx, hs, &ranges, early);
         CK(cudaEventRecord(ctx->hc_join, hs));
         if (rc2) {
             CK(cudaStreamWaitEvent(s, ctx->hc_join, 0));

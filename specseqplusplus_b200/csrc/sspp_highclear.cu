@@ -37,6 +37,30 @@ static unsigned gridn(int64_t n, int t, int cap = 65536) {
     return unsigned(g);
 }
 
+// The vertex tuple of a d-simplex (d >= 1) from its first two facets c0, c1:
+// the union of their sorted d-tuples is a sorted (d+1)-tuple; all -1 if not.
+__device__ __forceinline__ void tuple_union(int d, int32_t c0, int32_t c1, int32_t fb, const int32_t* tup_f,
+                                            int32_t* out) {
+    int32_t a[kMaxDim + 1], b[kMaxDim + 1];
+    for (int k = 0; k < d; k++) {
+        a[k] = (d == 1) ? c0 : tup_f[int64_t(c0 - fb) * d + k];
+        b[k] = (d == 1) ? c1 : tup_f[int64_t(c1 - fb) * d + k];
+    }
+    int ia = 0, ib = 0, m = 0;
+    bool ok = true;
+    while ((ia < d || ib < d) && m <= d) {
+        int32_t x;
+        if (ib >= d || (ia < d && a[ia] < b[ib])) x = a[ia++];
+        else if (ia >= d || b[ib] < a[ia]) x = b[ib++];
+        else { x = a[ia++]; ib++; }
+        if (x < 0) ok = false;
+        out[m++] = x;
+    }
+    if (!ok || m != d + 1 || ia != d || ib != d) {
+        for (int k = 0; k <= d; k++) out[k] = -1;
+    }
+}
+
 // Vertex tuple of every column of dimension d >= 1 (sorted, d+1 vertices),
 // from the first two facets' tuples.  tup_d / tup_f point at the tuple arrays of
 // dims d and d-1 (dim-0 tuples are the vertex indices themselves).
@@ -51,25 +75,36 @@ __global__ void k_tuples(int32_t cb, int32_t ce, int d, int32_t fb, const int32_
             for (int k = 0; k <= d; k++) out[k] = -1;
             continue;
         }
-        int32_t a[kMaxDim + 1], b[kMaxDim + 1];
-        for (int k = 0; k < d; k++) {
-            a[k] = (d == 1) ? c[0] : tup_f[int64_t(c[0] - fb) * d + k];
-            b[k] = (d == 1) ? c[1] : tup_f[int64_t(c[1] - fb) * d + k];
+        tuple_union(d, c[0], c[1], fb, tup_f, out);
+    }
+}
+
+// The same tuples read from the input matrix through the reorder's index maps
+// (perm, newidx), so that they need only the dimension assignment, not the
+// reordered columns: a face index outside the input, or outside dimension
+// d-1, gives no tuple (the reorder reports such a matrix as malformed).
+__global__ void k_tuples_in(int32_t cb, int32_t ce, int d, int32_t fb, int32_t fe, const int32_t* perm,
+                            const int32_t* newidx, const int64_t* colptr, const int32_t* rows, int64_t n,
+                            const int32_t* tup_f, int32_t* tup_d) {
+    for (int64_t i = cb + blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < ce; i += int64_t(gridDim.x) * blockDim.x) {
+        int32_t* out = tup_d + (i - cb) * (d + 1);
+        const int64_t j = perm[i], a = colptr[j];
+        bool ok = colptr[j + 1] - a == d + 1;
+        int32_t f0 = -1, f1 = -1;
+        if (ok) {
+            const int32_t r0 = rows[a], r1 = rows[a + 1];
+            ok = r0 >= 0 && r0 < n && r1 >= 0 && r1 < n;
+            if (ok) {
+                f0 = newidx[r0];
+                f1 = newidx[r1];
+                ok = f0 >= fb && f0 < fe && f1 >= fb && f1 < fe;
+            }
         }
-        // union of two sorted d-tuples is a sorted (d+1)-tuple
-        int ia = 0, ib = 0, m = 0;
-        bool ok = true;
-        while ((ia < d || ib < d) && m <= d) {
-            int32_t x;
-            if (ib >= d || (ia < d && a[ia] < b[ib])) x = a[ia++];
-            else if (ia >= d || b[ib] < a[ia]) x = b[ib++];
-            else { x = a[ia++]; ib++; }
-            if (x < 0) ok = false;
-            out[m++] = x;
-        }
-        if (!ok || m != d + 1 || ia != d || ib != d) {
+        if (!ok) {
             for (int k = 0; k <= d; k++) out[k] = -1;
+            continue;
         }
+        tuple_union(d, f0, f1, fb, tup_f, out);
     }
 }
 
@@ -114,24 +149,22 @@ __device__ int32_t hash_find(const int32_t* t, int k, const int32_t* table, uint
 }
 
 // adjacency of the vertices (reordered vertex index = column index in [0, V))
-__global__ void k_degree(int32_t eb, int32_t ee, const int32_t* arena, const uint64_t* desc, const uint8_t* dropped,
-                         int32_t* deg) {
+// (edges from their vertex tuples, tup1 = tuples of dimension 1)
+__global__ void k_degree(int32_t eb, int32_t ee, const int32_t* tup1, const uint8_t* dropped, int32_t* deg) {
     for (int64_t i = eb + blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < ee; i += int64_t(gridDim.x) * blockDim.x) {
-        uint64_t ds = desc[i];
-        if (desc_len(ds) != 2 || (dropped && dropped[i])) continue;
-        const int32_t* c = arena + desc_off(ds) + kHdr;
-        atomicAdd(deg + c[0], 1);
-        atomicAdd(deg + c[1], 1);
+        const int2 c = reinterpret_cast<const int2*>(tup1)[i - eb];
+        if (c.x < 0 || (dropped && dropped[i])) continue;
+        atomicAdd(deg + c.x, 1);
+        atomicAdd(deg + c.y, 1);
     }
 }
 
-__global__ void k_adj_fill(int32_t eb, int32_t ee, const int32_t* arena, const uint64_t* desc, const uint8_t* dropped,
-                           const int64_t* adj_off, int32_t* fill, int32_t* adj, int32_t* src) {
+__global__ void k_adj_fill(int32_t eb, int32_t ee, const int32_t* tup1, const uint8_t* dropped, const int64_t* adj_off,
+                           int32_t* fill, int32_t* adj, int32_t* src) {
     for (int64_t i = eb + blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < ee; i += int64_t(gridDim.x) * blockDim.x) {
-        uint64_t ds = desc[i];
-        if (desc_len(ds) != 2 || (dropped && dropped[i])) continue;
-        const int32_t* c = arena + desc_off(ds) + kHdr;
-        int32_t u = c[0], v = c[1];
+        const int2 c = reinterpret_cast<const int2*>(tup1)[i - eb];
+        if (c.x < 0 || (dropped && dropped[i])) continue;
+        const int32_t u = c.x, v = c.y;
         const int64_t pu = adj_off[u] + atomicAdd(fill + u, 1), pv = adj_off[v] + atomicAdd(fill + v, 1);
         adj[pu] = v;
         adj[pv] = u;
@@ -215,23 +248,27 @@ __device__ __forceinline__ bool adj_has(const int32_t* adj, const int64_t* adj_o
 // candidate is adjacent to another vertex b of the simplex depends on the edge
 // (a, b) alone: entry (a, b) of the lists gets the bit mask of a's candidates
 // that are neighbours of b (a merge of a's first L(a) neighbours with b's
-// sorted list).  One thread per list entry; src gives the entry's vertex.
+// sorted list).  Only entries with b > a are read (a is the smallest vertex of
+// the simplex), so the others get 0.  One thread per list entry; src gives
+// the entry's vertex.
 __global__ void k_adj_masks(int64_t nv, const int32_t* src, const int32_t* adj, const int64_t* adj_off, int max_iter,
                             uint64_t* nmask) {
     const int64_t entries = adj_off[nv];  // the lists hold the surviving edges only
     for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < entries; e += int64_t(gridDim.x) * blockDim.x) {
         const int32_t a = src[e], b = adj[e];
-        const int64_t a0 = adj_off[a], b0 = adj_off[b];
-        const int64_t na = adj_off[a + 1] - a0, nb = adj_off[b + 1] - b0;
-        const int L = int(na < max_iter ? na : max_iter);
         uint64_t m = 0;
-        int q = 0;
-        int64_t t = 0;
-        while (q < L && t < nb) {
-            const int32_t x = adj[a0 + q], y = adj[b0 + t];
-            if (x == y) m |= 1ull << q;
-            q += x <= y;
-            t += y <= x;
+        if (b > a) {
+            const int64_t a0 = adj_off[a], b0 = adj_off[b];
+            const int64_t na = adj_off[a + 1] - a0, nb = adj_off[b + 1] - b0;
+            const int L = int(na < max_iter ? na : max_iter);
+            int q = 0;
+            int64_t t = 0;
+            while (q < L && t < nb) {
+                const int32_t x = adj[a0 + q], y = adj[b0 + t];
+                if (x == y) m |= 1ull << q;
+                q += x <= y;
+                t += y <= x;
+            }
         }
         nmask[e] = m;
     }
@@ -403,7 +440,7 @@ __global__ void __launch_bounds__(kHcThreads) k_highclear(int32_t cb, int32_t ce
 }
 
 int highclear(Device& D, const DimInfo& info, int max_iteration, const uint8_t* dropped, HighclearScratch& S,
-              cudaStream_t s) {
+              cudaStream_t s, bool from_input) {
     // top dimension with columns
     int top = -1;
     for (int d = kMaxDim; d >= 1; d--)
@@ -414,8 +451,13 @@ int highclear(Device& D, const DimInfo& info, int max_iteration, const uint8_t* 
     const int32_t* prev = nullptr;
     for (int d = 1; d <= top; d++) {
         int32_t cb = info.col_begin[d], ce = info.col_end[d];
-        k_tuples<<<gridn(ce - cb, 256), 256, 0, s>>>(cb, ce, d, info.col_begin[d - 1], D.arena, D.desc, prev,
-                                                    S.tup[d], D.err);
+        if (from_input)
+            k_tuples_in<<<gridn(ce - cb, 256), 256, 0, s>>>(cb, ce, d, info.col_begin[d - 1], info.col_end[d - 1],
+                                                           D.perm, D.newidx, D.in_colptr, D.in_rows, D.n, prev,
+                                                           S.tup[d]);
+        else
+            k_tuples<<<gridn(ce - cb, 256), 256, 0, s>>>(cb, ce, d, info.col_begin[d - 1], D.arena, D.desc, prev,
+                                                        S.tup[d], D.err);
         launches++;
         prev = S.tup[d];
     }
@@ -423,7 +465,7 @@ int highclear(Device& D, const DimInfo& info, int max_iteration, const uint8_t* 
     const int64_t nv = info.col_end[0] - info.col_begin[0];
     cudaMemsetAsync(S.deg, 0, sizeof(int32_t) * (nv + 1), s);
     k_degree<<<gridn(info.col_end[1] - info.col_begin[1], 256), 256, 0, s>>>(info.col_begin[1], info.col_end[1],
-                                                                            D.arena, D.desc, dropped, S.deg);
+                                                                            S.tup[1], dropped, S.deg);
     const int32_t* deg = S.deg;
     int64_t* adj_off = S.adj_off;
     scan([=] __device__(int64_t v) -> int64_t { return v < nv ? deg[v] : 0; },
@@ -431,8 +473,7 @@ int highclear(Device& D, const DimInfo& info, int max_iteration, const uint8_t* 
     cudaMemsetAsync(S.deg, 0, sizeof(int32_t) * (nv + 1), s);
     const bool masks = max_iteration <= kMaskCandidates;
     k_adj_fill<<<gridn(info.col_end[1] - info.col_begin[1], 256), 256, 0, s>>>(
-        info.col_begin[1], info.col_end[1], D.arena, D.desc, dropped, S.adj_off, S.deg, S.adj,
-        masks ? S.adj_src : nullptr);
+        info.col_begin[1], info.col_end[1], S.tup[1], dropped, S.adj_off, S.deg, S.adj, masks ? S.adj_src : nullptr);
     k_adj_sort<<<gridn(nv, 128), 128, 0, s>>>(nv, S.adj_off, S.adj);
     launches += 6;
     const int64_t ne2 = 2 * int64_t(info.col_end[1] - info.col_begin[1]);  // list entries, at most

@@ -26,7 +26,10 @@ constexpr int kMaskCandidates = 64;
 
 // Sets cleared[] for the top-dimension columns the test proves positive;
 // returns the number of kernels launched.  Buffers must be sized by the caller.
+// from_input: the vertex tuples are read from the input matrix through
+// D.perm / D.newidx (which is all it needs of the reorder: it can run beside
+// the column scatter); otherwise from the reordered columns.
 int highclear(Device& D, const DimInfo& info, int max_iteration, const uint8_t* dropped, HighclearScratch& S,
-              cudaStream_t s);
+              cudaStream_t s, bool from_input = false);
 
 }  // namespace sspp

@@ -346,7 +346,7 @@ __global__ void k_scatter_cols(int64_t n, const int64_t* colptr, const int32_t* 
 
 int64_t reorder_total_slot(const Device& D) { return scan_blocks(D.n); }
 
-int reorder(Device& D, bool lows, cudaStream_t s) {
+int reorder(Device& D, bool lows, cudaStream_t s, cudaEvent_t assigned) {
     const int64_t n = D.n;
     const int64_t nb = (n + kPartThreads - 1) / kPartThreads;
     k_dim_count<<<unsigned(nb), kPartThreads, 0, s>>>(D.in_dims, n, D.dimcnt, D.err);
@@ -357,6 +357,7 @@ int reorder(Device& D, bool lows, cudaStream_t s) {
     k_dim_assign<<<unsigned(nb), kPartThreads, 0, s>>>(D.in_dims, D.in_colptr, n, D.dimcnt, D.diminfo, D.newidx,
                                                        D.perm, D.dim, rlen, D.leftmost, D.pivot, D.cleared,
                                                        D.negative);
+    if (assigned) cudaEventRecord(assigned, s);
     // padded column offsets in reordered order
     int64_t* off = D.scratch64;
     scan([=] __device__(int64_t i) -> int64_t { return slot_ints(rlen[i]); },

@@ -19,8 +19,10 @@ int validate(Device& D, cudaStream_t s);  // sets ERRB_BAD_INPUT
 // when a face index lies outside its own complex
 int batch_rebase(int64_t n, int64_t nnz, int32_t k, const int64_t* d_cstart, const int64_t* d_estart,
                  int64_t* colptr, int32_t* rows, int* d_bad, cudaStream_t s);
-// lows: also the lowest rows and leftmost columns (the first init pass)
-int reorder(Device& D, bool lows, cudaStream_t s);
+// lows: also the lowest rows and leftmost columns (the first init pass);
+// assigned: recorded once perm / newidx / dim are written (before the columns
+// are scattered), or null
+int reorder(Device& D, bool lows, cudaStream_t s, cudaEvent_t assigned = nullptr);
 int64_t reorder_total_slot(const Device& D);  // index into D.blk of the arena total
 
 // per-complex slice starts (k+1 each) of the sorted pairs and essentials

@@ -162,8 +162,14 @@ def test_empty_and_vertex_only_inputs():
     ([0, 0, 1], [[], [], [1, 0]]),        # unsorted
     ([0, 1, 1], [[], [0], [0, 1]]),       # face of the wrong dimension
     ([0, 0, 9], [[], [], []]),            # dimension out of range
+    ([0, 0, 0, 1, 1, 1, 2], [[], [], [], [0, 1], [0, 2], [1, 2], [3, 9]]),   # triangle face out of range
+    ([0, 0, 0, 1, 1, 1, 2], [[], [], [], [0, 1], [0, 2], [1, 2], [1, 3]]),   # triangle face of the wrong dimension
+    ([0, 0, 0, 1, 1, 1, 2], [[], [], [], [0, 1], [0, 2], [1, 2], [-4, 5]]),  # negative face index
 ])
-def test_malformed_inputs_are_rejected(dims, cols):
+@pytest.mark.parametrize("model", [0, 1, 3])
+def test_malformed_inputs_are_rejected(dims, cols, model):
+    # guided clearing (model bit 1) reads the input columns beside the reorder:
+    # a bad face must still end as a malformed-input error, not a fault
     col_ptr = np.zeros(len(cols) + 1, dtype=np.int64)
     for j, c in enumerate(cols):
         col_ptr[j + 1] = col_ptr[j] + len(c)
@@ -172,8 +178,13 @@ def test_malformed_inputs_are_rejected(dims, cols):
     with Engine(0) as e:
         e.load_csc(m)
         with pytest.raises(SsppError) as ei:
-            e.reduce(Params())
+            e.reduce(Params(model=model))
         assert ei.value.code == 1
+        good = gen.lowerstar(4, 1.0, 1)  # the context stays usable
+        e.load_csc(good)
+        e.reduce(Params(model=model))
+        ref = oracle.reduce(good, model=model)
+        assert np.array_equal(e.pairs(), ref.pairs)
 
 
 def test_bad_params_and_call_order():
