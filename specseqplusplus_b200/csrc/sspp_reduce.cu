@@ -1421,7 +1421,10 @@ __device__ void light_block_done(const ReduceArgs& A) {
 
 // Light tier: warps take `chunk` window entries at a time and reduce the
 // runnable ones (active, not cleared, lowest row inside the band).
-__global__ void __launch_bounds__(128) k_reduce_light(ReduceArgs A) {
+#ifndef SSPP_LIGHT_MIN_BLOCKS
+#define SSPP_LIGHT_MIN_BLOCKS 1
+#endif
+__global__ void __launch_bounds__(128, SSPP_LIGHT_MIN_BLOCKS) k_reduce_light(ReduceArgs A) {
     extern __shared__ __align__(16) int32_t smem[];
     WarpG g;
     const int lane = g.rank();

@@ -24,6 +24,11 @@ const Knobs kCandidates[] = {
 };
 constexpr int kNumBase = int(sizeof(kCandidates) / sizeof(kCandidates[0]));
 constexpr int kRetryEvery = 32;
+// Inputs this large are not used to explore: a poor candidate there (a dual
+// reduction of a large lower-star grid takes four times as long) costs more
+// than what it could teach.  They take the lowest estimate instead: their own
+// class's mean where measured, else what similar smaller classes measured.
+constexpr int64_t kExploreMaxCols = int64_t(1) << 20;
 
 struct Entry {
     std::vector<double> mean;   // ms per million columns
@@ -94,6 +99,20 @@ int tune_choose(int64_t ncols, int32_t shape, int32_t model, int32_t dualize, in
     // untried candidates, best first by what similar classes measured; those
     // over twice as slow there as the best are left out of the first round
     const std::vector<double> prior = prior_of(k, n);
+    if (ncols >= kExploreMaxCols) {
+        double bv = HUGE_VAL;
+        for (int c = 0; c < n; c++) {
+            const double v = e.runs[size_t(c)] > 0 ? e.mean[size_t(c)] : prior[size_t(c)];
+            if (v < bv) {
+                bv = v;
+                pick = c;
+            }
+        }
+        if (pick < 0) pick = 0;  // nothing measured yet: the first candidate (best on the measured workloads)
+        *out = kCandidates[pick % kNumBase];
+        out->dualize = allow_dual ? (pick >= kNumBase ? 2 : 0) : dualize;
+        return pick;
+    }
     double best_prior = HUGE_VAL;
     for (double v : prior) best_prior = std::min(best_prior, v);
     for (int c = 0; c < n; c++) {
