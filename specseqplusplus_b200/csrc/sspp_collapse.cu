@@ -535,6 +535,173 @@ __device__ void push_partners(const int32_t* A, const int32_t* B, int c, int32_t
     __syncwarp();
 }
 
+// Speculative cascades.  Every arrival's re-examinations run at once, one warp
+// per arrival, as if no earlier arrival's cascade had kept anything: an edge
+// counts as critical when the arrival pass kept it (crit_g) or this cascade
+// did.  Each run records the edges it keeps and every vertex whose neighbour
+// list it read (the arrival's endpoints, each popped edge's endpoints, the
+// common neighbours whose lists the domination test read).  A flag this run
+// read belongs to an edge in one of those lists, so an edge that an earlier
+// cascade keeps can change the run only if one of its endpoints is among the
+// recorded vertices; the ordered pass (k_cascade) applies a record whose
+// vertices no earlier cascade touched and re-runs the others.  A run that
+// outgrows its buffers records status 1 (re-run).
+constexpr int kSpecWarps = 4;
+constexpr int kSpecHeap = 64;
+constexpr int kSpecCrit = 16;
+constexpr int kSpecScan = 64;
+constexpr int kSpecCap = 128;    // common neighbours per warp
+constexpr int kSpecList = 256;   // staged neighbour-list entries per warp
+constexpr int kSpecRec = 4 + kSpecCrit + kSpecScan;  // ints per record: status, ncrit, nscan, 0, kept, vertices
+constexpr int kSpecMaxArrivals = 1 << 18;  // records kept; later arrivals run in order
+
+// critical: kept by the arrival pass, or by this speculative cascade
+struct FlagsSpec {
+    const uint8_t* base;
+    const int32_t* loc;
+    const int* nloc;
+    __device__ __forceinline__ bool get(int32_t x) const {
+        if (base[x]) return true;
+        const int n = *nloc;
+        for (int i = 0; i < n; i++)
+            if (loc[i] == x) return true;
+        return false;
+    }
+};
+
+struct SpecWarp {
+    int32_t heap[kSpecHeap];
+    int32_t lcrit[kSpecCrit];
+    int32_t scan[kSpecScan];
+    int32_t C[kSpecCap], A[kSpecCap], B[kSpecCap];
+    uint64_t list[kSpecList];
+    int64_t sbase[32];
+    int32_t spre[32], scnt[32];
+    int nheap, nlcrit, nscan, abort;
+};
+
+__device__ __forceinline__ bool spec_in_heap(const SpecWarp& W, int32_t x) {
+    for (int i = 0; i < W.nheap; i++)
+        if (W.heap[i] == x) return true;
+    return false;
+}
+
+// lane 0: add vertex x to the recorded set
+__device__ __forceinline__ void spec_scan_add(SpecWarp& W, int32_t x) {
+    for (int i = 0; i < W.nscan; i++)
+        if (W.scan[i] == x) return;
+    if (W.nscan == kSpecScan) {
+        W.abort = 1;
+        return;
+    }
+    W.scan[W.nscan++] = x;
+}
+
+// the lanes' candidates x (want) go into the pending heap, lane order
+__device__ __forceinline__ void spec_push(SpecWarp& W, bool want, int32_t x) {
+    const int lane = lane_id();
+    const unsigned bm = __ballot_sync(kFull, want);
+    for (unsigned m = bm; m; m &= m - 1) {
+        const int src = __ffs(m) - 1;
+        const int32_t y = __shfl_sync(kFull, x, src);
+        if (lane == 0) {
+            if (W.nheap == kSpecHeap) W.abort = 1;
+            else heap_push(W.heap, W.nheap, y);
+        }
+    }
+    __syncwarp();
+}
+
+__global__ void __launch_bounds__(kSpecWarps * 32) k_cascade_spec(const int32_t* cas, const int32_t* misc,
+                                                                   const int32_t* eu, const int32_t* ev,
+                                                                   const uint64_t* adj, const int64_t* off,
+                                                                   const uint8_t* crit_g, const int32_t* open,
+                                                                   const int8_t* nopen, const int4* erec,
+                                                                   const int2* vrec, int32_t* rec, int spec_cap) {
+    __shared__ SpecWarp sw[kSpecWarps];
+    const int lane = lane_id();
+    SpecWarp& W = sw[threadIdx.x >> 5];
+    const int ncas = min(misc[kMiscCascades], spec_cap);
+    const FlagsSpec crit{crit_g, W.lcrit, &W.nlcrit};
+    for (int i = blockIdx.x * kSpecWarps + (threadIdx.x >> 5); i < ncas; i += gridDim.x * kSpecWarps) {
+        const int32_t t = cas[i];
+        const int32_t u = eu[t], v = ev[t];
+        const int no = nopen[t];
+        if (lane == 0) {
+            W.nheap = W.nlcrit = W.nscan = W.abort = 0;
+            spec_scan_add(W, u);
+            spec_scan_add(W, v);
+        }
+        __syncwarp();
+        if (no >= 0) {  // the prefilter's list: edges before t, dominated at their own arrival
+            const int32_t x = lane < no ? open[int64_t(t) * kOpen + lane] : -1;
+            const bool want = lane < no && !crit.get(x) && !spec_in_heap(W, x);
+            spec_push(W, want, x);
+        } else {
+            const ValidT<FlagsSpec> ok{t, t, nullptr};
+            const int c = common_nbrs(adj, off, u, v, ok, W.C, W.A, W.B, kSpecCap);
+            if (c > kSpecCap) {
+                if (lane == 0) W.abort = 1;
+            } else {
+                for (int base = 0; base < 2 * c; base += 32) {
+                    const int k = base + lane;
+                    const int32_t x = k < 2 * c ? (k < c ? W.A[k] : W.B[k - c]) : -1;
+                    const bool want = k < 2 * c && x < t && !crit.get(x) && !spec_in_heap(W, x);
+                    spec_push(W, want, x);
+                }
+            }
+        }
+        __syncwarp();
+        while (__shfl_sync(kFull, W.nheap > 0 && !W.abort ? 1 : 0, 0)) {
+            int32_t e = 0;
+            if (lane == 0) e = heap_pop(W.heap, W.nheap);
+            e = __shfl_sync(kFull, e, 0);
+            const int32_t a = eu[e], b = ev[e];
+            if (lane == 0) {
+                spec_scan_add(W, a);
+                spec_scan_add(W, b);
+            }
+            __syncwarp();
+            if (crit.get(e)) continue;
+            const ValidT<FlagsSpec> ok{e, t, &crit};
+            const int c = common_nbrs_s(adj, off, a, b, erec[e], ok, W.C, W.A, W.B, kSpecCap, W.list, kSpecList);
+            if (c > kSpecCap) {
+                if (lane == 0) W.abort = 1;
+                __syncwarp();
+                break;
+            }
+            const bool dom =
+                (c == 1) || (c >= 2 && dominated_by_one_s(adj, off, vrec, ok, W.C, c, W.spre, W.sbase, W.scnt));
+            if (c >= 2 && lane == 0)
+                for (int k = 0; k < c; k++) spec_scan_add(W, W.C[k]);
+            __syncwarp();
+            if (dom) continue;
+            if (lane == 0) {
+                if (W.nlcrit == kSpecCrit) W.abort = 1;
+                else W.lcrit[W.nlcrit++] = e;
+            }
+            __syncwarp();
+            for (int base = 0; base < 2 * c; base += 32) {
+                const int k = base + lane;
+                const int32_t x = k < 2 * c ? (k < c ? W.A[k] : W.B[k - c]) : -1;
+                const bool want = k < 2 * c && x < e && !crit.get(x) && !spec_in_heap(W, x);
+                spec_push(W, want, x);
+            }
+        }
+        __syncwarp();
+        int32_t* r = rec + int64_t(i) * kSpecRec;
+        if (lane == 0) {
+            r[0] = W.abort;
+            r[1] = W.nlcrit;
+            r[2] = W.nscan;
+            r[3] = 0;
+        }
+        if (lane < W.nlcrit) r[4 + lane] = W.lcrit[lane];
+        for (int k = lane; k < W.nscan; k += 32) r[4 + kSpecCrit + k] = W.scan[k];
+        __syncwarp();  // the warp's buffers are rewritten by its next arrival
+    }
+}
+
 // Arrivals of the cascade list read ahead per round of one warp: the arrival,
 // its listed partner count and its partners.
 constexpr int kAhead = 32;
@@ -551,11 +718,11 @@ __global__ void __launch_bounds__(256) k_cascade(const int32_t* cas, int32_t* mi
                                                   uint8_t* crit_g, uint8_t* ins_g, int32_t* heap, const int32_t* open,
                                                   const int8_t* nopen, const int4* erec, const int2* vrec, int32_t* gC,
                                                   int32_t* gA, int32_t* gB, int64_t gcap, long long max_steps,
-                                                  int* err) {
+                                                  int* err, const int32_t* spec, int spec_cap, int64_t nv) {
     extern __shared__ uint32_t sbits[];
     __shared__ int32_t sC[kCapB], sA[kCapB], sB[kCapB];
     __shared__ int32_t sheap[kHeapS];
-    __shared__ int32_t s_t[kAhead], s_no[kAhead];
+    __shared__ int32_t s_t[kAhead], s_no[kAhead], s_st[kAhead], s_nk[kAhead], s_ns[kAhead];
     __shared__ int32_t s_open[kAhead][kOpen];
     __shared__ uint64_t s_list[kListS];
     __shared__ int64_t s_base[32];
@@ -563,10 +730,15 @@ __global__ void __launch_bounds__(256) k_cascade(const int32_t* cas, int32_t* mi
     const int lane = lane_id();
     const int64_t E = misc[kMiscE];
     F crit, ins;
+    FlagsS dirty{nullptr};  // with spec: vertices of edges an earlier cascade kept
     if constexpr (std::is_same<F, FlagsS>::value) {
         const int64_t nw = (E + 31) >> 5;
         crit.w = sbits;
         ins.w = sbits + nw;
+        if (spec) {
+            dirty.w = sbits + 2 * nw;
+            for (int64_t k = threadIdx.x; k < ((nv + 31) >> 5); k += blockDim.x) dirty.w[k] = 0;
+        }
         for (int64_t k = threadIdx.x; k < nw; k += blockDim.x) {
             uint32_t word = 0;
             const int64_t e0 = 32 * k;
@@ -593,6 +765,7 @@ __global__ void __launch_bounds__(256) k_cascade(const int32_t* cas, int32_t* mi
     int size = 0;                        // P.size, broadcast
     long long steps = 0;
     bool fail = false;
+    bool kept_any = false;  // warp-uniform: some cascade has kept an edge (dirty is not empty)
     for (int i0 = 0; i0 < ncas && !fail; i0 += kAhead) {
         const int nb = ncas - i0 < kAhead ? ncas - i0 : kAhead;
         if (lane < nb) {  // read ahead: nothing here changes while the cascade runs
@@ -600,6 +773,14 @@ __global__ void __launch_bounds__(256) k_cascade(const int32_t* cas, int32_t* mi
             const int no = nopen[t];
             s_t[lane] = t;
             s_no[lane] = no;
+            if (spec && i0 + lane < spec_cap) {
+                const int32_t* r = spec + int64_t(i0 + lane) * kSpecRec;
+                s_st[lane] = r[0];
+                s_nk[lane] = r[1];
+                s_ns[lane] = r[2];
+            } else {
+                s_st[lane] = 1;
+            }
             if (no > 0) {
                 const int4* q = reinterpret_cast<const int4*>(open + int64_t(t) * kOpen);
                 const int4 a = q[0], b = q[1];
@@ -611,6 +792,27 @@ __global__ void __launch_bounds__(256) k_cascade(const int32_t* cas, int32_t* mi
         for (int j = 0; j < nb && !fail; j++) {
             const int32_t t = s_t[j];
             const int no = s_no[j];
+            if (spec && s_st[j] == 0) {
+                // the speculative run of this arrival stands when none of the
+                // vertices it read is an endpoint of an edge an earlier cascade kept
+                const int32_t* r = spec + int64_t(i0 + j) * kSpecRec;
+                const int nk = s_nk[j], ns = s_ns[j];
+                bool touched = false;
+                if (kept_any)
+                    for (int k = lane; k < ns; k += 32) touched |= dirty.get(r[4 + kSpecCrit + k]);
+                if (!__any_sync(kFull, touched)) {
+                    if (lane < nk) {
+                        const int32_t x = r[4 + lane];
+                        crit.set(x);
+                        crit_g[x] = 1;
+                        dirty.set(eu[x]);
+                        dirty.set(ev[x]);
+                    }
+                    kept_any = kept_any || nk > 0;
+                    __syncwarp();
+                    continue;
+                }
+            }
             if (no >= 0) {  // the prefilter's list: edges before t, dominated at their own arrival
                 const int32_t x = lane < no ? s_open[j][lane] : -1;
                 const bool want = lane < no && !crit.get(x) && !ins.get(x);
@@ -668,7 +870,12 @@ __global__ void __launch_bounds__(256) k_cascade(const int32_t* cas, int32_t* mi
                 if (lane == 0) {
                     crit.set(e);
                     crit_g[e] = 1;
+                    if (spec) {
+                        dirty.set(eu[e]);
+                        dirty.set(ev[e]);
+                    }
                 }
+                kept_any = true;
                 __syncwarp();
                 push_partners(A, B, c, e, crit, ins, sC, P);
                 size = __shfl_sync(kFull, P.size, 0);
@@ -753,7 +960,7 @@ cudaError_t grow_buf(T*& p, int64_t want, cudaStream_t s) {
 
 void collapse_free(CollapseScratch& S) {
     void* ptrs[] = {S.eu, S.ev, S.ecol, S.deg, S.adj_off, S.adj, S.arr, S.crit, S.ins, S.heap, S.cas, S.open, S.nopen,
-                    S.cbuf, S.misc, S.erec, S.vrec};
+                    S.cbuf, S.misc, S.erec, S.vrec, S.spec};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     S = CollapseScratch();
@@ -869,15 +1076,31 @@ int collapse(Device& D, const DimInfo& info, uint8_t* dropped, CollapseScratch& 
     // flags as shared-memory bitsets while they fit next to the kernel's
     // static buffers, else the global byte arrays
     const size_t bits_bytes = size_t(2) * size_t((E + 31) >> 5) * sizeof(uint32_t);
-    if (bits_bytes <= cascade_shared_limit()) {
-        k_cascade<FlagsS><<<1, 256, bits_bytes, s>>>(S.cas, S.misc, S.eu, S.ev, S.adj, S.adj_off, S.crit, S.ins,
-                                                      S.heap, S.open, S.nopen, S.erec, S.vrec, S.cbuf, S.cbuf + gcap,
-                                                      S.cbuf + 2 * gcap, gcap, max_steps, D.err);
+    const size_t spec_bytes = bits_bytes + size_t((nv + 31) >> 5) * sizeof(uint32_t);  // plus the vertex bitset
+    const size_t limit = cascade_shared_limit();
+    if (bits_bytes <= limit) {
+        // speculative cascades first, when the vertex bitset fits beside the edge flags
+        const int spec_cap = int(std::min<int64_t>(E, kSpecMaxArrivals));
+        int32_t* spec = nullptr;
+        if (spec_bytes <= limit) {
+            const int64_t want_rec = int64_t(spec_cap) * kSpecRec;
+            if (want_rec > S.cap_spec) {
+                if (grow_buf(S.spec, want_rec, s)) return -1;
+                S.cap_spec = want_rec;
+            }
+            spec = S.spec;
+            k_cascade_spec<<<grid_of(spec_cap, kSpecWarps, 148 * 16), kSpecWarps * 32, 0, s>>>(
+                S.cas, S.misc, S.eu, S.ev, S.adj, S.adj_off, S.crit, S.open, S.nopen, S.erec, S.vrec, S.spec, spec_cap);
+            launches++;
+        }
+        k_cascade<FlagsS><<<1, 256, spec ? spec_bytes : bits_bytes, s>>>(
+            S.cas, S.misc, S.eu, S.ev, S.adj, S.adj_off, S.crit, S.ins, S.heap, S.open, S.nopen, S.erec, S.vrec, S.cbuf,
+            S.cbuf + gcap, S.cbuf + 2 * gcap, gcap, max_steps, D.err, spec, spec_cap, nv);
     } else {
         cudaMemsetAsync(S.ins, 0, size_t(E), s);
         k_cascade<FlagsG><<<1, 32, 0, s>>>(S.cas, S.misc, S.eu, S.ev, S.adj, S.adj_off, S.crit, S.ins, S.heap,
                                            S.open, S.nopen, S.erec, S.vrec, S.cbuf, S.cbuf + gcap, S.cbuf + 2 * gcap,
-                                           gcap, max_steps, D.err);
+                                           gcap, max_steps, D.err, nullptr, 0, nv);
     }
     k_drop_edges<<<grid_of(E, 256), 256, 0, s>>>(S.misc, S.crit, S.ecol, dropped);
     launches += 7;

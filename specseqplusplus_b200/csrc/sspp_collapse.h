@@ -24,7 +24,8 @@ struct CollapseScratch {
     int32_t* misc = nullptr;     // [8] device scalars
     int4* erec = nullptr;        // [E] neighbour-list bounds of both endpoints {off[u], off[u+1], off[v], off[v+1]}
     int2* vrec = nullptr;        // [nv] neighbour-list bounds {off[w], off[w+1]}
-    int64_t cap_e = 0, cap_v = 0, cap_cbuf = 0;
+    int32_t* spec = nullptr;     // speculative cascade records, one per arrival with re-examinations
+    int64_t cap_e = 0, cap_v = 0, cap_cbuf = 0, cap_spec = 0;
 };
 
 // Marks dropped[] (reordered numbering) for the edges the collapse removes and
