@@ -39,7 +39,7 @@ namespace {
 constexpr int kWarpsA = 8;     // arrival kernel: warps per block
 constexpr int kCapA = 256;     // common neighbours in shared memory per warp (arrival kernel)
 constexpr int kCapB = 2048;    // common neighbours in shared memory (re-examination kernel)
-constexpr int kMiscE = 0, kMiscMaxDeg = 1, kMiscCascades = 2, kMiscSteps = 3;
+constexpr int kMiscE = 0, kMiscMaxDeg = 1, kMiscCascades = 2, kMiscSteps = 3, kMiscFirst = 4;
 constexpr int kOpen = 8;       // partners listed per arrival by the prefilter
 
 unsigned grid_of(int64_t n, int threads, int64_t cap = 65536) {
@@ -552,7 +552,9 @@ constexpr int kSpecCrit = 16;
 constexpr int kSpecScan = 64;
 constexpr int kSpecCap = 128;    // common neighbours per warp
 constexpr int kSpecList = 256;   // staged neighbour-list entries per warp
-constexpr int kSpecRec = 4 + kSpecCrit + kSpecScan;  // ints per record: status, ncrit, nscan, 0, kept, vertices
+// record: status, kept count, vertex count, 0, kept edges, their endpoints, vertices
+constexpr int kRecKept = 4, kRecKA = kRecKept + kSpecCrit, kRecKB = kRecKA + kSpecCrit, kRecScan = kRecKB + kSpecCrit;
+constexpr int kSpecRec = kRecScan + kSpecScan;
 constexpr int kSpecMaxArrivals = 1 << 18;  // records kept; later arrivals run in order
 
 // critical: kept by the arrival pass, or by this speculative cascade
@@ -571,7 +573,7 @@ struct FlagsSpec {
 
 struct SpecWarp {
     int32_t heap[kSpecHeap];
-    int32_t lcrit[kSpecCrit];
+    int32_t lcrit[kSpecCrit], lca[kSpecCrit], lcb[kSpecCrit];  // kept edges and their endpoints
     int32_t scan[kSpecScan];
     int32_t C[kSpecCap], A[kSpecCap], B[kSpecCap];
     uint64_t list[kSpecList];
@@ -677,8 +679,13 @@ __global__ void __launch_bounds__(kSpecWarps * 32) k_cascade_spec(const int32_t*
             __syncwarp();
             if (dom) continue;
             if (lane == 0) {
-                if (W.nlcrit == kSpecCrit) W.abort = 1;
-                else W.lcrit[W.nlcrit++] = e;
+                if (W.nlcrit == kSpecCrit) {
+                    W.abort = 1;
+                } else {
+                    W.lca[W.nlcrit] = a;
+                    W.lcb[W.nlcrit] = b;
+                    W.lcrit[W.nlcrit++] = e;
+                }
             }
             __syncwarp();
             for (int base = 0; base < 2 * c; base += 32) {
@@ -696,9 +703,64 @@ __global__ void __launch_bounds__(kSpecWarps * 32) k_cascade_spec(const int32_t*
             r[2] = W.nscan;
             r[3] = 0;
         }
-        if (lane < W.nlcrit) r[4 + lane] = W.lcrit[lane];
-        for (int k = lane; k < W.nscan; k += 32) r[4 + kSpecCrit + k] = W.scan[k];
+        if (lane < W.nlcrit) {
+            r[kRecKept + lane] = W.lcrit[lane];
+            r[kRecKA + lane] = W.lca[lane];
+            r[kRecKB + lane] = W.lcb[lane];
+        }
+        for (int k = lane; k < W.nscan; k += 32) r[kRecScan + k] = W.scan[k];
         __syncwarp();  // the warp's buffers are rewritten by its next arrival
+    }
+}
+
+// Which speculative runs are exact, in parallel: if every record before i is
+// exact, the edges those cascades keep are their recorded ones, so record i is
+// exact when it completed and none of its vertices is an endpoint of an edge
+// kept by a record before it (first_mark: the smallest record index keeping an
+// edge at each vertex).  misc[kMiscFirst] gets the first record that is not
+// exact (the ordered pass starts there); every record before it is applied at
+// once.
+__global__ void k_spec_marks(int32_t* misc, const int32_t* rec, int spec_cap, int32_t* first_mark) {
+    const int n = min(misc[kMiscCascades], spec_cap);
+    if (blockIdx.x == 0 && threadIdx.x == 0) misc[kMiscFirst] = n;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int32_t* r = rec + int64_t(i) * kSpecRec;
+        if (r[0] != 0) continue;
+        for (int k = 0; k < r[1]; k++) {
+            atomicMin(first_mark + r[kRecKA + k], i);
+            atomicMin(first_mark + r[kRecKB + k], i);
+        }
+    }
+}
+
+__global__ void k_spec_first(int32_t* misc, const int32_t* rec, int spec_cap, const int32_t* first_mark) {
+    const int n = min(misc[kMiscCascades], spec_cap);
+    const int lane = lane_id();
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += (gridDim.x * blockDim.x) >> 5) {
+        const int32_t* r = rec + int64_t(i) * kSpecRec;
+        bool bad = r[0] != 0;
+        const int ns = r[2];
+        for (int k = lane; k < ns && !bad; k += 32) bad = first_mark[r[kRecScan + k]] < i;
+        if (__any_sync(kFull, bad) && lane == 0) atomicMin(misc + kMiscFirst, i);
+    }
+}
+
+// also the ordered pass's starting vertex bitset: the vertices of the edges
+// the applied records keep (first_mark below the first inexact record)
+__global__ void k_spec_apply(const int32_t* misc, const int32_t* rec, uint8_t* crit_g, const int32_t* first_mark,
+                             int64_t nv, uint32_t* dirty_words) {
+    const int n = misc[kMiscFirst];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int32_t* r = rec + int64_t(i) * kSpecRec;
+        for (int k = 0; k < r[1]; k++) crit_g[r[kRecKept + k]] = 1;
+    }
+    const int lane = lane_id();
+    const int64_t nwords = (nv + 31) >> 5;
+    for (int64_t w = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; w < nwords;
+         w += (int64_t(gridDim.x) * blockDim.x) >> 5) {
+        const int64_t v = 32 * w + lane;
+        const unsigned bits = __ballot_sync(kFull, v < nv && first_mark[v] < n);
+        if (lane == 0) dirty_words[w] = bits;
     }
 }
 
@@ -718,7 +780,8 @@ __global__ void __launch_bounds__(256) k_cascade(const int32_t* cas, int32_t* mi
                                                   uint8_t* crit_g, uint8_t* ins_g, int32_t* heap, const int32_t* open,
                                                   const int8_t* nopen, const int4* erec, const int2* vrec, int32_t* gC,
                                                   int32_t* gA, int32_t* gB, int64_t gcap, long long max_steps,
-                                                  int* err, const int32_t* spec, int spec_cap, int64_t nv) {
+                                                  int* err, const int32_t* spec, int spec_cap, int64_t nv,
+                                                  const uint32_t* dirty_words) {
     extern __shared__ uint32_t sbits[];
     __shared__ int32_t sC[kCapB], sA[kCapB], sB[kCapB];
     __shared__ int32_t sheap[kHeapS];
@@ -729,15 +792,21 @@ __global__ void __launch_bounds__(256) k_cascade(const int32_t* cas, int32_t* mi
     __shared__ int32_t s_pre[32], s_cnt[32];
     const int lane = lane_id();
     const int64_t E = misc[kMiscE];
+    // with spec, the arrivals before misc[kMiscFirst] were applied in parallel
+    const int start = spec ? misc[kMiscFirst] : 0;
+    if (start >= misc[kMiscCascades]) {
+        if (threadIdx.x == 0) misc[kMiscSteps] = 0;
+        return;
+    }
     F crit, ins;
     FlagsS dirty{nullptr};  // with spec: vertices of edges an earlier cascade kept
     if constexpr (std::is_same<F, FlagsS>::value) {
         const int64_t nw = (E + 31) >> 5;
         crit.w = sbits;
         ins.w = sbits + nw;
-        if (spec) {
+        if (spec) {  // vertices of the edges the applied cascades kept (built by k_spec_apply)
             dirty.w = sbits + 2 * nw;
-            for (int64_t k = threadIdx.x; k < ((nv + 31) >> 5); k += blockDim.x) dirty.w[k] = 0;
+            for (int64_t k = threadIdx.x; k < ((nv + 31) >> 5); k += blockDim.x) dirty.w[k] = dirty_words[k];
         }
         for (int64_t k = threadIdx.x; k < nw; k += blockDim.x) {
             uint32_t word = 0;
@@ -765,8 +834,8 @@ __global__ void __launch_bounds__(256) k_cascade(const int32_t* cas, int32_t* mi
     int size = 0;                        // P.size, broadcast
     long long steps = 0;
     bool fail = false;
-    bool kept_any = false;  // warp-uniform: some cascade has kept an edge (dirty is not empty)
-    for (int i0 = 0; i0 < ncas && !fail; i0 += kAhead) {
+    bool kept_any = start > 0;  // warp-uniform: some cascade may have kept an edge (dirty may be set)
+    for (int i0 = start; i0 < ncas && !fail; i0 += kAhead) {
         const int nb = ncas - i0 < kAhead ? ncas - i0 : kAhead;
         if (lane < nb) {  // read ahead: nothing here changes while the cascade runs
             const int32_t t = cas[i0 + lane];
@@ -789,26 +858,42 @@ __global__ void __launch_bounds__(256) k_cascade(const int32_t* cas, int32_t* mi
             }
         }
         __syncwarp();
+        // a record's vertices and kept edges (one or two per lane), loaded one
+        // arrival ahead so that the check does not wait for them
+        int32_t n_s0 = -1, n_s1 = -1, n_k = -1, n_a = -1, n_b = -1;
+        auto fetch = [&](int jj) {
+            n_s0 = n_s1 = n_k = n_a = n_b = -1;
+            if (spec && jj < nb && s_st[jj] == 0) {
+                const int32_t* r = spec + int64_t(i0 + jj) * kSpecRec;
+                const int ns = s_ns[jj], nk = s_nk[jj];
+                if (lane < ns) n_s0 = r[kRecScan + lane];
+                if (lane + 32 < ns) n_s1 = r[kRecScan + 32 + lane];
+                if (lane < nk) {
+                    n_k = r[kRecKept + lane];
+                    n_a = r[kRecKA + lane];
+                    n_b = r[kRecKB + lane];
+                }
+            }
+        };
+        fetch(0);
         for (int j = 0; j < nb && !fail; j++) {
             const int32_t t = s_t[j];
             const int no = s_no[j];
+            const int32_t c_s0 = n_s0, c_s1 = n_s1, c_k = n_k, c_a = n_a, c_b = n_b;
+            fetch(j + 1);
             if (spec && s_st[j] == 0) {
                 // the speculative run of this arrival stands when none of the
                 // vertices it read is an endpoint of an edge an earlier cascade kept
-                const int32_t* r = spec + int64_t(i0 + j) * kSpecRec;
-                const int nk = s_nk[j], ns = s_ns[j];
-                bool touched = false;
-                if (kept_any)
-                    for (int k = lane; k < ns; k += 32) touched |= dirty.get(r[4 + kSpecCrit + k]);
+                const bool touched =
+                    kept_any && ((c_s0 >= 0 && dirty.get(c_s0)) || (c_s1 >= 0 && dirty.get(c_s1)));
                 if (!__any_sync(kFull, touched)) {
-                    if (lane < nk) {
-                        const int32_t x = r[4 + lane];
-                        crit.set(x);
-                        crit_g[x] = 1;
-                        dirty.set(eu[x]);
-                        dirty.set(ev[x]);
+                    if (c_k >= 0) {
+                        crit.set(c_k);
+                        crit_g[c_k] = 1;
+                        dirty.set(c_a);
+                        dirty.set(c_b);
                     }
-                    kept_any = kept_any || nk > 0;
+                    kept_any = kept_any || s_nk[j] > 0;
                     __syncwarp();
                     continue;
                 }
@@ -960,7 +1045,7 @@ cudaError_t grow_buf(T*& p, int64_t want, cudaStream_t s) {
 
 void collapse_free(CollapseScratch& S) {
     void* ptrs[] = {S.eu, S.ev, S.ecol, S.deg, S.adj_off, S.adj, S.arr, S.crit, S.ins, S.heap, S.cas, S.open, S.nopen,
-                    S.cbuf, S.misc, S.erec, S.vrec, S.spec};
+                    S.cbuf, S.misc, S.erec, S.vrec, S.spec, S.first_mark, S.dirty_words};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     S = CollapseScratch();
@@ -985,7 +1070,9 @@ int collapse(Device& D, const DimInfo& info, uint8_t* dropped, CollapseScratch& 
         S.cap_e = ne;
     }
     if (nv + 1 > S.cap_v) {
-        if (grow_buf(S.deg, nv + 1, s) || grow_buf(S.adj_off, nv + 1, s) || grow_buf(S.vrec, nv + 1, s)) return -1;
+        if (grow_buf(S.deg, nv + 1, s) || grow_buf(S.adj_off, nv + 1, s) || grow_buf(S.vrec, nv + 1, s) ||
+            grow_buf(S.first_mark, nv + 1, s) || grow_buf(S.dirty_words, (nv + 32) / 32, s))
+            return -1;
         S.cap_v = nv + 1;
     }
     if (!S.misc && grow_buf(S.misc, 8, s)) return -1;
@@ -1009,22 +1096,17 @@ int collapse(Device& D, const DimInfo& info, uint8_t* dropped, CollapseScratch& 
              ne, D.blk, s);
         launches += 3;
     }
-    int64_t E = 0;
-    cudaMemcpyAsync(&E, D.blk + scan_blocks(ne), sizeof(int64_t), cudaMemcpyDeviceToHost, s);
-    // the edge count for the kernels (low 32 bits of the int64 total; E < 2^31)
+    // the edge count E for the kernels (low 32 bits of the int64 total: E <= ne < 2^30
+    // is checked here); the host sizes its launches by ne and reads E below,
+    // with the largest degree, in one synchronisation
+    if (2 * ne >= int64_t(INT32_MAX)) {  // neighbour-list offsets are kept as int32
+        *err_msg = "edge collapse: more than 2^30 edge columns";
+        return -1;
+    }
     cudaMemcpyAsync(S.misc + kMiscE, D.blk + scan_blocks(ne), sizeof(int32_t), cudaMemcpyDeviceToDevice, s);
-    if (cudaStreamSynchronize(s) != cudaSuccess) {
-        *err_msg = "edge collapse: edge count";
-        return -1;
-    }
-    if (E == 0) return launches;
-    if (2 * E >= int64_t(INT32_MAX)) {  // neighbour-list offsets are kept as int32
-        *err_msg = "edge collapse: more than 2^30 edges";
-        return -1;
-    }
     // adjacency: (neighbour, edge id), ascending per vertex
     cudaMemsetAsync(S.deg, 0, sizeof(int32_t) * (nv + 1), s);
-    k_cdeg<<<grid_of(E, 256), 256, 0, s>>>(S.misc, S.eu, S.ev, S.deg);
+    k_cdeg<<<grid_of(ne, 256), 256, 0, s>>>(S.misc, S.eu, S.ev, S.deg);
     {
         const int32_t* deg = S.deg;
         int64_t* off = S.adj_off;
@@ -1032,16 +1114,19 @@ int collapse(Device& D, const DimInfo& info, uint8_t* dropped, CollapseScratch& 
              [=] __device__(int64_t v, int64_t pre, int64_t) { off[v] = pre; }, nv + 1, D.blk, s);
     }
     cudaMemsetAsync(S.deg, 0, sizeof(int32_t) * (nv + 1), s);
-    k_cfill<<<grid_of(E, 256), 256, 0, s>>>(S.misc, S.eu, S.ev, S.adj_off, S.deg, S.adj);
+    k_cfill<<<grid_of(ne, 256), 256, 0, s>>>(S.misc, S.eu, S.ev, S.adj_off, S.deg, S.adj);
     k_csort<<<grid_of(nv, 128), 128, 0, s>>>(nv, S.adj_off, S.adj, S.misc);
-    k_cbounds<<<grid_of(std::max<int64_t>(E, nv), 256), 256, 0, s>>>(S.misc, nv, S.eu, S.ev, S.adj_off, S.erec, S.vrec);
+    k_cbounds<<<grid_of(std::max<int64_t>(ne, nv), 256), 256, 0, s>>>(S.misc, nv, S.eu, S.ev, S.adj_off, S.erec, S.vrec);
     launches += 7;
-    int32_t maxdeg = 0;
-    cudaMemcpyAsync(&maxdeg, S.misc + kMiscMaxDeg, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+    int32_t mm[2] = {0, 0};  // edge count, largest degree
+    cudaMemcpyAsync(mm, S.misc + kMiscE, sizeof(mm), cudaMemcpyDeviceToHost, s);
     if (cudaStreamSynchronize(s) != cudaSuccess) {
         *err_msg = "edge collapse: adjacency build";
         return -1;
     }
+    const int64_t E = mm[0];
+    const int32_t maxdeg = mm[1];
+    if (E == 0) return launches;
     // overflow buffers for common neighbourhoods larger than shared memory
     int64_t warps_a = std::min<int64_t>(E, 148 * 64);
     int64_t per_warp = maxdeg > kCapA ? maxdeg : 0;
@@ -1091,16 +1176,22 @@ int collapse(Device& D, const DimInfo& info, uint8_t* dropped, CollapseScratch& 
             spec = S.spec;
             k_cascade_spec<<<grid_of(spec_cap, kSpecWarps, 148 * 16), kSpecWarps * 32, 0, s>>>(
                 S.cas, S.misc, S.eu, S.ev, S.adj, S.adj_off, S.crit, S.open, S.nopen, S.erec, S.vrec, S.spec, spec_cap);
-            launches++;
+            cudaMemsetAsync(S.first_mark, 0x7f, sizeof(int32_t) * size_t(nv), s);  // 0x7f7f7f7f: no record
+            k_spec_marks<<<grid_of(spec_cap, 256, 148 * 8), 256, 0, s>>>(S.misc, S.spec, spec_cap, S.first_mark);
+            k_spec_first<<<grid_of(int64_t(spec_cap) * 32, 256, 148 * 16), 256, 0, s>>>(S.misc, S.spec, spec_cap,
+                                                                                        S.first_mark);
+            k_spec_apply<<<grid_of(std::max<int64_t>(spec_cap, (nv + 31) / 32 * 32), 256, 148 * 8), 256, 0, s>>>(
+                S.misc, S.spec, S.crit, S.first_mark, nv, S.dirty_words);
+            launches += 4;
         }
         k_cascade<FlagsS><<<1, 256, spec ? spec_bytes : bits_bytes, s>>>(
             S.cas, S.misc, S.eu, S.ev, S.adj, S.adj_off, S.crit, S.ins, S.heap, S.open, S.nopen, S.erec, S.vrec, S.cbuf,
-            S.cbuf + gcap, S.cbuf + 2 * gcap, gcap, max_steps, D.err, spec, spec_cap, nv);
+            S.cbuf + gcap, S.cbuf + 2 * gcap, gcap, max_steps, D.err, spec, spec_cap, nv, S.dirty_words);
     } else {
         cudaMemsetAsync(S.ins, 0, size_t(E), s);
         k_cascade<FlagsG><<<1, 32, 0, s>>>(S.cas, S.misc, S.eu, S.ev, S.adj, S.adj_off, S.crit, S.ins, S.heap,
                                            S.open, S.nopen, S.erec, S.vrec, S.cbuf, S.cbuf + gcap, S.cbuf + 2 * gcap,
-                                           gcap, max_steps, D.err, nullptr, 0, nv);
+                                           gcap, max_steps, D.err, nullptr, 0, nv, nullptr);
     }
     k_drop_edges<<<grid_of(E, 256), 256, 0, s>>>(S.misc, S.crit, S.ecol, dropped);
     launches += 7;

@@ -25,6 +25,8 @@ struct CollapseScratch {
     int4* erec = nullptr;        // [E] neighbour-list bounds of both endpoints {off[u], off[u+1], off[v], off[v+1]}
     int2* vrec = nullptr;        // [nv] neighbour-list bounds {off[w], off[w+1]}
     int32_t* spec = nullptr;     // speculative cascade records, one per arrival with re-examinations
+    int32_t* first_mark = nullptr;  // [nv] smallest record index keeping an edge at the vertex
+    uint32_t* dirty_words = nullptr;  // [nv / 32] vertices of edges the applied records keep
     int64_t cap_e = 0, cap_v = 0, cap_cbuf = 0, cap_spec = 0;
 };
 
