@@ -425,6 +425,7 @@ int run_highclear(sspp_ctx* ctx, cudaStream_t s, const DimInfo* ranges = nullptr
     const int64_t nv = info.col_end[0] - info.col_begin[0];
     const int64_t ne = info.col_end[1] - info.col_begin[1];
     CK(grow(S.deg, S.cap_deg, nv + 2, s));
+    CK(grow(S.blk, S.cap_blk, (nv + 1) / 4096 + 4, s));  // scan block sums (4,096 per block)
     CK(grow(S.adj_off, S.cap_adj_off, nv + 2, s));
     CK(grow(S.adj, S.cap_adj, 2 * ne + 1, s));
     if (ctx->params.max_iteration <= kMaskCandidates) {
@@ -1190,6 +1191,7 @@ void sspp_destroy(sspp_ctx* ctx) {
     if (ctx->hc.adj) cudaFree(ctx->hc.adj);
     if (ctx->hc.adj_src) cudaFree(ctx->hc.adj_src);
     if (ctx->hc.nmask) cudaFree(ctx->hc.nmask);
+    if (ctx->hc.blk) cudaFree(ctx->hc.blk);
     if (ctx->hc.table) cudaFree(ctx->hc.table);
     ctx->prof.release();
     for (int q = 0; q < sspp_ctx::kSide; q++)

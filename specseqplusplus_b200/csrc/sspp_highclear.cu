@@ -469,7 +469,7 @@ int highclear(Device& D, const DimInfo& info, int max_iteration, const uint8_t* 
     const int32_t* deg = S.deg;
     int64_t* adj_off = S.adj_off;
     scan([=] __device__(int64_t v) -> int64_t { return v < nv ? deg[v] : 0; },
-         [=] __device__(int64_t v, int64_t pre, int64_t) { adj_off[v] = pre; }, nv + 1, D.blk, s);
+         [=] __device__(int64_t v, int64_t pre, int64_t) { adj_off[v] = pre; }, nv + 1, S.blk, s);
     cudaMemsetAsync(S.deg, 0, sizeof(int32_t) * (nv + 1), s);
     const bool masks = max_iteration <= kMaskCandidates;
     k_adj_fill<<<gridn(info.col_end[1] - info.col_begin[1], 256), 256, 0, s>>>(

@@ -16,7 +16,8 @@ struct HighclearScratch {
     uint64_t* nmask = nullptr;      // [2 E] per entry (a, b): which candidates of a are neighbours of b
     int32_t* table = nullptr;       // open addressing, mask + 1 slots
     uint32_t mask = 0;
-    int64_t cap_deg = 0, cap_adj_off = 0, cap_adj = 0, cap_table = 0, cap_src = 0, cap_nmask = 0;
+    int64_t* blk = nullptr;         // block sums of its own scans (the branch runs beside the reorder's scans)
+    int64_t cap_deg = 0, cap_adj_off = 0, cap_adj = 0, cap_table = 0, cap_src = 0, cap_nmask = 0, cap_blk = 0;
 };
 
 // Up to this many candidates per simplex (max_iteration) the test runs on

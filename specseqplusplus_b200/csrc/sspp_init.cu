@@ -411,7 +411,7 @@ __global__ void k_init_apparent(int64_t n, const int32_t* arena, const uint64_t*
 // dimension row bounds of the schedule (min first row over non-empty columns,
 // max lowest row + 1 over active ones; ColumnShrink, include/specseq.h:374-398)
 // into info, whose bounds must start at INT_MAX / -1.
-__global__ void k_init_compress(int64_t n, int32_t* arena, uint64_t* desc, int32_t* low, const uint64_t* pivot,
+__global__ void k_init_compress(int64_t cb, int64_t n, int32_t* arena, uint64_t* desc, int32_t* low, const uint64_t* pivot,
                                 const uint8_t* cleared, const uint8_t* negative, uint8_t* state,
                                 const uint8_t* dropped, bool keep_rows, int4* app, const int32_t* rinfo,
                                 DimInfo* info, long long* counters, int* err) {
@@ -422,7 +422,7 @@ __global__ void k_init_compress(int64_t n, int32_t* arena, uint64_t* desc, int32
     }
     __syncthreads();
     long long ncl = 0, nact = 0;
-    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    for (int64_t i = cb + blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
         if (app && pivot[i] == kNoOwner) app[i] = make_int4(-1, INT_MAX, INT_MAX, INT_MAX);
         uint64_t d = desc[i];
         int32_t* hdr = arena + desc_off(d);
@@ -528,15 +528,17 @@ int init_passes(Device& D, bool lows_done, cudaStream_t s) {
     return lows_done ? 1 : 2;
 }
 
-int init_compress(Device& D, const uint8_t* dropped, bool keep_rows, bool final, cudaStream_t s) {
-    const int64_t n = D.n;
+int init_compress(Device& D, const uint8_t* dropped, bool keep_rows, bool final, cudaStream_t s, int64_t cb,
+                  int64_t ce, bool reset) {
+    const int64_t n = ce < 0 ? D.n : ce;
+    if (n <= cb) return 0;
     // the row bounds go to the DimInfo through a few atomics per block: few blocks
-    const unsigned g = grid_for(n, 256) > 4096 ? 4096 : grid_for(n, 256);
-    if (final) k_diminfo_reset<<<1, 32, 0, s>>>(D.diminfo);
-    k_init_compress<<<g, 256, 0, s>>>(n, D.arena, D.desc, D.low, D.pivot, D.cleared, D.negative, D.state, dropped,
+    const unsigned g = grid_for(n - cb, 256) > 4096 ? 4096 : grid_for(n - cb, 256);
+    if (final && reset) k_diminfo_reset<<<1, 32, 0, s>>>(D.diminfo);
+    k_init_compress<<<g, 256, 0, s>>>(cb, n, D.arena, D.desc, D.low, D.pivot, D.cleared, D.negative, D.state, dropped,
                                       keep_rows, final ? D.app : nullptr, final ? D.dim : nullptr, D.diminfo,
                                       D.counters, D.err);
-    return final ? 2 : 1;
+    return final && reset ? 2 : 1;
 }
 
 // Inline copies of the short apparent columns, by row (see Device::app).

@@ -38,7 +38,10 @@ int init_passes(Device& D, bool lows_done, cudaStream_t s);
 // representative cycles); otherwise they are removed.
 // final (no dualization follows): also the inline apparent columns (as
 // build_apparent) and the per-dimension row bounds (as active_list)
-int init_compress(Device& D, const uint8_t* dropped, bool keep_rows, bool final, cudaStream_t s);
+// columns [cb, ce) (ce < 0: to the end); reset: clear the row bounds first
+// (the first of the launches that together cover every column)
+int init_compress(Device& D, const uint8_t* dropped, bool keep_rows, bool final, cudaStream_t s, int64_t cb = 0,
+                  int64_t ce = -1, bool reset = true);
 // rows_done: init_compress already gathered the row bounds
 int active_list(Device& D, bool rows_done, cudaStream_t s);
 // D.app from the pivot table as it stands (apparent pairs only)
