@@ -24,11 +24,14 @@ const Knobs kCandidates[] = {
 };
 constexpr int kNumBase = int(sizeof(kCandidates) / sizeof(kCandidates[0]));
 constexpr int kRetryEvery = 32;
-// Inputs this large are not used to explore: a poor candidate there (a dual
-// reduction of a large lower-star grid takes four times as long) costs more
-// than what it could teach.  They take the lowest estimate instead: their own
-// class's mean where measured, else what similar smaller classes measured.
+// Inputs this large explore only once their class has run kExploreMinRuns
+// times (a repeated workload, where what is learnt pays back): a poor
+// candidate on a one-off large input (a dual reduction of a large lower-star
+// grid takes four times as long) costs more than it could teach.  Until then
+// they take the lowest estimate: their own class's mean where measured, else
+// what similar smaller classes measured.
 constexpr int64_t kExploreMaxCols = int64_t(1) << 20;
+constexpr int64_t kExploreMinRuns = 2;
 
 struct Entry {
     std::vector<double> mean;   // ms per million columns
@@ -99,7 +102,7 @@ int tune_choose(int64_t ncols, int32_t shape, int32_t model, int32_t dualize, in
     // untried candidates, best first by what similar classes measured; those
     // over twice as slow there as the best are left out of the first round
     const std::vector<double> prior = prior_of(k, n);
-    if (ncols >= kExploreMaxCols) {
+    if (ncols >= kExploreMaxCols && e.total < kExploreMinRuns) {
         double bv = HUGE_VAL;
         for (int c = 0; c < n; c++) {
             const double v = e.runs[size_t(c)] > 0 ? e.mean[size_t(c)] : prior[size_t(c)];
@@ -117,7 +120,9 @@ int tune_choose(int64_t ncols, int32_t shape, int32_t model, int32_t dualize, in
     for (double v : prior) best_prior = std::min(best_prior, v);
     for (int c = 0; c < n; c++) {
         if (e.runs[size_t(c)] > 0) continue;
-        if (std::isfinite(prior[size_t(c)]) && prior[size_t(c)] > 2.0 * best_prior) continue;  // measured slow
+        // measured slow on similar inputs: over twice the best, or a quarter more on large inputs
+        const double slack = ncols >= kExploreMaxCols ? 1.25 : 2.0;
+        if (std::isfinite(prior[size_t(c)]) && prior[size_t(c)] > slack * best_prior) continue;
         if (pick < 0 || prior[size_t(c)] < prior[size_t(pick)]) pick = c;
     }
     if (pick < 0 && e.total % kRetryEvery == kRetryEvery - 1) {

@@ -10,12 +10,14 @@
 // (same key but size), leaving out those over twice as slow there as the best,
 // then runs the fastest (by running mean of ms per column), re-trying the least
 // recently measured one every 32nd run so that the choice follows drift.
-// Inputs of 2^20 columns or more never explore: they take the lowest estimate
-// (their class's own mean, else the similar classes'), or the first candidate
-// when nothing is known.  Every candidate gives the same pairs; only the time
-// differs.  The history also
-// keeps the largest arena fill seen per class (arena ints used / base ints),
-// which admission control turns into a device-memory estimate.
+// Inputs of 2^20 columns or more explore only once their class has run twice
+// (a repeated workload), and skip candidates a quarter slower than the best on
+// similar inputs; before that they take the lowest estimate (their class's own
+// mean, else the similar classes'), or the first candidate when nothing is
+// known.  Every candidate gives the same pairs; only the time
+// differs.  The history also keeps the largest arena fill seen per class
+// (arena ints used / base ints), which admission control turns into a
+// device-memory estimate.
 #pragma once
 #include <stdint.h>
 
