@@ -628,6 +628,32 @@ constexpr int kCacheRefill = 16;  // cache lanes used before the cache is filled
 #define SSPP_FAST_PVPF 0
 #endif
 
+// Inline apparent columns of the delta's entries (SSPP_FAST_DAP): when an
+// entry enters the delta, its row's inline column is copied asynchronously
+// (cp.async) into a ring of shared-memory slots, and the entry's lane keeps
+// the insertion index with it as entries shift.  When the delta's top becomes
+// the lowest row, often many additions after it was inserted, its column is
+// already in shared memory: no dependent global load on the chain.  Copies are
+// committed once per addition (or run); a read waits only for the group its
+// entry was inserted in, and each commit first lets all but the last two
+// groups finish, so a slot is never reused while a copy to it is in flight
+// (two groups hold at most 2 x 96 insertions, the ring has 256 slots).
+#ifndef SSPP_FAST_DAP
+#define SSPP_FAST_DAP 1
+#endif
+constexpr int kDapSlots = 256;
+static_assert(!(SSPP_FAST_DAP && SSPP_FAST_TOGGLE3), "the three-entry toggle does not carry insertion indices");
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 // largest entry of an inline apparent column below its top (-1 if none)
 __device__ __forceinline__ int app_max_below(int4 q) {
     return q.x <= 0 ? -1 : (q.x == 1 ? q.y : (q.x == 2 ? q.z : q.w));
@@ -638,6 +664,9 @@ __device__ int fast_adds(const BlockG<T>& g, const ReduceArgs& A, int32_t minrow
                          uint64_t& e, int32_t* tmp, int32_t* sb, long long& adds, long long& add_ints,
                          int iters_left) {
     __shared__ FastState fs;
+#if SSPP_FAST_DAP
+    __shared__ int4 s_dap[kDapSlots];
+#endif
     (void)sb;
     if (threadIdx.x < 32) {
         const int lane = threadIdx.x;
@@ -663,6 +692,18 @@ __device__ int fast_adds(const BlockG<T>& g, const ReduceArgs& A, int32_t minrow
         uint64_t ec_pf = kNoOwner;
         int next_clear = kClearCheck;  // additions before the next look at the cleared flag
         bool have_e = true;  // ec is the pivot entry of Lc
+#if SSPP_FAST_DAP
+        int dslot = 0;  // insertion index of dv (lanes < d); its inline column is s_dap[dslot % kDapSlots]
+        int nslot = 0;  // insertions so far
+        int g_open = 0, g_last = 0, g_prev = 0;  // first insertion of the open, last and previous groups
+        auto dap_commit = [&]() {
+            cp_async_commit();
+            cp_async_wait<2>();  // every group before the last two has landed
+            g_prev = g_last;
+            g_last = g_open;
+            g_open = nslot;
+        };
+#endif
         // toggles x in the delta (a fold into the bulk when the delta is full
         // invalidates the bulk cache)
         auto toggle = [&](int x) {
@@ -670,7 +711,15 @@ __device__ int fast_adds(const BlockG<T>& g, const ReduceArgs& A, int32_t minrow
             if (eq) {
                 const int q = __ffs(eq) - 1;
                 const int nx = __shfl_down_sync(kFull, dv, 1);
+#if SSPP_FAST_DAP
+                const int ns = __shfl_down_sync(kFull, dslot, 1);
+                if (lane >= q) {
+                    dv = lane + 1 < d ? nx : INT_MAX;
+                    dslot = ns;
+                }
+#else
                 if (lane >= q) dv = lane + 1 < d ? nx : INT_MAX;
+#endif
                 d--;
             } else {
                 if (d == 32) {  // full: the bulk absorbs the delta
@@ -681,8 +730,24 @@ __device__ int fast_adds(const BlockG<T>& g, const ReduceArgs& A, int32_t minrow
                 }
                 const int q = __popc(__ballot_sync(kFull, lane < d && dv < x));
                 const int pv = __shfl_up_sync(kFull, dv, 1);
+#if SSPP_FAST_DAP
+                const int ps = __shfl_up_sync(kFull, dslot, 1);
+                if (lane > q && lane <= d) {
+                    dv = pv;
+                    dslot = ps;
+                }
+                if (lane == q) {
+                    dv = x;
+                    dslot = nslot;
+                    int4* dst = s_dap + (nslot & (kDapSlots - 1));
+                    if (x >= 0 && x < A.ncols) cp_async16(dst, A.app + x);
+                    else *dst = make_int4(-1, 0, 0, 0);
+                }
+                nslot++;
+#else
                 if (lane > q && lane <= d) dv = pv;
                 if (lane == q) dv = x;
+#endif
                 d++;
             }
         };
@@ -764,6 +829,14 @@ __device__ int fast_adds(const BlockG<T>& g, const ReduceArgs& A, int32_t minrow
                     break;
                 }
             } else {
+#if SSPP_FAST_DAP
+                // the low is the delta's top (lane d - 1): its column is in the ring
+                const int idx = __shfl_sync(kFull, dslot, d - 1);
+                if (idx >= g_last) cp_async_wait<0>();
+                else if (idx >= g_prev) cp_async_wait<1>();
+                __syncwarp();
+                ap = s_dap[idx & (kDapSlots - 1)];
+#else
                 const unsigned pm = __ballot_sync(kFull, pf_row == Lc);
                 const int src = pm ? __ffs(pm) - 1 : 31;
                 ap = pf_ap;
@@ -777,6 +850,7 @@ __device__ int fast_adds(const BlockG<T>& g, const ReduceArgs& A, int32_t minrow
                 ap.w = __shfl_sync(kFull, ap.w, src);
                 have_pf_pv = pm != 0 && ap.x < 0 && SSPP_FAST_PREFETCH && SSPP_FAST_PVPF;
                 if (have_pf_pv) ec_pf = __shfl_sync(kFull, (unsigned long long)pf_pv, src);
+#endif
             }
             if (top_in_bulk && ap.x >= 0) {
                 // a run from cache lane h: lane l (> h) joins while lanes h..l-1
@@ -829,6 +903,9 @@ __device__ int fast_adds(const BlockG<T>& g, const ReduceArgs& A, int32_t minrow
                     done += P;
                     n_inline += P;
                     pf_row = -1;
+#if SSPP_FAST_DAP
+                    dap_commit();
+#endif
                     // the next lowest row: the larger top; equal tops cancel
                     int nl = -1;
                     while (true) {
@@ -887,7 +964,7 @@ __device__ int fast_adds(const BlockG<T>& g, const ReduceArgs& A, int32_t minrow
             // the addend's three largest other entries: their inline apparent
             // columns load while this addition runs
             pf_row = -1;
-            if (SSPP_FAST_PREFETCH && lane < m && lane >= m - 3 && bj >= 0 && bj < A.ncols) {
+            if (SSPP_FAST_PREFETCH && !SSPP_FAST_DAP && lane < m && lane >= m - 3 && bj >= 0 && bj < A.ncols) {
                 pf_row = bj;
                 pf_ap = __ldg(A.app + bj);
                 if (SSPP_FAST_PVPF) pf_pv = ld_relaxed_u64(A.pivot + bj);
@@ -904,6 +981,9 @@ __device__ int fast_adds(const BlockG<T>& g, const ReduceArgs& A, int32_t minrow
             } else {
                 for (int j = 0; j < m; j++) toggle(__shfl_sync(kFull, bj, j));
             }
+#if SSPP_FAST_DAP
+            dap_commit();
+#endif
             // the next lowest row: the larger top; equal tops cancel
             int nl = -1;
             while (true) {
@@ -931,6 +1011,9 @@ __device__ int fast_adds(const BlockG<T>& g, const ReduceArgs& A, int32_t minrow
             ec = kNoOwner;  // unknown; the general path's claim retries with the real entry
         }
         if (d > 0) nb = fold_delta(a, nb, dv, d, tmp, A.err);
+#if SSPP_FAST_DAP
+        cp_async_wait<0>();  // no copy may land in the ring after this call
+#endif
         if (lane == 0) {
             fs.len = nb;
             fs.L = nb > 0 ? lds(a + nb - 1) : -1;
