@@ -361,7 +361,7 @@ def leg_batched(steps):
             "oracle_sample": f"{len(sample)} of {len(mats)} instances (every 32nd)"}
 
 
-def leg_served(count=48, rates=(100.0, None)):
+def leg_served(count=48, rates=(100.0, None), workers=2):
     """Poisson request stream (Rips 300-20,000 pts 2-D/3-D degree 8-40; lower-star 16^3-96^3 sigma 1-3):
     the serving loop (2 workers, autotune 2, continuous batching) vs a serial one-at-a-time loop with the
     reference's default parameters."""
@@ -400,7 +400,7 @@ def leg_served(count=48, rates=(100.0, None)):
         cp, lp, pres = plain(Params())
         if plain_results is None:
             plain_results = pres
-        with Server(Params(autotune=2), workers=2) as srv:
+        with Server(Params(autotune=2), workers=workers) as srv:
             for _ in range(3):
                 ids = [srv.submit(m, copy=False) for m in warm]
                 for i in ids:
@@ -425,6 +425,8 @@ def leg_served(count=48, rates=(100.0, None)):
                              "served_mean_batch": st["mean_batch_requests"],
                              "plain_cols_per_s": cp, "plain_p50_ms": float(lp[0]), "plain_p95_ms": float(lp[1]),
                              "plain_p99_ms": float(lp[2]), "speedup_vs_plain": st["cols_per_s"] / cp,
+                             "served_phase_s": {"load": st["load_s"], "reduce": st["reduce_s"],
+                                                "results": st["results_s"]},
                              "results_equal_plain": bool(same)})
     # the serial loop's results (which every served result equals) against the
     # oracle on a sample: every 6th request by size, up to 5 M columns each
@@ -435,11 +437,12 @@ def leg_served(count=48, rates=(100.0, None)):
                               "exact": bool(all(np.array_equal(plain_results[i][0], r.pairs) and
                                                 np.array_equal(plain_results[i][1], r.essential)
                                                 for i, r in ((i, orc.reduce(mats[i])) for i in sample)))}
-    out["built"] = served_built(stream, N, plain_results)
+    out["workers"] = workers
+    out["built"] = served_built(stream, N, plain_results, workers)
     return out
 
 
-def served_built(stream, N, want):
+def served_built(stream, N, want, workers=2):
     """The same requests given as point clouds and fields (the complexes are built on the device), all at
     once: the server against a serial one-at-a-time loop of device build + reduction."""
     from specseqplusplus_b200 import Engine, Params, Server, gen
@@ -470,7 +473,7 @@ def served_built(stream, N, want):
             res.append((e.pairs(), e.essentials()))
             lat.append(1000 * (time.perf_counter() - t0))
         plain = N / (time.perf_counter() - t0)
-    with Server(Params(autotune=2), workers=2) as srv:
+    with Server(Params(autotune=2), workers=workers) as srv:
         for _ in range(2):
             ids = [srv.submit_rips(x[1], x[2], x[3], copy=False) if x[0] == "r" else
                    srv.submit_lowerstar(x[1], x[3], copy=False) for x in inputs[:16]]
