@@ -361,9 +361,9 @@ def leg_batched(steps):
             "oracle_sample": f"{len(sample)} of {len(mats)} instances (every 32nd)"}
 
 
-def leg_served(count=48, rates=(100.0, None), workers=2):
+def leg_served(count=48, rates=(100.0, None), workers=3):
     """Poisson request stream (Rips 300-20,000 pts 2-D/3-D degree 8-40; lower-star 16^3-96^3 sigma 1-3):
-    the serving loop (2 workers, autotune 2, continuous batching) vs a serial one-at-a-time loop with the
+    the serving loop (3 workers, autotune 2, continuous batching) vs a serial one-at-a-time loop with the
     reference's default parameters."""
     from specseqplusplus_b200 import Engine, Params, Server, workloads
 
@@ -442,7 +442,7 @@ def leg_served(count=48, rates=(100.0, None), workers=2):
     return out
 
 
-def served_built(stream, N, want, workers=2):
+def served_built(stream, N, want, workers=3):
     """The same requests given as point clouds and fields (the complexes are built on the device), all at
     once: the server against a serial one-at-a-time loop of device build + reduction."""
     from specseqplusplus_b200 import Engine, Params, Server, gen

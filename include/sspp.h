@@ -43,7 +43,10 @@ typedef struct sspp_config {
     int32_t host_threads;    /* host threads for staged copies; 0 = all cores         */
     int32_t sm_share;        /* persistent reduction launches use 1/sm_share of the
                                 GPU (contexts that run side by side, e.g. a server's
-                                workers); 0 or 1 = the whole GPU                     */
+                                workers); 0 or 1 = the whole GPU.  Above 1 the
+                                autotuner also tries no candidate on inputs of 2^20
+                                columns or more (a slow trial would delay the other
+                                contexts' work)                                      */
 } sspp_config;
 
 /* The reference's 12 positional CLI values (src/main.cu:281-294) minus file

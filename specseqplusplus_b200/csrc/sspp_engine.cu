@@ -456,7 +456,9 @@ int autotune_choose(sspp_ctx* ctx) {
     ctx->tune_shape = top * 4 + std::min(3, int(frac * 4.0));
     const sspp_params& u = ctx->user_params;
     Knobs k;
-    ctx->tune_cand = tune_choose(D.n, ctx->tune_shape, u.model, u.dualize, tune_allows_dual(u), &k);
+    // contexts that share the GPU (a server's workers) do not try candidates on large inputs
+    ctx->tune_cand = tune_choose(D.n, ctx->tune_shape, u.model, u.dualize, tune_allows_dual(u), &k,
+                                 ctx->cfg.sm_share <= 1);
     sspp_params& q = ctx->params;
     q.ss_block_size = k.ss_block_size;
     q.growth = k.growth;

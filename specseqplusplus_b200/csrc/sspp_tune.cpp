@@ -93,7 +93,8 @@ std::vector<double> prior_of(const Key& k, int n) {
 
 }  // namespace
 
-int tune_choose(int64_t ncols, int32_t shape, int32_t model, int32_t dualize, int32_t allow_dual, Knobs* out) {
+int tune_choose(int64_t ncols, int32_t shape, int32_t model, int32_t dualize, int32_t allow_dual, Knobs* out,
+                bool explore_large) {
     std::lock_guard<std::mutex> l(g_mu);
     const Key k = key_of(ncols, shape, model, dualize, allow_dual);
     Entry& e = entry_of(k, allow_dual);
@@ -102,7 +103,7 @@ int tune_choose(int64_t ncols, int32_t shape, int32_t model, int32_t dualize, in
     // untried candidates, best first by what similar classes measured; those
     // over twice as slow there as the best are left out of the first round
     const std::vector<double> prior = prior_of(k, n);
-    if (ncols >= kExploreMaxCols && e.total < kExploreMinRuns) {
+    if (ncols >= kExploreMaxCols && (!explore_large || e.total < kExploreMinRuns)) {
         double bv = HUGE_VAL;
         for (int c = 0; c < n; c++) {
             const double v = e.runs[size_t(c)] > 0 ? e.mean[size_t(c)] : prior[size_t(c)];

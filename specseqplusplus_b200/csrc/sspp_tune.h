@@ -39,7 +39,11 @@ struct Knobs {
 // shape: a coarse description of the complex (top dimension and the share of
 // its columns there), so that, e.g., grids and Rips complexes of one size
 // class are tuned apart
-int tune_choose(int64_t ncols, int32_t shape, int32_t model, int32_t dualize, int32_t allow_dual, Knobs* out);
+// explore_large = false: inputs of 2^20 columns or more never explore (a
+// context that shares the GPU with others, e.g. a server worker: a slow trial
+// there delays every request behind it)
+int tune_choose(int64_t ncols, int32_t shape, int32_t model, int32_t dualize, int32_t allow_dual, Knobs* out,
+                bool explore_large = true);
 void tune_record(int64_t ncols, int32_t shape, int32_t model, int32_t dualize, int32_t allow_dual, int cand,
                  double ms, double arena_fill);
 // largest arena fill (used / base) recorded for this class (or, before any
